@@ -1,0 +1,852 @@
+// CPU oracle for the HDG element hot path -- TEST INFRASTRUCTURE ONLY.
+//
+// This is a plain restatement of the reference's algorithm, used by the tests,
+// by the smoke check and by the bench's CPU-baseline leg as the checker.  The
+// product path never calls it.  Each routine cites the reference code it
+// restates (paths relative to the exapde/hfem tree).
+//
+// Parity of this restatement is pinned against the reference C++ itself,
+// compiled from its own sources (oracle/Makefile -> oracle/_ref/hfem_ref), on
+// identical inputs; the golden fixtures under tests/golden were made that way.
+//
+// Layout conventions follow the reference (column-major, quadrature point or
+// node index fastest):
+//   udg  : npv x nc  per element   (u = comps 0..ncu-1, q_d = comps ncu*(1+d)+c)
+//   uh   : nch x ndofuh
+//   D    : (npv*ncu) x (npv*ncu)   D[i + npv*(j + ncu*(n + npv*k))]
+//   F    : (npv*ncu) x (nch*ndf)   F[i + npv*(j + ncu*(m + nch*fn))]
+//   K    : (nch*ndf) x (npv*ncu)   K[j + nch*fn + nb*(n + npv*m)]
+//   H    : (nch*ndf) x (nch*ndf)   H[j + nch*fn + nb*(m + nch*fn2)]
+//   Hg   : numBlocks x bsz x bsz (column-major blocks), Rg : nf x bsz
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+extern "C" {
+
+struct oracle_problem {
+    int nd, npv, npf, nfe, ngv, ngf, ne, nf;
+    const double *shapvt, *shapvg, *shapvgdotshapvl;   // master volume tables
+    const double *shapft, *shapfg, *shapfgdotshapfc;   // master face tables (one face)
+    const int *perm;                                   // nfe x npf (face-major)
+    const double *dgnodes;                             // npv x nd x ne
+    const int *elcon;                                  // ndf x ne
+    const int *t2f;                                    // nfe x ne
+    const int *rowstart, *colidx;                      // face-block CSR, diagonal first
+    double param[6];                                   // gamma eps Re Pr Mach tau
+    int tdep;
+    double fc_u, fc_q, time;
+};
+
+}  // extern "C"
+
+namespace {
+
+// ------------------------------------------------------------ dual numbers
+// Forward-mode derivatives for the pointwise flux Jacobian (the reference uses
+// symbolically generated derivatives, application/FM/nsNew/flux_ns2dNEW.c).
+constexpr int NDMAX = 20;
+struct Dual {
+    double v;
+    double d[NDMAX];
+    int n;
+};
+static Dual dconst(double v, int n) { Dual r; r.v = v; r.n = n; for (int i = 0; i < n; i++) r.d[i] = 0; return r; }
+static Dual dvar(double v, int n, int k) { Dual r = dconst(v, n); r.d[k] = 1.0; return r; }
+static Dual operator+(const Dual& a, const Dual& b) { Dual r = a; r.v += b.v; for (int i = 0; i < a.n; i++) r.d[i] += b.d[i]; return r; }
+static Dual operator-(const Dual& a, const Dual& b) { Dual r = a; r.v -= b.v; for (int i = 0; i < a.n; i++) r.d[i] -= b.d[i]; return r; }
+static Dual operator*(const Dual& a, const Dual& b) { Dual r; r.n = a.n; r.v = a.v * b.v; for (int i = 0; i < a.n; i++) r.d[i] = a.d[i] * b.v + a.v * b.d[i]; return r; }
+static Dual operator*(double s, const Dual& a) { Dual r = a; r.v *= s; for (int i = 0; i < a.n; i++) r.d[i] *= s; return r; }
+static Dual operator/(const Dual& a, const Dual& b) {
+    Dual r; r.n = a.n; r.v = a.v / b.v;
+    for (int i = 0; i < a.n; i++) r.d[i] = (a.d[i] * b.v - a.v * b.d[i]) / (b.v * b.v);
+    return r;
+}
+
+// Compressible Navier-Stokes flux F(u, q) (application/FM/nsNew/flux_ns2dNEW.c:22-74
+// and flux_ns3dNEW.c), constant viscosity mu = 1 (FM/getViscosity.c:5-12):
+//   f_rho^d = m_d
+//   f_mi^d  = m_i v_d + p delta_id + tau_id
+//   f_E^d   = (E + p) v_d + sum_i tau_id v_i + mu gamma/(Re Pr) (q_E^d/rho - E q_rho^d/rho^2 - sum_i v_i dv_i/dx_d)
+// with dv_i/dx_d := (q_mi^d - v_i q_rho^d)/rho, tau_ij = mu/Re (dv_i/dx_j + dv_j/dx_i - 2/3 delta_ij div v).
+static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*ncu + c] */) {
+    const int ncu = nd + 2;
+    const int n = w[0].n;
+    const double gam = param[0], Re = param[2], Pr = param[3];
+    Dual rho = w[0];
+    Dual E = w[nd + 1];
+    Dual v[3], dv[3][3];
+    Dual ke = dconst(0.0, n);
+    for (int i = 0; i < nd; i++) { v[i] = w[1 + i] / rho; ke = ke + v[i] * w[1 + i]; }
+    Dual p = (gam - 1.0) * (E - 0.5 * ke);
+    for (int d = 0; d < nd; d++) {
+        const Dual* q = &w[ncu * (1 + d)];
+        for (int i = 0; i < nd; i++) dv[i][d] = (q[1 + i] - v[i] * q[0]) / rho;
+    }
+    Dual div = dconst(0.0, n);
+    for (int i = 0; i < nd; i++) div = div + dv[i][i];
+    Dual tau[3][3];
+    for (int i = 0; i < nd; i++)
+        for (int j = 0; j < nd; j++) {
+            Dual t = dv[i][j] + dv[j][i];
+            if (i == j) t = t - (2.0 / 3.0) * div;
+            tau[i][j] = (1.0 / Re) * t;
+        }
+    const double kappa = gam / (Re * Pr);
+    for (int d = 0; d < nd; d++) {
+        const Dual* q = &w[ncu * (1 + d)];
+        f[d * ncu + 0] = w[1 + d];
+        for (int i = 0; i < nd; i++) {
+            Dual t = w[1 + i] * v[d] + tau[i][d];
+            if (i == d) t = t + p;
+            f[d * ncu + 1 + i] = t;
+        }
+        Dual fe = (E + p) * v[d];
+        Dual vdv = dconst(0.0, n);
+        for (int i = 0; i < nd; i++) { fe = fe + tau[i][d] * v[i]; vdv = vdv + v[i] * dv[i][d]; }
+        Dual heat = q[nd + 1] / rho - E * q[0] / (rho * rho) - vdv;
+        f[d * ncu + nd + 1] = fe + kappa * heat;
+    }
+}
+
+// Pointwise flux and Jacobian: f[g + ng*(c + ncu*d)], f_udg[g + ng*(c + ncu*(d + nd*k))].
+static void flux_points(int nd, const double* param, int ng, const double* udg /* ng x nc */,
+                        double* f, double* f_udg) {
+    const int ncu = nd + 2, nc = ncu * (nd + 1);
+    std::vector<Dual> w(nc), fl(ncu * nd);
+    for (int g = 0; g < ng; g++) {
+        for (int k = 0; k < nc; k++) w[k] = dvar(udg[g + ng * k], nc, k);
+        ns_flux(nd, param, w.data(), fl.data());
+        for (int d = 0; d < nd; d++)
+            for (int c = 0; c < ncu; c++) {
+                const Dual& x = fl[d * ncu + c];
+                f[g + ng * (c + ncu * d)] = x.v;
+                for (int k = 0; k < nc; k++) f_udg[g + ng * (c + ncu * (d + nd * k))] = x.d[k];
+            }
+    }
+}
+
+// ------------------------------------------------------------ small dense LA
+// column-major helpers
+static void cholesky(int n, double* a) {       // lower factor in place (upper untouched)
+    for (int j = 0; j < n; j++) {
+        double s = a[j + n * j];
+        for (int k = 0; k < j; k++) s -= a[j + n * k] * a[j + n * k];
+        s = std::sqrt(s);
+        a[j + n * j] = s;
+        for (int i = j + 1; i < n; i++) {
+            double t = a[i + n * j];
+            for (int k = 0; k < j; k++) t -= a[i + n * k] * a[j + n * k];
+            a[i + n * j] = t / s;
+        }
+    }
+}
+static void chol_solve(int n, const double* l, int nrhs, double* b) {
+    for (int r = 0; r < nrhs; r++) {
+        double* x = b + (size_t)n * r;
+        for (int i = 0; i < n; i++) { double t = x[i]; for (int k = 0; k < i; k++) t -= l[i + n * k] * x[k]; x[i] = t / l[i + n * i]; }
+        for (int i = n - 1; i >= 0; i--) { double t = x[i]; for (int k = i + 1; k < n; k++) t -= l[k + n * i] * x[k]; x[i] = t / l[i + n * i]; }
+    }
+}
+static int lu_factor(int n, double* a, int* piv) {  // partial pivoting, LAPACK-style row swaps
+    for (int j = 0; j < n; j++) {
+        int p = j;
+        double m = std::fabs(a[j + n * j]);
+        for (int i = j + 1; i < n; i++) if (std::fabs(a[i + n * j]) > m) { m = std::fabs(a[i + n * j]); p = i; }
+        piv[j] = p;
+        if (a[p + n * j] == 0.0) return j + 1;
+        if (p != j) for (int k = 0; k < n; k++) std::swap(a[j + n * k], a[p + n * k]);
+        double inv = 1.0 / a[j + n * j];
+        for (int i = j + 1; i < n; i++) a[i + n * j] *= inv;
+        for (int k = j + 1; k < n; k++) {
+            double t = a[j + n * k];
+            if (t != 0.0) for (int i = j + 1; i < n; i++) a[i + n * k] -= a[i + n * j] * t;
+        }
+    }
+    return 0;
+}
+static void lu_solve(int n, const double* lu, const int* piv, int nrhs, double* b) {
+    for (int r = 0; r < nrhs; r++) {
+        double* x = b + (size_t)n * r;
+        for (int i = 0; i < n; i++) if (piv[i] != i) std::swap(x[i], x[piv[i]]);
+        for (int i = 0; i < n; i++) { double t = x[i]; for (int k = 0; k < i; k++) t -= lu[i + n * k] * x[k]; x[i] = t; }
+        for (int i = n - 1; i >= 0; i--) { double t = x[i]; for (int k = i + 1; k < n; k++) t -= lu[i + n * k] * x[k]; x[i] = t / lu[i + n * i]; }
+    }
+}
+
+struct Dims {
+    int nd, npv, npf, nfe, ngv, ngf, ncu, nc, nch, ndf, nd1, n, nb, bsz;
+    explicit Dims(const oracle_problem& P) {
+        nd = P.nd; npv = P.npv; npf = P.npf; nfe = P.nfe; ngv = P.ngv; ngf = P.ngf;
+        ncu = nd + 2; nc = ncu * (nd + 1); nch = ncu; ndf = npf * nfe; nd1 = nd + 1;
+        n = npv * ncu; nb = nch * ndf; bsz = nch * npf;
+    }
+};
+
+// Volume and face geometry (elementassembly.cpp:11-127 elementgeom, 129-237 facegeom).
+//   jac[g], Xx[g + ngv*(d + nd*i)] = adj(J)_{i d} with J_{d i} = dx_d/dxi_i
+//   face: pgf, nl[g' + ngf*nfe*d], jacf[g'] with g' = g + ngf*face
+struct Geom {
+    std::vector<double> jac, Xx, jacf, nl;
+};
+static void geometry(const oracle_problem& P, const Dims& D, int ie, Geom& G) {
+    const int nd = D.nd, npv = D.npv, ngv = D.ngv, ngf = D.ngf, nfe = D.nfe, npf = D.npf;
+    const double* x = P.dgnodes + (size_t)ie * npv * nd;
+    G.jac.assign(ngv, 0.0);
+    G.Xx.assign(ngv * nd * nd, 0.0);
+    for (int g = 0; g < ngv; g++) {
+        double J[3][3] = {{0}};
+        for (int d = 0; d < nd; d++)
+            for (int i = 0; i < nd; i++) {
+                double s = 0;
+                for (int a = 0; a < npv; a++) s += P.shapvt[g + ngv * (a + npv * (i + 1))] * x[a + npv * d];
+                J[d][i] = s;
+            }
+        double adj[3][3];
+        double det;
+        if (nd == 2) {
+            det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+            adj[0][0] = J[1][1]; adj[0][1] = -J[0][1];
+            adj[1][0] = -J[1][0]; adj[1][1] = J[0][0];
+        } else {
+            adj[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+            adj[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+            adj[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+            adj[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+            adj[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+            adj[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+            adj[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+            adj[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+            adj[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+            det = J[0][0] * adj[0][0] + J[0][1] * adj[1][0] + J[0][2] * adj[2][0];
+        }
+        G.jac[g] = det;
+        for (int d = 0; d < nd; d++)
+            for (int i = 0; i < nd; i++) G.Xx[g + ngv * (d + nd * i)] = adj[i][d];
+    }
+    const int na = ngf * nfe;
+    G.jacf.assign(na, 0.0);
+    G.nl.assign(na * nd, 0.0);
+    for (int f = 0; f < nfe; f++)
+        for (int g = 0; g < ngf; g++) {
+            double T[3][2] = {{0}};
+            for (int d = 0; d < nd; d++)
+                for (int r = 0; r < nd - 1; r++) {
+                    double s = 0;
+                    for (int m = 0; m < npf; m++)
+                        s += P.shapft[g + ngf * (m + npf * (r + 1))] * x[P.perm[f * npf + m] + npv * d];
+                    T[d][r] = s;
+                }
+            double nv[3];
+            if (nd == 2) { nv[0] = T[1][0]; nv[1] = -T[0][0]; }
+            else {
+                nv[0] = T[1][0] * T[2][1] - T[2][0] * T[1][1];
+                nv[1] = T[2][0] * T[0][1] - T[0][0] * T[2][1];
+                nv[2] = T[0][0] * T[1][1] - T[1][0] * T[0][1];
+            }
+            double j = 0;
+            for (int d = 0; d < nd; d++) j += nv[d] * nv[d];
+            j = std::sqrt(j);
+            const int gg = g + ngf * f;
+            G.jacf[gg] = j;
+            for (int d = 0; d < nd; d++) G.nl[gg + na * d] = nv[d] / j;
+        }
+}
+
+// q-equation matrices (elementassembly.cpp:1323-1412 qint):
+//   M = fc_q (phi_j, phi_i), C_d(j,i) = (dphi_j/dx_d, phi_i), E_d(i, fn) = <phi_i, psi_fn n_d>
+static void qmatrices(const oracle_problem& P, const Dims& D, const Geom& G,
+                      std::vector<double>& M, std::vector<double>& C, std::vector<double>& E) {
+    const int nd = D.nd, npv = D.npv, ngv = D.ngv, ngf = D.ngf, nfe = D.nfe, npf = D.npf, ndf = D.ndf;
+    const int npv2 = npv * npv;
+    M.assign(npv2, 0.0);
+    C.assign(npv2 * nd, 0.0);
+    E.assign(npv * ndf * nd, 0.0);
+    for (int r = 0; r < npv2; r++) {
+        double s = 0;
+        for (int g = 0; g < ngv; g++) s += P.shapvgdotshapvl[r + npv2 * g] * G.jac[g];
+        M[r] = P.fc_q * s;
+        for (int d = 0; d < nd; d++) {
+            double c = 0;
+            for (int i = 0; i < nd; i++)
+                for (int g = 0; g < ngv; g++)
+                    c += P.shapvgdotshapvl[r + npv2 * (g + ngv * (i + 1))] * G.Xx[g + ngv * (d + nd * i)];
+            C[r + npv2 * d] = c;
+        }
+    }
+    const int na = ngf * nfe, npf2 = npf * npf;
+    for (int d = 0; d < nd; d++)
+        for (int f = 0; f < nfe; f++)
+            for (int j = 0; j < npf; j++)
+                for (int k = 0; k < npf; k++) {
+                    double s = 0;
+                    for (int g = 0; g < ngf; g++)
+                        s += P.shapfgdotshapfc[(k + npf * j) + npf2 * g] * G.nl[g + ngf * f + na * d] * G.jacf[g + ngf * f];
+                    E[P.perm[f * npf + k] + npv * ((f * npf + j) + ndf * d)] = s;
+                }
+}
+
+struct ElemOut {
+    std::vector<double> Dm, F, K, H, Ru, Rh;
+};
+
+// Element residual and Jacobian blocks before condensation:
+//   elementint (elementassembly.cpp:307-572) + faceint (717-1321), flag_q = 1.
+static void element(const oracle_problem& P, const Dims& D, const double* udg_all, const double* uh_all,
+                    const double* sh_all, int ie, ElemOut& O) {
+    const int nd = D.nd, npv = D.npv, ngv = D.ngv, ngf = D.ngf, nfe = D.nfe, npf = D.npf;
+    const int ncu = D.ncu, nc = D.nc, nch = D.nch, ndf = D.ndf, nd1 = D.nd1, n = D.n, nb = D.nb;
+    const double* udg = udg_all + (size_t)ie * npv * nc;
+    const double* sh = sh_all + (size_t)ie * npv * nc;
+    Geom G;
+    geometry(P, D, ie, G);
+    std::vector<double> M, C, E;
+    qmatrices(P, D, G, M, C, E);
+
+    // ---- volume: u, flux, source at quadrature points
+    std::vector<double> ug(ngv * nc, 0.0), f(ngv * ncu * nd), fu(ngv * ncu * nd * nc);
+    for (int k = 0; k < nc; k++)
+        for (int g = 0; g < ngv; g++) {
+            double s = 0;
+            for (int a = 0; a < npv; a++) s += P.shapvt[g + ngv * a] * udg[a + npv * k];
+            ug[g + ngv * k] = s;
+        }
+    flux_points(nd, P.param, ngv, ug.data(), f.data(), fu.data());
+    std::vector<double> s(ngv * ncu, 0.0), su(ngv * ncu * nc, 0.0);   // NS source is zero
+    if (P.tdep) {                                                      // elementassembly.cpp:293-304
+        for (int j = 0; j < ncu; j++)
+            for (int g = 0; g < ngv; g++) {
+                double t = 0;
+                for (int a = 0; a < npv; a++) t += P.shapvt[g + ngv * a] * sh[a + npv * j];
+                s[g + ngv * j] += t - ug[g + ngv * j] * P.fc_u;
+                su[g + ngv * (j + ncu * j)] -= P.fc_u;
+            }
+    }
+    // Ru(i, j) = sum_g [phi_i s_j jac + sum_m dphi_i/dxi_m sum_d f_jd Xx(d,m)] w_g
+    O.Ru.assign(n, 0.0);
+    for (int j = 0; j < ncu; j++)
+        for (int i = 0; i < npv; i++) {
+            double acc = 0;
+            for (int g = 0; g < ngv; g++) {
+                acc += P.shapvg[i + npv * g] * s[g + ngv * j] * G.jac[g];
+                for (int m = 0; m < nd; m++) {
+                    double fx = 0;
+                    for (int d = 0; d < nd; d++) fx += f[g + ngv * (j + ncu * d)] * G.Xx[g + ngv * (d + nd * m)];
+                    acc += P.shapvg[i + npv * (g + ngv * (m + 1))] * fx;
+                }
+            }
+            O.Ru[i + npv * j] = acc;
+        }
+    // wrl(g, r, j, k) = -[s_u jac ; f_u Xx]   (r = 0 value, r = 1..nd derivative)
+    std::vector<double> wrl(ngv * nd1 * ncu * nc);
+    auto WRL = [&](int g, int r, int j, int k) -> double& { return wrl[g + ngv * (r + nd1 * (j + ncu * k))]; };
+    for (int k = 0; k < nc; k++)
+        for (int j = 0; j < ncu; j++)
+            for (int g = 0; g < ngv; g++) {
+                WRL(g, 0, j, k) = -su[g + ngv * (j + ncu * k)] * G.jac[g];
+                for (int m = 0; m < nd; m++) {
+                    double t = 0;
+                    for (int d = 0; d < nd; d++) t += fu[g + ngv * (j + ncu * (d + nd * k))] * G.Xx[g + ngv * (d + nd * m)];
+                    WRL(g, m + 1, j, k) = -t;
+                }
+            }
+    // q elimination: Cholesky of M, M^-1 C_d, M^-1 E_d (elementassembly.cpp:453-478)
+    std::vector<double> L = M;
+    cholesky(npv, L.data());
+    std::vector<double> MiC = C, MiE = E;
+    chol_solve(npv, L.data(), npv * nd, MiC.data());
+    chol_solve(npv, L.data(), ndf * nd, MiE.data());
+    // dq_d/du_(a,k) at point g = phi-weighted M^-1 C ; dq_d/duh_fn = -phi-weighted M^-1 E
+    std::vector<double> sMiC(ngv * npv * nd), sMiE(ngv * ndf * nd);
+    for (int d = 0; d < nd; d++)
+        for (int g = 0; g < ngv; g++) {
+            for (int a = 0; a < npv; a++) {
+                double t = 0;
+                for (int b = 0; b < npv; b++) t += P.shapvt[g + ngv * b] * MiC[b + npv * (a + npv * d)];
+                sMiC[g + ngv * (a + npv * d)] = t;
+            }
+            for (int fn = 0; fn < ndf; fn++) {
+                double t = 0;
+                for (int b = 0; b < npv; b++) t += P.shapvt[g + ngv * b] * MiE[b + npv * (fn + ndf * d)];
+                sMiE[g + ngv * (fn + ndf * d)] = -t;
+            }
+        }
+    // D(i,j,a,k) = sum_{g,r} shapvg(i,g,r) [wrl(g,r,j,k) phi_a(g) + sum_d wrl(g,r,j,q_dk) sMiC(g,a,d)]
+    // F(i,j,k,fn) = sum_{g,r} shapvg(i,g,r) sum_d wrl(g,r,j,q_dk) sMiE(g,fn,d)
+    O.Dm.assign((size_t)n * n, 0.0);
+    O.F.assign((size_t)n * nb, 0.0);
+    std::vector<double> col(ngv * nd1);
+    for (int k = 0; k < ncu; k++)
+        for (int j = 0; j < ncu; j++) {
+            for (int a = 0; a < npv; a++) {
+                for (int r = 0; r < nd1; r++)
+                    for (int g = 0; g < ngv; g++) {
+                        double t = WRL(g, r, j, k) * P.shapvt[g + ngv * a];
+                        for (int d = 0; d < nd; d++) t += WRL(g, r, j, ncu * (1 + d) + k) * sMiC[g + ngv * (a + npv * d)];
+                        col[g + ngv * r] = t;
+                    }
+                for (int i = 0; i < npv; i++) {
+                    double acc = 0;
+                    for (int q = 0; q < ngv * nd1; q++) acc += P.shapvg[i + npv * q] * col[q];
+                    O.Dm[i + npv * (j + ncu * (a + npv * k))] = acc;
+                }
+            }
+            for (int fn = 0; fn < ndf; fn++) {
+                for (int r = 0; r < nd1; r++)
+                    for (int g = 0; g < ngv; g++) {
+                        double t = 0;
+                        for (int d = 0; d < nd; d++) t += WRL(g, r, j, ncu * (1 + d) + k) * sMiE[g + ngv * (fn + ndf * d)];
+                        col[g + ngv * r] = t;
+                    }
+                for (int i = 0; i < npv; i++) {
+                    double acc = 0;
+                    for (int q = 0; q < ngv * nd1; q++) acc += P.shapvg[i + npv * q] * col[q];
+                    O.F[i + npv * (j + ncu * (k + nch * fn))] = acc;
+                }
+            }
+        }
+
+    // ---- faces: trace flux fhat = F(uh, q).n + tau (u - uh)  (fhatDriver.cpp:54-236)
+    const int na = ngf * nfe;
+    std::vector<double> uhe(ndf * nch);
+    for (int fn = 0; fn < ndf; fn++) {
+        const int gdof = P.elcon[(size_t)ie * ndf + fn];
+        for (int c = 0; c < nch; c++) uhe[fn + ndf * c] = uh_all[(size_t)gdof * nch + c];
+    }
+    std::vector<double> ugf(na * nc), uhg(na * nch);
+    for (int fc = 0; fc < nfe; fc++)
+        for (int g = 0; g < ngf; g++) {
+            for (int c = 0; c < nc; c++) {
+                double t = 0;
+                for (int m = 0; m < npf; m++) t += P.shapft[g + ngf * m] * udg[P.perm[fc * npf + m] + npv * c];
+                ugf[g + ngf * fc + na * c] = t;
+            }
+            for (int c = 0; c < nch; c++) {
+                double t = 0;
+                for (int m = 0; m < npf; m++) t += P.shapft[g + ngf * m] * uhe[fc * npf + m + ndf * c];
+                uhg[g + ngf * fc + na * c] = t;
+            }
+        }
+    std::vector<double> waux(na * nc), fh(na * ncu * nd), fhu(na * ncu * nd * nc);
+    for (int g = 0; g < na; g++) {
+        for (int c = 0; c < ncu; c++) waux[g + na * c] = uhg[g + na * c];
+        for (int c = ncu; c < nc; c++) waux[g + na * c] = ugf[g + na * c];
+    }
+    flux_points(nd, P.param, na, waux.data(), fh.data(), fhu.data());
+    const double tau = P.param[5];
+    // fhn (na x nch), fhn_u (na x nch x nc), fhn_uh (na x nch x nch), all times jacf
+    std::vector<double> fn_(na * nch), fn_u(na * nch * nc, 0.0), fn_uh(na * nch * nch, 0.0);
+    for (int g = 0; g < na; g++) {
+        const double jf = G.jacf[g];
+        for (int j = 0; j < ncu; j++) {
+            double t = tau * (ugf[g + na * j] - uhg[g + na * j]);
+            for (int d = 0; d < nd; d++) t += fh[g + na * (j + ncu * d)] * G.nl[g + na * d];
+            fn_[g + na * j] = t * jf;
+            for (int k = 0; k < nc; k++) {
+                double v = 0;
+                if (k >= ncu)
+                    for (int d = 0; d < nd; d++) v += fhu[g + na * (j + ncu * (d + nd * k))] * G.nl[g + na * d];
+                if (k == j) v += tau;
+                fn_u[g + na * (j + nch * k)] = v * jf;
+            }
+            for (int k = 0; k < nch; k++) {
+                double v = 0;
+                for (int d = 0; d < nd; d++) v += fhu[g + na * (j + ncu * (d + nd * k))] * G.nl[g + na * d];
+                if (k == j) v -= tau;
+                fn_uh[g + na * (j + nch * k)] = v * jf;
+            }
+        }
+    }
+    // face residual Rutmp(m, fc, j) = sum_g psi_m w fhn
+    O.Rh.assign(nb, 0.0);
+    for (int fc = 0; fc < nfe; fc++)
+        for (int j = 0; j < nch; j++)
+            for (int m = 0; m < npf; m++) {
+                double t = 0;
+                for (int g = 0; g < ngf; g++) t += P.shapfg[m + npf * g] * fn_[g + ngf * fc + na * j];
+                O.Ru[P.perm[fc * npf + m] + npv * j] -= t;                       // faceint 853-855
+                O.Rh[j + nch * (fc * npf + m)] = -t;                              // faceint 1248-1251
+            }
+    // face mass-weighted Jacobians: BDtmp (wrt u), Ftmp (wrt uh)
+    O.K.assign((size_t)nb * n, 0.0);
+    O.H.assign((size_t)nb * nb, 0.0);
+    const int npf2 = npf * npf;
+    for (int fc = 0; fc < nfe; fc++)
+        for (int kk = 0; kk < npf; kk++)          // trial node
+            for (int ks = 0; ks < npf; ks++) {    // test node
+                const int row_e = P.perm[fc * npf + ks], col_e = P.perm[fc * npf + kk];
+                for (int j = 0; j < nch; j++) {
+                    for (int m = 0; m < ncu; m++) {
+                        double t = 0;
+                        for (int g = 0; g < ngf; g++)
+                            t += P.shapfgdotshapfc[(ks + npf * kk) + npf2 * g] * fn_u[g + ngf * fc + na * (j + nch * m)];
+                        O.Dm[row_e + npv * (j + ncu * (col_e + npv * m))] += t;                     // faceint 909-917
+                        O.K[j + nch * (fc * npf + ks) + nb * (col_e + npv * m)] = t;                 // faceint 1254-1277
+                    }
+                    for (int m = 0; m < nch; m++) {
+                        double t = 0;
+                        for (int g = 0; g < ngf; g++)
+                            t += P.shapfgdotshapfc[(ks + npf * kk) + npf2 * g] * fn_uh[g + ngf * fc + na * (j + nch * m)];
+                        O.F[row_e + npv * (j + ncu * (m + nch * (fc * npf + kk)))] += t;          // faceint 897-905
+                        O.H[j + nch * (fc * npf + ks) + nb * (m + nch * (fc * npf + kk))] = t;       // faceint 1281-1296
+                    }
+                }
+            }
+    // q-elimination face terms (faceint 927-1072, 1299-1320):
+    //   Df(fn, j, a, k) = sum_g psi_fn w sum_d fhn_u(j, q_dk) phi-face(M^-1 C_d)(a)
+    //   Ff(fn, j, k, fn2) = same with (+M^-1 E_d), subtracted from F and H
+    std::vector<double> sMiCf(na * npv * nd), sMiEf(na * ndf * nd);
+    for (int d = 0; d < nd; d++)
+        for (int fc = 0; fc < nfe; fc++)
+            for (int g = 0; g < ngf; g++) {
+                for (int a = 0; a < npv; a++) {
+                    double t = 0;
+                    for (int m = 0; m < npf; m++) t += P.shapft[g + ngf * m] * MiC[P.perm[fc * npf + m] + npv * (a + npv * d)];
+                    sMiCf[g + ngf * fc + na * (a + npv * d)] = t;
+                }
+                for (int fn = 0; fn < ndf; fn++) {
+                    double t = 0;
+                    for (int m = 0; m < npf; m++) t += P.shapft[g + ngf * m] * MiE[P.perm[fc * npf + m] + npv * (fn + ndf * d)];
+                    sMiEf[g + ngf * fc + na * (fn + ndf * d)] = t;     // + M^-1 E here; F and H subtract
+                }
+            }
+    for (int fc = 0; fc < nfe; fc++)
+        for (int ip = 0; ip < npf; ip++) {
+            const int fdof = fc * npf + ip, row_e = P.perm[fc * npf + ip];
+            for (int k = 0; k < ncu; k++)
+                for (int j = 0; j < ncu; j++) {
+                    for (int a = 0; a < npv; a++) {
+                        double t = 0;
+                        for (int g = 0; g < ngf; g++) {
+                            double v = 0;
+                            for (int d = 0; d < nd; d++)
+                                v += fn_u[g + ngf * fc + na * (j + nch * (ncu * (1 + d) + k))] * sMiCf[g + ngf * fc + na * (a + npv * d)];
+                            t += P.shapfg[ip + npf * g] * v;
+                        }
+                        O.Dm[row_e + npv * (j + ncu * (a + npv * k))] += t;
+                        O.K[j + nch * fdof + nb * (a + npv * k)] += t;
+                    }
+                    for (int fn2 = 0; fn2 < ndf; fn2++) {
+                        double t = 0;
+                        for (int g = 0; g < ngf; g++) {
+                            double v = 0;
+                            for (int d = 0; d < nd; d++)
+                                v += fn_u[g + ngf * fc + na * (j + nch * (ncu * (1 + d) + k))] * sMiEf[g + ngf * fc + na * (fn2 + ndf * d)];
+                            t += P.shapfg[ip + npf * g] * v;
+                        }
+                        O.F[row_e + npv * (j + ncu * (k + nch * fn2))] -= t;
+                        O.H[j + nch * fdof + nb * (k + nch * fn2)] -= t;
+                    }
+                }
+        }
+}
+
+// q from (u, uh): q_d = M^-1 (M sh_q + C_d u - E_d uh)  (elementassembly.cpp:1414-1479 getQ)
+static void getq_element(const oracle_problem& P, const Dims& D, double* udg_all, const double* uh_all,
+                         const double* sh_all, int ie) {
+    const int nd = D.nd, npv = D.npv, ncu = D.ncu, nc = D.nc, nch = D.nch, ndf = D.ndf;
+    Geom G;
+    geometry(P, D, ie, G);
+    std::vector<double> M, C, E;
+    qmatrices(P, D, G, M, C, E);
+    double* u = udg_all + (size_t)ie * npv * nc;
+    const double* sh = sh_all + (size_t)ie * npv * nc;
+    std::vector<double> q(npv * ncu * nd);
+    for (int d = 0; d < nd; d++)
+        for (int c = 0; c < ncu; c++)
+            for (int i = 0; i < npv; i++) {
+                double t = 0;
+                for (int a = 0; a < npv; a++) t += M[i + npv * a] * sh[a + npv * (ncu * (1 + d) + c)];
+                for (int a = 0; a < npv; a++) t += C[i + npv * (a + npv * d)] * u[a + npv * c];
+                for (int fn = 0; fn < ndf; fn++)
+                    t -= E[i + npv * (fn + ndf * d)] * uh_all[(size_t)P.elcon[(size_t)ie * ndf + fn] * nch + c];
+                q[i + npv * (c + ncu * d)] = t;
+            }
+    cholesky(npv, M.data());
+    chol_solve(npv, M.data(), ncu * nd, q.data());
+    for (int d = 0; d < nd; d++)
+        for (int c = 0; c < ncu; c++)
+            for (int i = 0; i < npv; i++) u[i + npv * (ncu * (1 + d) + c)] = q[i + npv * (c + ncu * d)];
+}
+
+// Static condensation (elementschur.cpp:6-329): D = LU, F <- D^-1 F, H <- H - K D^-1 F,
+// Ru <- D^-1 Ru, Rh <- Rh - K D^-1 Ru.
+static int schur(const Dims& D, ElemOut& O) {
+    const int n = D.n, nb = D.nb;
+    std::vector<int> piv(n);
+    int info = lu_factor(n, O.Dm.data(), piv.data());
+    if (info) return info;
+    lu_solve(n, O.Dm.data(), piv.data(), nb, O.F.data());
+    lu_solve(n, O.Dm.data(), piv.data(), 1, O.Ru.data());
+    for (int c = 0; c < nb; c++)
+        for (int k = 0; k < n; k++) {
+            const double f = O.F[k + (size_t)n * c];
+            if (f != 0.0) for (int r = 0; r < nb; r++) O.H[r + (size_t)nb * c] -= O.K[r + (size_t)nb * k] * f;
+        }
+    for (int k = 0; k < n; k++) {
+        const double f = O.Ru[k];
+        for (int r = 0; r < nb; r++) O.Rh[r] -= O.K[r + (size_t)nb * k] * f;
+    }
+    return 0;
+}
+
+static int find_block(const oracle_problem& P, int i, int j) {
+    for (int k = P.rowstart[i]; k < P.rowstart[i + 1]; k++) if (P.colidx[k] == j) return k;
+    return -1;
+}
+
+// Scatter into the face-block system (globalassembly.cpp:40-89, HDG branch)
+static int scatter(const oracle_problem& P, const Dims& D, int ie, const double* He, const double* Re, const double* Ro,
+                   double* Hg, double* Rg, double* Rr) {
+    const int nfe = D.nfe, npf = D.npf, nch = D.nch, bsz = D.bsz, nb = D.nb, ndf = D.ndf;
+    const int* elc = P.elcon + (size_t)ie * ndf;
+    for (int a = 0; a < nfe; a++) {
+        const int i = P.t2f[(size_t)ie * nfe + a];
+        for (int m1 = 0; m1 < npf; m1++) {
+            const int ind = elc[a * npf + m1] - i * npf;
+            for (int c = 0; c < nch; c++) {
+                if (Rg) Rg[(size_t)i * bsz + m1 * nch + c] += Re[a * bsz + ind * nch + c];
+                if (Rr) Rr[(size_t)i * bsz + m1 * nch + c] += Ro[a * bsz + ind * nch + c];
+            }
+        }
+        if (!Hg) continue;
+        for (int b = 0; b < nfe; b++) {
+            const int j = P.t2f[(size_t)ie * nfe + b];
+            const int k = find_block(P, i, j);
+            if (k < 0) return -1;
+            for (int m1 = 0; m1 < npf; m1++) {
+                const int jnd = elc[b * npf + m1] - j * npf;
+                for (int n1 = 0; n1 < nch; n1++)
+                    for (int m2 = 0; m2 < npf; m2++) {
+                        const int ind = elc[a * npf + m2] - i * npf;
+                        for (int n2 = 0; n2 < nch; n2++)
+                            Hg[(size_t)k * bsz * bsz + (m1 * nch + n1) * bsz + m2 * nch + n2] +=
+                                He[(a * bsz + ind * nch + n2) + (size_t)nb * (b * bsz + jnd * nch + n1)];
+                    }
+            }
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Per-element blocks before condensation (D, F, K, H, Ru, Rh), for parity tests.
+int oracle_element(const oracle_problem* P, const double* udg, const double* uh, const double* sh, int ie,
+                   double* Dm, double* F, double* K, double* H, double* Ru, double* Rh) {
+    Dims D(*P);
+    ElemOut O;
+    element(*P, D, udg, uh, sh, ie, O);
+    std::memcpy(Dm, O.Dm.data(), sizeof(double) * O.Dm.size());
+    std::memcpy(F, O.F.data(), sizeof(double) * O.F.size());
+    std::memcpy(K, O.K.data(), sizeof(double) * O.K.size());
+    std::memcpy(H, O.H.data(), sizeof(double) * O.H.size());
+    std::memcpy(Ru, O.Ru.data(), sizeof(double) * O.Ru.size());
+    std::memcpy(Rh, O.Rh.data(), sizeof(double) * O.Rh.size());
+    return 0;
+}
+
+int oracle_getq(const oracle_problem* P, double* udg, const double* uh, const double* sh) {
+    Dims D(*P);
+    for (int ie = 0; ie < P->ne; ie++) getq_element(*P, D, udg, uh, sh, ie);
+    return 0;
+}
+
+// assembleLinearSystem (globalassembly.cpp:423-556).  Any output pointer may be NULL.
+// elem_H / elem_Rh (optional) receive the condensed per-element blocks.
+int oracle_assemble(const oracle_problem* P, const double* udg, const double* uh, const double* sh,
+                    double* Hg, double* Rg, double* Rr, double* DinvRu, double* DinvF, double* rnorm,
+                    double* elem_H, double* elem_Rh, int e0, int e1) {
+    Dims D(*P);
+    const size_t nblk = (size_t)P->rowstart[P->nf];
+    if (e0 < 0) e0 = 0;
+    if (e1 < 0 || e1 > P->ne) e1 = P->ne;
+    if (Hg) std::memset(Hg, 0, sizeof(double) * nblk * D.bsz * D.bsz);
+    if (Rg) std::memset(Rg, 0, sizeof(double) * (size_t)P->nf * D.bsz);
+    std::vector<double> r((size_t)P->nf * D.bsz, 0.0);
+    double ru2 = 0.0;
+    ElemOut O;
+    for (int ie = e0; ie < e1; ie++) {
+        element(*P, D, udg, uh, sh, ie, O);
+        for (double v : O.Ru) ru2 += v * v;
+        std::vector<double> Ro = O.Rh;
+        if (schur(D, O)) return 1000 + ie;
+        if (DinvRu) std::memcpy(DinvRu + (size_t)ie * D.n, O.Ru.data(), sizeof(double) * D.n);
+        if (DinvF) std::memcpy(DinvF + (size_t)ie * D.n * D.nb, O.F.data(), sizeof(double) * D.n * D.nb);
+        if (elem_H) std::memcpy(elem_H + (size_t)(ie - e0) * D.nb * D.nb, O.H.data(), sizeof(double) * D.nb * D.nb);
+        if (elem_Rh) std::memcpy(elem_Rh + (size_t)(ie - e0) * D.nb, O.Rh.data(), sizeof(double) * D.nb);
+        if (scatter(*P, D, ie, O.H.data(), O.Rh.data(), Ro.data(), Hg, Rg, r.data())) return 2;
+    }
+    double rr = 0.0;
+    for (double v : r) rr += v * v;
+    if (Rr) std::memcpy(Rr, r.data(), sizeof(double) * r.size());
+    if (rnorm) *rnorm = std::sqrt(ru2 + rr);
+    return 0;
+}
+
+// computeResidualNorm (globalassembly.cpp:618-678): element residuals only.
+int oracle_residual(const oracle_problem* P, const double* udg, const double* uh, const double* sh, double* rnorm) {
+    Dims D(*P);
+    std::vector<double> r((size_t)P->nf * D.bsz, 0.0);
+    double ru2 = 0.0;
+    ElemOut O;
+    for (int ie = 0; ie < P->ne; ie++) {
+        element(*P, D, udg, uh, sh, ie, O);
+        for (double v : O.Ru) ru2 += v * v;
+        scatter(*P, D, ie, nullptr, O.Rh.data(), O.Rh.data(), nullptr, nullptr, r.data());
+    }
+    double rr = 0.0;
+    for (double v : r) rr += v * v;
+    *rnorm = std::sqrt(ru2 + rr);
+    return 0;
+}
+
+// updateSol (solutionupdate.cpp:70-98): uh += alpha duh; u += alpha (DinvRu - DinvF duh_e); q from getQ.
+int oracle_update(const oracle_problem* P, double* udg, double* uh, const double* sh, const double* DinvRu,
+                  const double* DinvF, const double* duh, double alpha) {
+    Dims D(*P);
+    const size_t nuh = (size_t)P->nf * D.bsz;
+    for (size_t i = 0; i < nuh; i++) uh[i] += alpha * duh[i];
+    std::vector<double> de(D.nb);
+    for (int ie = 0; ie < P->ne; ie++) {
+        for (int fn = 0; fn < D.ndf; fn++)
+            for (int c = 0; c < D.nch; c++) de[fn * D.nch + c] = duh[(size_t)P->elcon[(size_t)ie * D.ndf + fn] * D.nch + c];
+        double* u = udg + (size_t)ie * D.npv * D.nc;
+        const double* df = DinvF + (size_t)ie * D.n * D.nb;
+        for (int r = 0; r < D.n; r++) {
+            double t = 0;
+            for (int c = 0; c < D.nb; c++) t += df[r + (size_t)D.n * c] * de[c];
+            u[r] += -alpha * t;
+        }
+        for (int r = 0; r < D.n; r++) u[r] += alpha * DinvRu[(size_t)ie * D.n + r];
+        getq_element(*P, D, udg, uh, sh, ie);
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- GMRES
+// Block-Jacobi preconditioner (kernel/mkBlockJacobi.m:1-16): inverse of each row's
+// diagonal block (the first block of the row).
+int oracle_bj_inverse(int nrows, int bsz, const int* rowstart, const double* Hg, double* Minv) {
+    std::vector<double> a(bsz * bsz);
+    std::vector<int> piv(bsz);
+    for (int i = 0; i < nrows; i++) {
+        std::memcpy(a.data(), Hg + (size_t)rowstart[i] * bsz * bsz, sizeof(double) * bsz * bsz);
+        if (lu_factor(bsz, a.data(), piv.data())) return 1 + i;
+        double* out = Minv + (size_t)i * bsz * bsz;
+        for (int c = 0; c < bsz; c++) for (int r = 0; r < bsz; r++) out[r + bsz * c] = (r == c) ? 1.0 : 0.0;
+        lu_solve(bsz, a.data(), piv.data(), bsz, out);
+    }
+    return 0;
+}
+
+static void bsr_matvec(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                       const double* x, double* y) {   // kernel/matvec.m:1-12
+    for (int i = 0; i < nrows; i++) {
+        double* yi = y + (size_t)i * bsz;
+        for (int r = 0; r < bsz; r++) yi[r] = 0.0;
+        for (int k = rowstart[i]; k < rowstart[i + 1]; k++) {
+            const double* blk = Hg + (size_t)k * bsz * bsz;
+            const double* xj = x + (size_t)colidx[k] * bsz;
+            for (int c = 0; c < bsz; c++) {
+                const double xv = xj[c];
+                for (int r = 0; r < bsz; r++) yi[r] += blk[r + bsz * c] * xv;
+            }
+        }
+    }
+}
+
+static void bj_apply(int nrows, int bsz, const double* Minv, const double* x, double* y) {
+    for (int i = 0; i < nrows; i++) {
+        const double* m = Minv + (size_t)i * bsz * bsz;
+        for (int r = 0; r < bsz; r++) {
+            double t = 0;
+            for (int c = 0; c < bsz; c++) t += m[r + bsz * c] * x[(size_t)i * bsz + c];
+            y[(size_t)i * bsz + r] = t;
+        }
+    }
+}
+
+// Restarted GMRES, left block-Jacobi preconditioning, modified Gram-Schmidt,
+// Givens least squares; follows kernel/gmres_bilu0.m:17-105 with the BJ apply of
+// mkBlockJacobi.m (Minv == NULL: no preconditioner).  x holds the initial guess
+// on entry.  hist[it] = relative preconditioned residual after Arnoldi step it.
+int oracle_gmres(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                 const double* Minv, const double* b, double* x, int restart, double tol, int maxit,
+                 int* iters, double* hist, int hist_len) {
+    const size_t N = (size_t)nrows * bsz;
+    std::vector<double> V(N * (restart + 1)), w(N), t(N), pb(N);
+    std::vector<double> h((size_t)(restart + 1) * restart), cs(restart), sn(restart), g(restart + 1), y(restart);
+    auto prec = [&](const double* in, double* out) {
+        if (Minv) bj_apply(nrows, bsz, Minv, in, out); else std::memcpy(out, in, sizeof(double) * N);
+    };
+    prec(b, pb.data());
+    double nrmb = 0;
+    for (size_t i = 0; i < N; i++) nrmb += pb[i] * pb[i];
+    nrmb = std::sqrt(nrmb);
+    if (nrmb == 0.0) nrmb = 1.0;
+    int it = 0, flag = -2;
+    while (flag == -2) {
+        bsr_matvec(nrows, bsz, rowstart, colidx, Hg, x, t.data());
+        prec(t.data(), w.data());
+        double beta = 0;
+        for (size_t i = 0; i < N; i++) { w[i] = pb[i] - w[i]; beta += w[i] * w[i]; }
+        beta = std::sqrt(beta);
+        if (beta / nrmb <= tol) { flag = 0; break; }
+        for (size_t i = 0; i < N; i++) V[i] = w[i] / beta;
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        for (; j < restart; j++) {
+            bsr_matvec(nrows, bsz, rowstart, colidx, Hg, &V[N * j], t.data());
+            double* vn = &V[N * (j + 1)];
+            prec(t.data(), vn);
+            for (int i = 0; i <= j; i++) {
+                const double* vi = &V[N * i];
+                double s = 0;
+                for (size_t k = 0; k < N; k++) s += vi[k] * vn[k];
+                h[i + (restart + 1) * j] = s;
+                for (size_t k = 0; k < N; k++) vn[k] -= s * vi[k];
+            }
+            double nn = 0;
+            for (size_t k = 0; k < N; k++) nn += vn[k] * vn[k];
+            nn = std::sqrt(nn);
+            h[j + 1 + (restart + 1) * j] = nn;
+            if (nn != 0.0) for (size_t k = 0; k < N; k++) vn[k] /= nn;
+            for (int i = 0; i < j; i++) {
+                double a = h[i + (restart + 1) * j], bb = h[i + 1 + (restart + 1) * j];
+                h[i + (restart + 1) * j] = cs[i] * a + sn[i] * bb;
+                h[i + 1 + (restart + 1) * j] = -sn[i] * a + cs[i] * bb;
+            }
+            double a = h[j + (restart + 1) * j], bb = h[j + 1 + (restart + 1) * j];
+            double rr = std::sqrt(a * a + bb * bb);
+            cs[j] = a / rr; sn[j] = bb / rr;
+            h[j + (restart + 1) * j] = rr;
+            h[j + 1 + (restart + 1) * j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            const double res = std::fabs(g[j + 1]);
+            if (hist && it < hist_len) hist[it] = res / nrmb;
+            it++;
+            if (res / nrmb <= tol) { flag = 0; j++; break; }
+            if (it >= maxit) { flag = 1; j++; break; }
+            if (nn == 0.0) { flag = -1; j++; break; }
+        }
+        for (int i = j - 1; i >= 0; i--) {
+            double s = g[i];
+            for (int k = i + 1; k < j; k++) s -= h[i + (restart + 1) * k] * y[k];
+            y[i] = s / h[i + (restart + 1) * i];
+        }
+        for (int i = 0; i < j; i++)
+            for (size_t k = 0; k < N; k++) x[k] += V[N * i + k] * y[i];
+    }
+    if (iters) *iters = it;
+    return flag;
+}
+
+}  // extern "C"
