@@ -1,0 +1,868 @@
+// HDG element kernels for sm_100a: local assembly, static condensation,
+// face-block scatter, q recovery and solution update.
+//
+// One CTA owns one element at a time (persistent grid, elements strided by
+// gridDim.x).  Small per-element data live in shared memory; the larger
+// per-element intermediates live in a per-CTA global workspace slot that stays
+// L2-resident while the CTA works on the element.  Outputs are written exactly
+// once per entry; no atomics, so results are bit-reproducible run to run.
+//
+// Structure of the element blocks (restating elementassembly.cpp faceint
+// 717-1321): every face contribution to the element equations is the
+// trace-equation entry lifted to the element node that carries the face dof,
+//   D = D_vol + P K,   F = F_vol + P H,   Ru = Ru_vol + P Rh,
+// where P (npv x ndf) is the incidence perm[fdof] = node.  So K, H, Rh are
+// computed first and D, F, Ru gather them.
+#pragma once
+#include <cuda_runtime.h>
+#include "ns_flux.cuh"
+
+namespace hfem {
+
+template <int ND_, int NPV_, int NPF_, int NGV_, int NGF_>
+struct Shape {
+    static constexpr int ND = ND_, NPV = NPV_, NPF = NPF_, NGV = NGV_, NGF = NGF_;
+    static constexpr int NFE = ND + 1, NCU = ND + 2, NC = NCU * (ND + 1), NCH = NCU;
+    static constexpr int NDF = NPF * NFE, ND1 = ND + 1, N = NPV * NCU, NB = NCH * NDF, BSZ = NCH * NPF;
+    static constexpr int NA = NGF * NFE;          // face points of one element
+    static constexpr int NQ = NGV * ND1;          // (volume point, derivative) pairs
+    static constexpr int MAXINC = ND;             // faces meeting at a node
+    // per-CTA global workspace (doubles)
+    static constexpr int W_WRL = NQ * NCU * NC;
+    static constexpr int W_SMIC = NGV * NPV * ND;
+    static constexpr int W_SMIE = NGV * NDF * ND;
+    static constexpr int W_SMICF = NA * NPV * ND;
+    static constexpr int W_SMIEF = NA * NDF * ND;
+    static constexpr int W_FNU = NA * NCH * NC;
+    static constexpr int W_FNUH = NA * NCH * NCH;
+    static constexpr int WS = W_WRL + W_SMIC + W_SMIE + W_SMICF + W_SMIEF + W_FNU + W_FNUH;
+};
+
+struct Tables {                 // master element tables, reference layouts
+    const double *shapvt, *shapvg, *svsv, *shapft, *shapfg, *sfsf;
+    const int* perm;            // nfe x npf
+};
+
+struct ElemArgs {
+    Tables T;
+    const double* dgnodes;      // ne x nd x npv
+    const int* elcon;           // ne x ndf
+    const double *udg, *uh, *sh;
+    double param[6];
+    int tdep;
+    double fc_u, fc_q;
+    int ne;
+    double *D, *F, *K, *H, *Ru, *Rh, *Ro, *ru2;
+    double* ws;                 // gridDim.x slots of Shape::WS doubles
+};
+
+constexpr int NT = 256;         // threads per CTA for element kernels
+
+// --------------------------------------------------------------- helpers
+__device__ __forceinline__ double block_sum(double v, double* red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += red[i];
+    return s;                   // valid on thread 0
+}
+
+// Geometry at volume and face points (elementassembly.cpp:11-237).
+template <class S>
+__device__ void geometry(const Tables& T, const double* x, double* jac, double* Xx, double* jacf, double* nl) {
+    constexpr int ND = S::ND, NPV = S::NPV, NGV = S::NGV, NGF = S::NGF, NPF = S::NPF, NA = S::NA;
+    for (int g = threadIdx.x; g < NGV + NA; g += blockDim.x) {
+        if (g < NGV) {
+            double J[ND][ND];
+#pragma unroll
+            for (int d = 0; d < ND; d++)
+#pragma unroll
+                for (int i = 0; i < ND; i++) {
+                    double s = 0.0;
+                    for (int a = 0; a < NPV; a++) s += T.shapvt[g + NGV * (a + NPV * (i + 1))] * x[a + NPV * d];
+                    J[d][i] = s;
+                }
+            double adj[ND][ND], det;
+            if constexpr (ND == 2) {
+                det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+                adj[0][0] = J[1][1]; adj[0][1] = -J[0][1];
+                adj[1][0] = -J[1][0]; adj[1][1] = J[0][0];
+            } else {
+                adj[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+                adj[0][1] = J[0][2] * J[2][1] - J[0][1] * J[2][2];
+                adj[0][2] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+                adj[1][0] = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+                adj[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+                adj[1][2] = J[0][2] * J[1][0] - J[0][0] * J[1][2];
+                adj[2][0] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+                adj[2][1] = J[0][1] * J[2][0] - J[0][0] * J[2][1];
+                adj[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+                det = J[0][0] * adj[0][0] + J[0][1] * adj[1][0] + J[0][2] * adj[2][0];
+            }
+            jac[g] = det;
+#pragma unroll
+            for (int d = 0; d < ND; d++)
+#pragma unroll
+                for (int i = 0; i < ND; i++) Xx[g + NGV * (d + ND * i)] = adj[i][d];
+        } else {
+            const int gg = g - NGV, fc = gg / NGF, q = gg % NGF;
+            double Tt[ND][ND - 1];
+#pragma unroll
+            for (int d = 0; d < ND; d++)
+#pragma unroll
+                for (int r = 0; r < ND - 1; r++) {
+                    double s = 0.0;
+                    for (int m = 0; m < NPF; m++)
+                        s += T.shapft[q + NGF * (m + NPF * (r + 1))] * x[T.perm[fc * NPF + m] + NPV * d];
+                    Tt[d][r] = s;
+                }
+            double nv[ND];
+            if constexpr (ND == 2) {
+                nv[0] = Tt[1][0];
+                nv[1] = -Tt[0][0];
+            } else {
+                nv[0] = Tt[1][0] * Tt[2][1] - Tt[2][0] * Tt[1][1];
+                nv[1] = Tt[2][0] * Tt[0][1] - Tt[0][0] * Tt[2][1];
+                nv[2] = Tt[0][0] * Tt[1][1] - Tt[1][0] * Tt[0][1];
+            }
+            double j = 0.0;
+#pragma unroll
+            for (int d = 0; d < ND; d++) j += nv[d] * nv[d];
+            j = sqrt(j);
+            jacf[gg] = j;
+#pragma unroll
+            for (int d = 0; d < ND; d++) nl[gg + NA * d] = nv[d] / j;
+        }
+    }
+}
+
+// q-equation matrices (elementassembly.cpp:1323-1412): M (npv^2), C (npv^2 nd), E (npv ndf nd).
+template <class S>
+__device__ void qmatrices(const Tables& T, double fc_q, const double* jac, const double* Xx, const double* jacf,
+                          const double* nl, double* M, double* C, double* E) {
+    constexpr int ND = S::ND, NPV = S::NPV, NGV = S::NGV, NGF = S::NGF, NPF = S::NPF, NA = S::NA, NDF = S::NDF;
+    constexpr int NPV2 = NPV * NPV, NPF2 = NPF * NPF;
+    for (int t = threadIdx.x; t < NPV2 * (ND + 1); t += blockDim.x) {
+        const int r = t % NPV2, d = t / NPV2;
+        if (d == 0) {
+            double s = 0.0;
+            for (int g = 0; g < NGV; g++) s += T.svsv[r + NPV2 * g] * jac[g];
+            M[r] = fc_q * s;
+        } else {
+            double c = 0.0;
+            for (int i = 0; i < ND; i++)
+                for (int g = 0; g < NGV; g++)
+                    c += T.svsv[r + NPV2 * (g + NGV * (i + 1))] * Xx[g + NGV * ((d - 1) + ND * i)];
+            C[r + NPV2 * (d - 1)] = c;
+        }
+    }
+    for (int t = threadIdx.x; t < NPV * NDF * ND; t += blockDim.x) E[t] = 0.0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < ND * NDF * NPF; t += blockDim.x) {
+        const int k = t % NPF, j = (t / NPF) % NPF, fc = (t / NPF2) % S::NFE, d = t / (NPF2 * S::NFE);
+        double s = 0.0;
+        for (int g = 0; g < NGF; g++)
+            s += T.sfsf[(k + NPF * j) + NPF2 * g] * nl[g + NGF * fc + NA * d] * jacf[g + NGF * fc];
+        E[T.perm[fc * NPF + k] + NPV * ((fc * NPF + j) + NDF * d)] = s;
+    }
+}
+
+// Lower Cholesky of M (npv x npv) in place, one warp.
+template <int NPV>
+__device__ void cholesky_warp(double* a) {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    for (int j = 0; j < NPV; j++) {
+        if (lane == 0) {
+            double s = a[j + NPV * j];
+            for (int k = 0; k < j; k++) s -= a[j + NPV * k] * a[j + NPV * k];
+            a[j + NPV * j] = sqrt(s);
+        }
+        __syncwarp();
+        const double djj = a[j + NPV * j];
+        for (int i = j + 1 + lane; i < NPV; i += 32) {
+            double t = a[i + NPV * j];
+            for (int k = 0; k < j; k++) t -= a[i + NPV * k] * a[j + NPV * k];
+            a[i + NPV * j] = t / djj;
+        }
+        __syncwarp();
+    }
+}
+
+template <int NPV>
+__device__ __forceinline__ void chol_solve_col(const double* l, double* x) {
+    for (int i = 0; i < NPV; i++) {
+        double t = x[i];
+        for (int k = 0; k < i; k++) t -= l[i + NPV * k] * x[k];
+        x[i] = t / l[i + NPV * i];
+    }
+    for (int i = NPV - 1; i >= 0; i--) {
+        double t = x[i];
+        for (int k = i + 1; k < NPV; k++) t -= l[k + NPV * i] * x[k];
+        x[i] = t / l[i + NPV * i];
+    }
+}
+
+// ------------------------------------------------------------ element kernel
+template <class S>
+struct ElemSmem {
+    double x[S::NPV * S::ND];
+    double u[S::NPV * S::NC];
+    double uhe[S::NDF * S::NCH];
+    double shu[S::NPV * S::NCU];
+    double jac[S::NGV], Xx[S::NGV * S::ND * S::ND];
+    double jacf[S::NA], nl[S::NA * S::ND];
+    double M[S::NPV * S::NPV];
+    double C[S::NPV * S::NPV * S::ND];
+    double E[S::NPV * S::NDF * S::ND];
+    double ug[S::NGV * S::NC];
+    double ugf[S::NA * S::NC];
+    double uhg[S::NA * S::NCH];
+    double wrk[S::NQ * S::NCU];
+    double fn[S::NA * S::NCH];
+    double shapvg[S::NPV * S::NQ];
+    double red[NT / 32];
+    int perm[S::NDF];
+    int inc_n[S::NPV];
+    int inc_f[S::NPV * S::MAXINC];
+};
+
+template <class S>
+__global__ void __launch_bounds__(NT) element_kernel(ElemArgs A) {
+    constexpr int ND = S::ND, NPV = S::NPV, NPF = S::NPF, NGV = S::NGV, NGF = S::NGF, NFE = S::NFE;
+    constexpr int NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, ND1 = S::ND1, N = S::N, NB = S::NB;
+    constexpr int NA = S::NA, NQ = S::NQ, NPF2 = NPF * NPF;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ElemSmem<S>& sm = *reinterpret_cast<ElemSmem<S>*>(smem_raw);
+    const Tables& T = A.T;
+    const int tid = threadIdx.x;
+
+    double* ws = A.ws + (size_t)blockIdx.x * S::WS;
+    double* wrl = ws;                               // [g + NGV*(r + ND1*(j + NCU*k))]
+    double* sMiC = wrl + S::W_WRL;                  // [g + NGV*(a + NPV*d)]
+    double* sMiE = sMiC + S::W_SMIC;                // [g + NGV*(fn + NDF*d)]  (carries the minus sign)
+    double* sMiCf = sMiE + S::W_SMIE;               // [g' + NA*(a + NPV*d)]
+    double* sMiEf = sMiCf + S::W_SMICF;             // [g' + NA*(fn + NDF*d)]
+    double* fnu = sMiEf + S::W_SMIEF;               // [g' + NA*(j + NCH*k)]
+    double* fnuh = fnu + S::W_FNU;                  // [g' + NA*(j + NCH*k)]
+
+    // master tables that every element reuses
+    for (int t = tid; t < NPV * NQ; t += NT) sm.shapvg[t] = T.shapvg[t];
+    for (int t = tid; t < NDF; t += NT) sm.perm[t] = T.perm[t];
+    __syncthreads();
+    for (int i = tid; i < NPV; i += NT) {           // node -> incident face dofs, ascending
+        int c = 0;
+        for (int f = 0; f < NDF; f++)
+            if (sm.perm[f] == i && c < S::MAXINC) sm.inc_f[i * S::MAXINC + c++] = f;
+        sm.inc_n[i] = c;
+    }
+
+    for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
+        __syncthreads();
+        // ---- gather element data
+        const double* xg = A.dgnodes + (size_t)e * NPV * ND;
+        const double* ugl = A.udg + (size_t)e * NPV * NC;
+        const double* shg = A.sh + (size_t)e * NPV * NC;
+        for (int t = tid; t < NPV * ND; t += NT) sm.x[t] = xg[t];
+        for (int t = tid; t < NPV * NC; t += NT) sm.u[t] = ugl[t];
+        for (int t = tid; t < NPV * NCU; t += NT) sm.shu[t] = shg[t];
+        for (int t = tid; t < NDF * NCH; t += NT) {
+            const int fn = t / NCH, c = t % NCH;
+            sm.uhe[fn + NDF * c] = A.uh[(size_t)A.elcon[(size_t)e * NDF + fn] * NCH + c];
+        }
+        __syncthreads();
+        geometry<S>(T, sm.x, sm.jac, sm.Xx, sm.jacf, sm.nl);
+        __syncthreads();
+        qmatrices<S>(T, A.fc_q, sm.jac, sm.Xx, sm.jacf, sm.nl, sm.M, sm.C, sm.E);
+        // solution at volume / face points
+        for (int t = tid; t < NGV * NC; t += NT) {
+            const int g = t % NGV, c = t / NGV;
+            double s = 0.0;
+            for (int a = 0; a < NPV; a++) s += T.shapvt[g + NGV * a] * sm.u[a + NPV * c];
+            sm.ug[t] = s;
+        }
+        for (int t = tid; t < NA * (NC + NCH); t += NT) {
+            const int gg = t % NA, c = t / NA, fc = gg / NGF, q = gg % NGF;
+            double s = 0.0;
+            if (c < NC) {
+                for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.u[sm.perm[fc * NPF + m] + NPV * c];
+                sm.ugf[gg + NA * c] = s;
+            } else {
+                for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.uhe[fc * NPF + m + NDF * (c - NC)];
+                sm.uhg[gg + NA * (c - NC)] = s;
+            }
+        }
+        __syncthreads();
+        cholesky_warp<NPV>(sm.M);
+        __syncthreads();
+        // M^-1 C, M^-1 E in place (one right-hand side per thread)
+        for (int t = tid; t < NPV * ND + NDF * ND; t += NT) {
+            double* col = (t < NPV * ND) ? &sm.C[NPV * t] : &sm.E[NPV * (t - NPV * ND)];
+            chol_solve_col<NPV>(sm.M, col);
+        }
+        __syncthreads();
+        // q sensitivities at volume and face points
+        for (int t = tid; t < NGV * NPV * ND; t += NT) {
+            const int g = t % NGV, ad = t / NGV;   // ad = a + NPV*d
+            double s = 0.0;
+            for (int b = 0; b < NPV; b++) s += T.shapvt[g + NGV * b] * sm.C[b + NPV * ad];
+            sMiC[t] = s;
+        }
+        for (int t = tid; t < NGV * NDF * ND; t += NT) {
+            const int g = t % NGV, fd = t / NGV;   // fd = fn + NDF*d
+            double s = 0.0;
+            for (int b = 0; b < NPV; b++) s += T.shapvt[g + NGV * b] * sm.E[b + NPV * fd];
+            sMiE[t] = -s;
+        }
+        for (int t = tid; t < NA * NPV * ND; t += NT) {
+            const int gg = t % NA, ad = t / NA, fc = gg / NGF, q = gg % NGF;
+            double s = 0.0;
+            for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.C[sm.perm[fc * NPF + m] + NPV * ad];
+            sMiCf[t] = s;
+        }
+        for (int t = tid; t < NA * NDF * ND; t += NT) {
+            const int gg = t % NA, fd = t / NA, fc = gg / NGF, q = gg % NGF;
+            double s = 0.0;
+            for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.E[sm.perm[fc * NPF + m] + NPV * fd];
+            sMiEf[t] = s;
+        }
+        // pointwise fluxes: volume points (threads [0, NGV)), face points ([NGV, NGV+NA))
+        if (tid < NGV + NA) {
+            using DD = Dual<NC>;
+            DD w[NC], f[ND * NCU];
+            const bool vol = tid < NGV;
+            const int g = vol ? tid : tid - NGV;
+#pragma unroll
+            for (int k = 0; k < NC; k++) {
+                double val;
+                if (vol) val = sm.ug[g + NGV * k];
+                else val = (k < NCU) ? sm.uhg[g + NA * k] : sm.ugf[g + NA * k];
+                w[k] = dc<NC>(val);
+                w[k].d[k] = 1.0;
+            }
+            ns_flux_dual<ND>(A.param, w, f);
+            if (vol) {
+                const double jg = sm.jac[g];
+#pragma unroll
+                for (int j = 0; j < NCU; j++) {
+                    double s = 0.0;
+                    if (A.tdep) {
+                        double t = 0.0;
+                        for (int a = 0; a < NPV; a++) t += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
+                        s = t - sm.ug[g + NGV * j] * A.fc_u;
+                    }
+                    sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
+#pragma unroll
+                    for (int m = 0; m < ND; m++) {
+                        double fx = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
+                        sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
+                    }
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        const double su = (A.tdep && k == j) ? -A.fc_u : 0.0;
+                        wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
+#pragma unroll
+                        for (int m = 0; m < ND; m++) {
+                            double t = 0.0;
+#pragma unroll
+                            for (int d = 0; d < ND; d++) t += f[d * NCU + j].d[k] * sm.Xx[g + NGV * (d + ND * m)];
+                            wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -t;
+                        }
+                    }
+                }
+            } else {
+                // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
+                const double tau = A.param[5];
+                const double jf = sm.jacf[g];
+#pragma unroll
+                for (int j = 0; j < NCU; j++) {
+                    double t = tau * (sm.ugf[g + NA * j] - sm.uhg[g + NA * j]);
+#pragma unroll
+                    for (int d = 0; d < ND; d++) t += f[d * NCU + j].v * sm.nl[g + NA * d];
+                    sm.fn[g + NA * j] = t * jf;
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        double dn = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[k] * sm.nl[g + NA * d];
+                        if (k < NCU) {
+                            fnuh[g + NA * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
+                            fnu[g + NA * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
+                        } else {
+                            fnu[g + NA * (j + NCH * k)] = dn * jf;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- trace-equation blocks K (nb x n), H (nb x nb), Rh (nb)
+        double* Ke = A.K + (size_t)e * NB * N;
+        double* He = A.H + (size_t)e * NB * NB;
+        double* Rhe = A.Rh + (size_t)e * NB;
+        double* Roe = A.Ro + (size_t)e * NB;
+        for (int t = tid; t < NB * N; t += NT) {
+            const int r = t % NB, c = t / NB;
+            const int j = r % NCH, fdof = r / NCH, fc = fdof / NPF, ip = fdof % NPF;
+            const int a = c % NPV, m = c / NPV;
+            double s = 0.0;
+            for (int kk = 0; kk < NPF; kk++)
+                if (sm.perm[fc * NPF + kk] == a)
+                    for (int q = 0; q < NGF; q++)
+                        s += T.sfsf[(ip + NPF * kk) + NPF2 * q] * fnu[q + NGF * fc + NA * (j + NCH * m)];
+            for (int q = 0; q < NGF; q++) {
+                const int gg = q + NGF * fc;
+                double v = 0.0;
+#pragma unroll
+                for (int d = 0; d < ND; d++) v += fnu[gg + NA * (j + NCH * (NCU * (1 + d) + m))] * sMiCf[gg + NA * (a + NPV * d)];
+                s += T.shapfg[ip + NPF * q] * v;
+            }
+            Ke[t] = s;
+        }
+        for (int t = tid; t < NB * NB; t += NT) {
+            const int r = t % NB, c = t / NB;
+            const int j = r % NCH, fdof = r / NCH, fc = fdof / NPF, ip = fdof % NPF;
+            const int m = c % NCH, fdof2 = c / NCH;
+            double s = 0.0;
+            if (fdof2 / NPF == fc) {
+                const int kk = fdof2 % NPF;
+                for (int q = 0; q < NGF; q++)
+                    s += T.sfsf[(ip + NPF * kk) + NPF2 * q] * fnuh[q + NGF * fc + NA * (j + NCH * m)];
+            }
+            double s2 = 0.0;
+            for (int q = 0; q < NGF; q++) {
+                const int gg = q + NGF * fc;
+                double v = 0.0;
+#pragma unroll
+                for (int d = 0; d < ND; d++) v += fnu[gg + NA * (j + NCH * (NCU * (1 + d) + m))] * sMiEf[gg + NA * (fdof2 + NDF * d)];
+                s2 += T.shapfg[ip + NPF * q] * v;
+            }
+            He[t] = s - s2;
+        }
+        for (int t = tid; t < NB; t += NT) {
+            const int j = t % NCH, fdof = t / NCH, fc = fdof / NPF, ip = fdof % NPF;
+            double s = 0.0;
+            for (int q = 0; q < NGF; q++) s += T.shapfg[ip + NPF * q] * sm.fn[q + NGF * fc + NA * j];
+            Rhe[t] = -s;
+            Roe[t] = -s;
+        }
+        __syncthreads();
+
+        // ---- element blocks D (n x n), F (n x nb), Ru (n): volume part + lifted trace part
+        double* De = A.D + (size_t)e * N * N;
+        double* Fe = A.F + (size_t)e * N * NB;
+        for (int col = tid; col < NCU * NPV * NCU + NCU * NCU * NDF; col += NT) {
+            double acc[NPV];
+#pragma unroll
+            for (int i = 0; i < NPV; i++) acc[i] = 0.0;
+            if (col < NCU * NPV * NCU) {            // D column (j, a, k) -> rows (i, j)
+                const int j = col % NCU, a = (col / NCU) % NPV, k = col / (NCU * NPV);
+                for (int r = 0; r < ND1; r++)
+                    for (int g = 0; g < NGV; g++) {
+                        double w = wrl[g + NGV * (r + ND1 * (j + NCU * k))] * T.shapvt[g + NGV * a];
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            w += wrl[g + NGV * (r + ND1 * (j + NCU * (NCU * (1 + d) + k)))] * sMiC[g + NGV * (a + NPV * d)];
+                        const int q = g + NGV * r;
+#pragma unroll
+                        for (int i = 0; i < NPV; i++) acc[i] += sm.shapvg[i + NPV * q] * w;
+                    }
+                const int kcol = a + NPV * k;
+#pragma unroll
+                for (int i = 0; i < NPV; i++) {
+                    double s = acc[i];
+                    for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
+                        s += Ke[j + NCH * sm.inc_f[i * S::MAXINC + c2] + NB * kcol];
+                    De[i + NPV * (j + NCU * kcol)] = s;
+                }
+            } else {                                 // F column (j, k, fn2)
+                const int cc = col - NCU * NPV * NCU;
+                const int j = cc % NCU, k = (cc / NCU) % NCU, fn2 = cc / (NCU * NCU);
+                for (int r = 0; r < ND1; r++)
+                    for (int g = 0; g < NGV; g++) {
+                        double w = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++)
+                            w += wrl[g + NGV * (r + ND1 * (j + NCU * (NCU * (1 + d) + k)))] * sMiE[g + NGV * (fn2 + NDF * d)];
+                        const int q = g + NGV * r;
+#pragma unroll
+                        for (int i = 0; i < NPV; i++) acc[i] += sm.shapvg[i + NPV * q] * w;
+                    }
+                const int hcol = k + NCH * fn2;
+#pragma unroll
+                for (int i = 0; i < NPV; i++) {
+                    double s = acc[i];
+                    for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
+                        s += He[j + NCH * sm.inc_f[i * S::MAXINC + c2] + NB * hcol];
+                    Fe[i + NPV * (j + NCU * hcol)] = s;
+                }
+            }
+        }
+        double ru2 = 0.0;
+        for (int t = tid; t < N; t += NT) {
+            const int i = t % NPV, j = t / NPV;
+            double s = 0.0;
+            for (int q = 0; q < NQ; q++) s += sm.shapvg[i + NPV * q] * sm.wrk[q + NQ * j];
+            for (int c2 = 0; c2 < sm.inc_n[i]; c2++) s += Rhe[j + NCH * sm.inc_f[i * S::MAXINC + c2]];
+            A.Ru[(size_t)e * N + t] = s;
+            ru2 += s * s;
+        }
+        const double tot = block_sum(ru2, sm.red);
+        if (tid == 0) A.ru2[e] = tot;
+    }
+}
+
+// --------------------------------------------------------- condensation
+struct SchurArgs {
+    int ne;
+    double *D, *F, *K, *H, *Ru, *Rh;     // F -> D^-1 F in place, Ru -> D^-1 Ru, H and Rh condensed
+    int* info;                            // per element: 0 or 1 + singular pivot index
+};
+
+// CTA-wide C (M x Ncol) = beta C + alpha A (M x Kd) B (Kd x Ncol), column-major, generic pointers.
+// 64 x 64 output tiles, 16-deep k panels staged in shared memory, 4 x 4 per thread.
+__device__ void cta_gemm(int M, int Ncol, int Kd, double alpha, const double* A, int lda, const double* B, int ldb,
+                         double beta, double* C, int ldc, double* tile /* 2*16*64 */) {
+    constexpr int BM = 64, BN = 64, BK = 16;
+    double* As = tile;
+    double* Bs = tile + BK * BM;
+    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+    for (int m0 = 0; m0 < M; m0 += BM)
+        for (int n0 = 0; n0 < Ncol; n0 += BN) {
+            double acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+            for (int k0 = 0; k0 < Kd; k0 += BK) {
+                __syncthreads();
+                for (int t = tid; t < BK * BM; t += blockDim.x) {
+                    const int m = t % BM, k = t / BM;
+                    As[k * BM + m] = (m0 + m < M && k0 + k < Kd) ? A[(m0 + m) + (size_t)lda * (k0 + k)] : 0.0;
+                }
+                for (int t = tid; t < BK * BN; t += blockDim.x) {
+                    const int k = t % BK, n = t / BK;
+                    Bs[k * BN + n] = (n0 + n < Ncol && k0 + k < Kd) ? B[(k0 + k) + (size_t)ldb * (n0 + n)] : 0.0;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int k = 0; k < BK; k++) {
+                    double a[4], b[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) a[i] = As[k * BM + ty + 16 * i];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) b[j] = Bs[k * BN + tx + 16 * j];
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
+                    if (m < M && n < Ncol) {
+                        double* c = &C[m + (size_t)ldc * n];
+                        *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[i][j];
+                    }
+                }
+        }
+    __syncthreads();
+}
+
+// Static condensation per element (elementschur.cpp:6-329): D^-1 by Gauss-Jordan with
+// partial pivoting in shared memory, F <- D^-1 F, H <- H - K D^-1 F, Ru <- D^-1 Ru,
+// Rh <- Rh - K D^-1 Ru.
+template <int N, int NB>
+__global__ void __launch_bounds__(NT) schur_kernel(SchurArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* Ai = reinterpret_cast<double*>(smem_raw);          // N x N
+    constexpr int PW = 32;                                       // F panel width
+    double* panel = Ai + N * N;                                  // N x PW
+    double* tile = panel + N * PW;                               // 2*16*64
+    double* vec = tile + 2 * 16 * 64;                            // N
+    __shared__ int piv[N];
+    __shared__ int s_p;
+    __shared__ double s_red[NT / 32];
+    __shared__ int s_redi[NT / 32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+    for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
+        __syncthreads();
+        const double* De = A.D + (size_t)e * N * N;
+        for (int t = tid; t < N * N; t += NT) Ai[t] = De[t];
+        __syncthreads();
+        int bad = 0;
+        for (int k = 0; k < N; k++) {
+            // pivot: first row of maximal |A(i,k)|, i >= k (LAPACK idamax tie rule)
+            double best = -1.0;
+            int bi = N;
+            for (int i = k + tid; i < N; i += NT) {
+                const double v = fabs(Ai[i + N * k]);
+                if (v > best) { best = v; bi = i; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) { s_red[wid] = best; s_redi[wid] = bi; }
+            __syncthreads();
+            if (tid == 0) {
+                double b = s_red[0];
+                int p = s_redi[0];
+                for (int w = 1; w < NT / 32; w++)
+                    if (s_red[w] > b || (s_red[w] == b && s_redi[w] < p)) { b = s_red[w]; p = s_redi[w]; }
+                s_p = p;
+                piv[k] = p;
+            }
+            __syncthreads();
+            const int p = s_p;
+            if (Ai[p + N * k] == 0.0) { bad = k + 1; break; }
+            if (p != k)
+                for (int c = tid; c < N; c += NT) {
+                    const double t = Ai[k + N * c];
+                    Ai[k + N * c] = Ai[p + N * c];
+                    Ai[p + N * c] = t;
+                }
+            __syncthreads();
+            const double dinv = 1.0 / Ai[k + N * k];
+            // column k of the eliminated rows, saved before the row update
+            for (int i = tid; i < N; i += NT) vec[i] = (i == k) ? 0.0 : Ai[i + N * k];
+            __syncthreads();
+            for (int c = tid; c < N; c += NT) Ai[k + N * c] = (c == k ? 1.0 : Ai[k + N * c]) * dinv;
+            __syncthreads();
+            for (int t = tid; t < N * N; t += NT) {
+                const int i = t % N, c = t / N;
+                if (i != k) {
+                    const double base = (c == k) ? 0.0 : Ai[i + N * c];
+                    Ai[i + N * c] = base - vec[i] * Ai[k + N * c];
+                }
+            }
+            __syncthreads();
+        }
+        if (bad) {
+            if (tid == 0) A.info[e] = bad;
+            continue;
+        }
+        // undo the row interchanges on the columns of the inverse
+        for (int k = N - 1; k >= 0; k--) {
+            const int p = piv[k];
+            if (p != k)
+                for (int i = tid; i < N; i += NT) {
+                    const double t = Ai[i + N * k];
+                    Ai[i + N * k] = Ai[i + N * p];
+                    Ai[i + N * p] = t;
+                }
+            __syncthreads();
+        }
+        if (tid == 0) A.info[e] = 0;
+        // F <- D^-1 F, panel by panel (in place in global memory)
+        double* Fe = A.F + (size_t)e * N * NB;
+        for (int c0 = 0; c0 < NB; c0 += PW) {
+            const int w = min(PW, NB - c0);
+            for (int t = tid; t < N * w; t += NT) panel[t] = Fe[(t % N) + (size_t)N * (c0 + t / N)];
+            __syncthreads();
+            for (int t = tid; t < N * w; t += NT) {
+                const int i = t % N, c = t / N;
+                double s = 0.0;
+                for (int k = 0; k < N; k++) s += Ai[i + N * k] * panel[k + N * c];
+                Fe[i + (size_t)N * (c0 + c)] = s;
+            }
+            __syncthreads();
+        }
+        // Ru <- D^-1 Ru
+        double* Rue = A.Ru + (size_t)e * N;
+        for (int t = tid; t < N; t += NT) vec[t] = Rue[t];
+        __syncthreads();
+        for (int i = tid; i < N; i += NT) {
+            double s = 0.0;
+            for (int k = 0; k < N; k++) s += Ai[i + N * k] * vec[k];
+            Rue[i] = s;
+        }
+        __syncthreads();
+        // H <- H - K (D^-1 F);  Rh <- Rh - K (D^-1 Ru)
+        const double* Ke = A.K + (size_t)e * NB * N;
+        cta_gemm(NB, NB, N, -1.0, Ke, NB, Fe, N, 1.0, A.H + (size_t)e * NB * NB, NB, tile);
+        double* Rhe = A.Rh + (size_t)e * NB;
+        for (int r = tid; r < NB; r += NT) {
+            double s = 0.0;
+            for (int k = 0; k < N; k++) s += Ke[r + (size_t)NB * k] * Rue[k];
+            Rhe[r] -= s;
+        }
+    }
+}
+
+// --------------------------------------------------------------- scatter
+// Owner-gather into the face-block system (globalassembly.cpp:40-89): every
+// Hg entry sums its (at most two) element contributions in ascending element
+// order, exactly the order of the reference's serial element loop.
+struct ScatterArgs {
+    int nblk, nf, npf, nch, nfe, nb;
+    const int* blk_src;        // nblk x 2 x 3: (element, a, b) or -1
+    const int* face_src;       // nf x 2 x 2: (element, a) or -1
+    const int* elcon;          // ne x ndf
+    const int* rowface;        // nblk: row face i of block k
+    const int* colface;        // nblk: column face j of block k
+    const double *H, *Rh, *Ro;
+    double *Hg, *Rg, *Rr;
+};
+
+__global__ void scatter_H_kernel(ScatterArgs A) {
+    const int bsz = A.npf * A.nch, ndf = A.npf * A.nfe;
+    const long long total = (long long)A.nblk * bsz * bsz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / (bsz * bsz));
+        const int w = (int)(t % (bsz * bsz));
+        const int colpos = w / bsz, rowpos = w % bsz;     // Hg block column-major: rowpos fastest
+        const int m1 = colpos / A.nch, n1 = colpos % A.nch, m2 = rowpos / A.nch, n2 = rowpos % A.nch;
+        const int i = A.rowface[k], j = A.colface[k];
+        double s = 0.0;
+        for (int c = 0; c < 2; c++) {
+            const int e = A.blk_src[(k * 2 + c) * 3 + 0];
+            if (e < 0) break;
+            const int a = A.blk_src[(k * 2 + c) * 3 + 1], b = A.blk_src[(k * 2 + c) * 3 + 2];
+            const int ind = A.elcon[(size_t)e * ndf + a * A.npf + m2] - i * A.npf;
+            const int jnd = A.elcon[(size_t)e * ndf + b * A.npf + m1] - j * A.npf;
+            s += A.H[(size_t)e * A.nb * A.nb + (a * bsz + ind * A.nch + n2) + (size_t)A.nb * (b * bsz + jnd * A.nch + n1)];
+        }
+        A.Hg[t] = s;
+    }
+}
+
+__global__ void scatter_R_kernel(ScatterArgs A) {
+    const int bsz = A.npf * A.nch, ndf = A.npf * A.nfe;
+    const int total = A.nf * bsz;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int i = t / bsz, w = t % bsz, m1 = w / A.nch, n1 = w % A.nch;
+        double s = 0.0, so = 0.0;
+        for (int c = 0; c < 2; c++) {
+            const int e = A.face_src[(i * 2 + c) * 2 + 0];
+            if (e < 0) break;
+            const int a = A.face_src[(i * 2 + c) * 2 + 1];
+            const int ind = A.elcon[(size_t)e * ndf + a * A.npf + m1] - i * A.npf;
+            const size_t idx = (size_t)e * A.nb + a * bsz + ind * A.nch + n1;
+            s += A.Rh[idx];
+            if (A.Ro) so += A.Ro[idx];
+        }
+        if (A.Rg) A.Rg[t] = s;
+        if (A.Rr) A.Rr[t] = so;
+    }
+}
+
+// sqrt(sum ru2 + sum Rr^2), one CTA, fixed summation order.
+__global__ void rnorm_kernel(int ne, const double* ru2, int nr, const double* rr, double* out) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) s += ru2[i];
+    double s2 = 0.0;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) s2 += rr[i] * rr[i];
+    s += s2;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        *out = sqrt(t);
+    }
+}
+
+// ------------------------------------------------------ q recovery / update
+struct QArgs {
+    Tables T;
+    const double* dgnodes;
+    const int* elcon;
+    double* udg;                // u read, q written
+    const double *uh, *sh;
+    double fc_q;
+    int ne;
+    // optional update before the q solve: u += alpha (DinvRu - DinvF duh_e)
+    const double *DinvRu, *DinvF, *duh;
+    double alpha;
+};
+
+template <class S>
+struct QSmem {
+    double x[S::NPV * S::ND];
+    double jac[S::NGV], Xx[S::NGV * S::ND * S::ND];
+    double jacf[S::NA], nl[S::NA * S::ND];
+    double M[S::NPV * S::NPV];
+    double C[S::NPV * S::NPV * S::ND];
+    double E[S::NPV * S::NDF * S::ND];
+    double u[S::NPV * S::NCU];
+    double uhe[S::NDF * S::NCH];
+    double de[S::NB];
+    double q[S::NPV * S::NCU * S::ND];
+};
+
+// getQ (elementassembly.cpp:1414-1479), optionally preceded by getU (solutionupdate.cpp:6-68).
+template <class S>
+__global__ void __launch_bounds__(NT) getq_kernel(QArgs A) {
+    constexpr int ND = S::ND, NPV = S::NPV, NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, N = S::N, NB = S::NB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    QSmem<S>& sm = *reinterpret_cast<QSmem<S>*>(smem_raw);
+    const int tid = threadIdx.x;
+    for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
+        __syncthreads();
+        double* ue = A.udg + (size_t)e * NPV * NC;
+        for (int t = tid; t < NPV * ND; t += NT) sm.x[t] = A.dgnodes[(size_t)e * NPV * ND + t];
+        for (int t = tid; t < NDF * NCH; t += NT) {
+            const int fn = t / NCH, c = t % NCH;
+            const int gd = A.elcon[(size_t)e * NDF + fn];
+            sm.uhe[fn + NDF * c] = A.uh[(size_t)gd * NCH + c];
+            if (A.DinvF) sm.de[fn * NCH + c] = A.duh[(size_t)gd * NCH + c];
+        }
+        __syncthreads();
+        for (int t = tid; t < N; t += NT) {
+            double v = ue[t];
+            if (A.DinvF) {
+                const double* df = A.DinvF + (size_t)e * N * NB;
+                double s = 0.0;
+                for (int c = 0; c < NB; c++) s += df[t + (size_t)N * c] * sm.de[c];
+                v += -A.alpha * s;
+                v += A.alpha * A.DinvRu[(size_t)e * N + t];
+                ue[t] = v;
+            }
+            sm.u[t] = v;
+        }
+        geometry<S>(A.T, sm.x, sm.jac, sm.Xx, sm.jacf, sm.nl);
+        __syncthreads();
+        qmatrices<S>(A.T, A.fc_q, sm.jac, sm.Xx, sm.jacf, sm.nl, sm.M, sm.C, sm.E);
+        __syncthreads();
+        const double* she = A.sh + (size_t)e * NPV * NC;
+        for (int t = tid; t < NPV * NCU * ND; t += NT) {
+            const int i = t % NPV, c = (t / NPV) % NCU, d = t / (NPV * NCU);
+            double s = 0.0;
+            for (int a = 0; a < NPV; a++) s += sm.M[i + NPV * a] * she[a + NPV * (NCU * (1 + d) + c)];
+            for (int a = 0; a < NPV; a++) s += sm.C[i + NPV * (a + NPV * d)] * sm.u[a + NPV * c];
+            for (int fn = 0; fn < NDF; fn++) s -= sm.E[i + NPV * (fn + NDF * d)] * sm.uhe[fn + NDF * c];
+            sm.q[t] = s;
+        }
+        __syncthreads();
+        cholesky_warp<NPV>(sm.M);
+        __syncthreads();
+        for (int t = tid; t < NCU * ND; t += NT) chol_solve_col<NPV>(sm.M, &sm.q[NPV * t]);
+        __syncthreads();
+        for (int t = tid; t < NPV * NCU * ND; t += NT) {
+            const int i = t % NPV, c = (t / NPV) % NCU, d = t / (NPV * NCU);
+            ue[i + NPV * (NCU * (1 + d) + c)] = sm.q[t];
+        }
+    }
+}
+
+__global__ void axpy_kernel(long long n, double alpha, const double* x, double* y) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] += alpha * x[i];
+}
+
+}  // namespace hfem

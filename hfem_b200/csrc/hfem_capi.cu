@@ -1,0 +1,825 @@
+// C ABI of the B200 HDG element hot path (declared in include/hfem_b200.h).
+//
+// Host side of the library: context and device buffers, connectivity checks,
+// kernel dispatch over the compiled element shapes, GMRES and the Newton
+// driver (restating solvers/dgsolvers.cpp:40-205).  Every entry point returns
+// a status code; nothing exits the process.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/hfem_b200.h"
+#include "elem_kernels.cuh"
+#include "krylov_kernels.cuh"
+
+using namespace hfem;
+
+namespace {
+
+struct KernelTimer {
+    bool on = false;
+    std::map<std::string, std::pair<double, int>> acc;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+
+// Element shapes with compiled kernels: (nd, npv, npf, ngv, ngf).
+#define HFEM_SHAPES(X)          \
+    X(2, 3, 2, 3, 2)            \
+    X(2, 6, 3, 6, 3)            \
+    X(2, 10, 4, 12, 4)          \
+    X(2, 15, 5, 16, 5)          \
+    X(3, 4, 3, 4, 3)            \
+    X(3, 10, 6, 14, 6)          \
+    X(3, 20, 10, 24, 12)
+
+struct Launch {
+    int nd, npv, npf, ngv, ngf;
+    size_t ws;                  // workspace doubles per CTA slot
+    size_t elem_smem, schur_smem, q_smem;
+    void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
+    void (*schur)(dim3, size_t, cudaStream_t, const SchurArgs&);
+    void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
+    const void *elem_fn, *schur_fn, *q_fn;
+};
+
+template <class S>
+void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel<S><<<g, NT, sm, st>>>(a); }
+template <class S>
+void launch_schur(dim3 g, size_t sm, cudaStream_t st, const SchurArgs& a) { schur_kernel<S::N, S::NB><<<g, NT, sm, st>>>(a); }
+template <class S>
+void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
+
+template <class S>
+Launch make_launch() {
+    Launch L;
+    L.nd = S::ND; L.npv = S::NPV; L.npf = S::NPF; L.ngv = S::NGV; L.ngf = S::NGF;
+    L.ws = S::WS;
+    L.elem_smem = sizeof(ElemSmem<S>);
+    L.schur_smem = sizeof(double) * ((size_t)S::N * S::N + (size_t)S::N * 32 + 2 * 16 * 64 + S::N);
+    L.q_smem = sizeof(QSmem<S>);
+    L.element = launch_element<S>;
+    L.schur = launch_schur<S>;
+    L.getq = launch_getq<S>;
+    L.elem_fn = (const void*)element_kernel<S>;
+    L.schur_fn = (const void*)schur_kernel<S::N, S::NB>;
+    L.q_fn = (const void*)getq_kernel<S>;
+    return L;
+}
+
+const std::vector<Launch>& launches() {
+    static std::vector<Launch> v = {
+#define X(a, b, c, d, e) make_launch<Shape<a, b, c, d, e>>(),
+        HFEM_SHAPES(X)
+#undef X
+    };
+    return v;
+}
+
+}  // namespace
+
+struct hfem_ctx {
+    hfem_dims dims{};
+    int device = 0;
+    int ncu = 0, nc = 0, nch = 0, ndf = 0, n = 0, nb = 0, bsz = 0;
+    const Launch* L = nullptr;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string err;
+    bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
+    int grid_elem = 0, grid_schur = 0;
+    // master tables
+    double *shapvt = nullptr, *shapvg = nullptr, *svsv = nullptr, *shapft = nullptr, *shapfg = nullptr, *sfsf = nullptr;
+    int* perm = nullptr;
+    // mesh
+    double* dgnodes = nullptr;
+    int *elcon = nullptr, *rowstart = nullptr, *colidx = nullptr, *blk_src = nullptr, *face_src = nullptr;
+    int *rowface = nullptr, *colface = nullptr;
+    std::vector<int> h_rowstart, h_colidx;
+    // physics
+    double param[6] = {0};
+    int tdep = 0;
+    double fc_u = 0, fc_q = 1, time = 0;
+    // state
+    double *udg = nullptr, *uh = nullptr, *sh = nullptr;
+    // assembly outputs and workspace
+    double *D = nullptr, *F = nullptr, *K = nullptr, *H = nullptr, *Ru = nullptr, *Rh = nullptr, *Ro = nullptr;
+    double *ru2 = nullptr, *Hg = nullptr, *Rg = nullptr, *Rr = nullptr, *rnorm = nullptr, *ws = nullptr;
+    int* info = nullptr;
+    // Krylov
+    double *Minv = nullptr, *V = nullptr, *w = nullptr, *x = nullptr, *pb = nullptr, *scal = nullptr, *part = nullptr;
+    int* binfo = nullptr;
+    int krylov_restart = 0;
+    KernelTimer timer;
+};
+
+namespace {
+
+int fail(hfem_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(c, HFEM_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dalloc(hfem_ctx* c, T** p, size_t count) {
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(c, HFEM_E_NOMEM, "cudaMalloc of %zu bytes: %s", sizeof(T) * count, cudaGetErrorString(e));
+    }
+    return 0;
+}
+
+template <class T>
+int upload(hfem_ctx* c, T** p, const T* h, size_t count) {
+    int rc = dalloc(c, p, count);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(*p, h, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
+    return 0;
+}
+
+struct Timed {
+    hfem_ctx* c;
+    const char* name;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timed(hfem_ctx* c_, const char* n) : c(c_), name(n) {
+        if (c->timer.on) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~Timed() {
+        if (c->timer.on) {
+            cudaEventRecord(b, c->stream);
+            c->timer.pending.push_back({name, {a, b}});
+        }
+    }
+};
+
+void flush_timer(hfem_ctx* c) {
+    for (auto& p : c->timer.pending) {
+        cudaEventSynchronize(p.second.second);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+        auto& slot = c->timer.acc[p.first];
+        slot.first += ms;
+        slot.second += 1;
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    c->timer.pending.clear();
+}
+
+int check_launch(hfem_ctx* c, const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, HFEM_E_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+    return 0;
+}
+
+int sms(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    return v > 0 ? v : 1;
+}
+
+int ensure_assembly_buffers(hfem_ctx* c) {
+    if (c->D) return 0;
+    const size_t ne = c->dims.ne, n = c->n, nb = c->nb;
+    int rc = 0;
+    if ((rc = dalloc(c, &c->D, ne * n * n))) return rc;
+    if ((rc = dalloc(c, &c->F, ne * n * nb))) return rc;
+    if ((rc = dalloc(c, &c->K, ne * nb * n))) return rc;
+    if ((rc = dalloc(c, &c->H, ne * nb * nb))) return rc;
+    if ((rc = dalloc(c, &c->Ru, ne * n))) return rc;
+    if ((rc = dalloc(c, &c->Rh, ne * nb))) return rc;
+    if ((rc = dalloc(c, &c->Ro, ne * nb))) return rc;
+    if ((rc = dalloc(c, &c->ru2, ne))) return rc;
+    if ((rc = dalloc(c, &c->info, ne))) return rc;
+    if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws))) return rc;
+    return 0;
+}
+
+ElemArgs elem_args(hfem_ctx* c) {
+    ElemArgs a;
+    a.T = Tables{c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm};
+    a.dgnodes = c->dgnodes;
+    a.elcon = c->elcon;
+    a.udg = c->udg;
+    a.uh = c->uh;
+    a.sh = c->sh;
+    for (int i = 0; i < 6; i++) a.param[i] = c->param[i];
+    a.tdep = c->tdep;
+    a.fc_u = c->fc_u;
+    a.fc_q = c->fc_q;
+    a.ne = c->dims.ne;
+    a.D = c->D; a.F = c->F; a.K = c->K; a.H = c->H;
+    a.Ru = c->Ru; a.Rh = c->Rh; a.Ro = c->Ro; a.ru2 = c->ru2;
+    a.ws = c->ws;
+    return a;
+}
+
+ScatterArgs scatter_args(hfem_ctx* c) {
+    ScatterArgs s;
+    s.nblk = c->dims.nblocks; s.nf = c->dims.nf; s.npf = c->dims.npf; s.nch = c->nch; s.nfe = c->dims.nfe; s.nb = c->nb;
+    s.blk_src = c->blk_src; s.face_src = c->face_src; s.elcon = c->elcon;
+    s.rowface = c->rowface; s.colface = c->colface;
+    s.H = c->H; s.Rh = c->Rh; s.Ro = c->Ro;
+    s.Hg = c->Hg; s.Rg = c->Rg; s.Rr = c->Rr;
+    return s;
+}
+
+int ready(hfem_ctx* c) {
+    if (!c) return HFEM_E_ARG;
+    if (!c->have_master || !c->have_mesh || !c->have_phys || !c->have_sol)
+        return fail(c, HFEM_E_STATE, "master, mesh, physics and solution must be set first");
+    return 0;
+}
+
+// Element pass: local blocks, condensation (matrix=true) and scatter.
+int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
+    int rc = ready(c);
+    if (rc) return rc;
+    if ((rc = ensure_assembly_buffers(c))) return rc;
+    const dim3 ge(c->grid_elem), gs(c->grid_schur);
+    {
+        Timed t(c, "element");
+        c->L->element(ge, c->L->elem_smem, c->stream, elem_args(c));
+        if ((rc = check_launch(c, "element"))) return rc;
+    }
+    ScatterArgs sa = scatter_args(c);
+    if (matrix) {
+        SchurArgs s{c->dims.ne, c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->info};
+        {
+            Timed t(c, "schur");
+            c->L->schur(gs, c->L->schur_smem, c->stream, s);
+            if ((rc = check_launch(c, "schur"))) return rc;
+        }
+        {
+            Timed t(c, "scatter_H");
+            scatter_H_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(sa);
+            if ((rc = check_launch(c, "scatter_H"))) return rc;
+        }
+    } else {
+        sa.Rg = nullptr;
+    }
+    {
+        Timed t(c, "scatter_R");
+        scatter_R_kernel<<<sms(c->device) * 4, 256, 0, c->stream>>>(sa);
+        if ((rc = check_launch(c, "scatter_R"))) return rc;
+    }
+    rnorm_kernel<<<1, 1024, 0, c->stream>>>(c->dims.ne, c->ru2, c->dims.nf * c->bsz, c->Rr, c->rnorm);
+    if ((rc = check_launch(c, "rnorm"))) return rc;
+    if (matrix) {
+        std::vector<int> info(c->dims.ne);
+        CK(cudaMemcpyAsync(info.data(), c->info, sizeof(int) * info.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int e = 0; e < c->dims.ne; e++)
+            if (info[e]) return fail(c, HFEM_E_SINGULAR, "element %d: singular local matrix (pivot %d)", e, info[e]);
+        c->assembled = true;
+    }
+    double rn = 0.0;
+    CK(cudaMemcpyAsync(&rn, c->rnorm, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    flush_timer(c);
+    if (rnorm_out) *rnorm_out = rn;
+    return 0;
+}
+
+int launch_getq(hfem_ctx* c, const double* duh, double alpha) {
+    QArgs q;
+    q.T = Tables{c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm};
+    q.dgnodes = c->dgnodes;
+    q.elcon = c->elcon;
+    q.udg = c->udg;
+    q.uh = c->uh;
+    q.sh = c->sh;
+    q.fc_q = c->fc_q;
+    q.ne = c->dims.ne;
+    q.DinvRu = duh ? c->Ru : nullptr;
+    q.DinvF = duh ? c->F : nullptr;
+    q.duh = duh;
+    q.alpha = alpha;
+    Timed t(c, duh ? "update" : "getq");
+    c->L->getq(dim3(c->grid_elem), c->L->q_smem, c->stream, q);
+    return check_launch(c, "getq");
+}
+
+long long nvec(hfem_ctx* c) { return (long long)c->dims.nf * c->bsz; }
+
+int dot(hfem_ctx* c, const double* a, const double* b, double* out, bool sq) {
+    dot_partial_kernel<<<DOT_CTAS, DOT_THREADS, 0, c->stream>>>(nvec(c), a, b, c->part);
+    dot_final_kernel<<<1, 256, 0, c->stream>>>(c->part, out, sq ? 1 : 0);
+    return check_launch(c, "dot");
+}
+
+int matvec_prec(hfem_ctx* c, const double* x, double* z, bool prec) {
+    Timed t(c, "matvec");
+    bsr_matvec_bj_kernel<<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
+        c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, prec ? c->Minv : nullptr, x, z);
+    return check_launch(c, "matvec");
+}
+
+int ensure_krylov(hfem_ctx* c, int restart) {
+    int rc;
+    const size_t n = nvec(c);
+    if (!c->x) {
+        if ((rc = dalloc(c, &c->x, n))) return rc;
+        if ((rc = dalloc(c, &c->w, n))) return rc;
+        if ((rc = dalloc(c, &c->pb, n))) return rc;
+        if ((rc = dalloc(c, &c->Minv, (size_t)c->dims.nf * c->bsz * c->bsz))) return rc;
+        if ((rc = dalloc(c, &c->part, DOT_CTAS))) return rc;
+        if ((rc = dalloc(c, &c->binfo, c->dims.nf))) return rc;
+    }
+    if (c->krylov_restart < restart) {
+        if ((rc = dalloc(c, &c->V, n * (restart + 1)))) return rc;
+        if ((rc = dalloc(c, &c->scal, (size_t)(restart + 2) * (restart + 2)))) return rc;
+        c->krylov_restart = restart;
+    }
+    return 0;
+}
+
+int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters, double* hist,
+               int hist_len) {
+    int rc;
+    if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before gmres");
+    if (restart < 1 || maxit < 1 || !(tol > 0.0)) return fail(c, HFEM_E_ARG, "restart, maxit and tol must be positive");
+    if (precond != -1 && precond != 2) return fail(c, HFEM_E_ARG, "precond must be -1 (none) or 2 (block Jacobi)");
+    if ((rc = ensure_krylov(c, restart))) return rc;
+    const long long n = nvec(c);
+    const int g = sms(c->device) * 4;
+    const bool prec = precond == 2;
+    if (prec) {
+        Timed t(c, "bj_inverse");
+        const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
+        bj_inverse_kernel<<<std::min(c->dims.nf, sms(c->device) * 8), 64, smem, c->stream>>>(
+            c->dims.nf, c->bsz, c->rowstart, c->Hg, c->Minv, c->binfo);
+        if ((rc = check_launch(c, "bj_inverse"))) return rc;
+        std::vector<int> bi(c->dims.nf);
+        CK(cudaMemcpyAsync(bi.data(), c->binfo, sizeof(int) * bi.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < c->dims.nf; i++)
+            if (bi[i]) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d is singular", i);
+        bj_apply_kernel<<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv, c->Rg, c->pb);
+    } else {
+        CK(cudaMemcpyAsync(c->pb, c->Rg, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CK(cudaMemsetAsync(c->x, 0, sizeof(double) * n, c->stream));
+    // scal layout: [0] nrmb, [1] beta, [2 .. 2+restart] current Hessenberg column, [..] y
+    double* d_nrmb = c->scal;
+    double* d_beta = c->scal + 1;
+    double* d_h = c->scal + 2;
+    double* d_y = c->scal + 3 + restart;
+    if ((rc = dot(c, c->pb, c->pb, d_nrmb, true))) return rc;
+    double nrmb = 0.0;
+    CK(cudaMemcpyAsync(&nrmb, d_nrmb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (nrmb == 0.0) nrmb = 1.0;
+    std::vector<double> h((size_t)(restart + 1) * restart), cs(restart), sn(restart), gv(restart + 1), y(restart),
+        hcol(restart + 2);
+    int it = 0, flag = -2;
+    while (flag == -2) {
+        // r = M^-1 (b - A x) computed as M^-1 b - M^-1 A x (the same left-preconditioned residual)
+        if ((rc = matvec_prec(c, c->x, c->w, prec))) return rc;
+        sub_from_kernel<<<g, 256, 0, c->stream>>>(n, c->pb, c->w);
+        if ((rc = dot(c, c->w, c->w, d_beta, true))) return rc;
+        double beta = 0.0;
+        CK(cudaMemcpyAsync(&beta, d_beta, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (beta / nrmb <= tol) { flag = 0; break; }
+        scale_dev_kernel<<<g, 256, 0, c->stream>>>(n, d_beta, c->w, c->V);
+        std::fill(gv.begin(), gv.end(), 0.0);
+        gv[0] = beta;
+        int j = 0;
+        for (; j < restart; j++) {
+            double* vj = c->V + (size_t)j * n;
+            double* vn = c->V + (size_t)(j + 1) * n;
+            if ((rc = matvec_prec(c, vj, vn, prec))) return rc;
+            {
+                Timed t(c, "orthogonalise");
+                for (int i = 0; i <= j; i++) {             // modified Gram-Schmidt
+                    if ((rc = dot(c, c->V + (size_t)i * n, vn, d_h + i, false))) return rc;
+                    axpy_dev_kernel<<<g, 256, 0, c->stream>>>(n, d_h + i, c->V + (size_t)i * n, vn);
+                }
+                if ((rc = dot(c, vn, vn, d_h + j + 1, true))) return rc;
+                scale_dev_kernel<<<g, 256, 0, c->stream>>>(n, d_h + j + 1, vn, vn);
+            }
+            CK(cudaMemcpyAsync(hcol.data(), d_h, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            for (int i = 0; i <= j + 1; i++) h[i + (restart + 1) * j] = hcol[i];
+            const double nn = hcol[j + 1];
+            for (int i = 0; i < j; i++) {
+                const double a = h[i + (restart + 1) * j], b = h[i + 1 + (restart + 1) * j];
+                h[i + (restart + 1) * j] = cs[i] * a + sn[i] * b;
+                h[i + 1 + (restart + 1) * j] = -sn[i] * a + cs[i] * b;
+            }
+            const double a = h[j + (restart + 1) * j], b = h[j + 1 + (restart + 1) * j];
+            const double rr = std::sqrt(a * a + b * b);
+            cs[j] = a / rr;
+            sn[j] = b / rr;
+            h[j + (restart + 1) * j] = rr;
+            h[j + 1 + (restart + 1) * j] = 0.0;
+            gv[j + 1] = -sn[j] * gv[j];
+            gv[j] = cs[j] * gv[j];
+            const double res = std::fabs(gv[j + 1]);
+            if (hist && it < hist_len) hist[it] = res / nrmb;
+            it++;
+            if (res / nrmb <= tol) { flag = 0; j++; break; }
+            if (it >= maxit) { flag = 1; j++; break; }
+            if (nn == 0.0) { flag = -1; j++; break; }
+        }
+        for (int i = j - 1; i >= 0; i--) {
+            double s = gv[i];
+            for (int k = i + 1; k < j; k++) s -= h[i + (restart + 1) * k] * y[k];
+            y[i] = s / h[i + (restart + 1) * i];
+        }
+        CK(cudaMemcpyAsync(d_y, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, c->stream));
+        combine_kernel<<<g, 256, 0, c->stream>>>(n, j, c->V, d_y, c->x);
+        if ((rc = check_launch(c, "combine"))) return rc;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    flush_timer(c);
+    if (iters) *iters = it;
+    if (conv) *conv = (flag == 0) ? 1 : (flag == 1 ? 0 : -1);
+    return 0;
+}
+
+int update_impl(hfem_ctx* c, double alpha) {
+    int rc;
+    if (!c->assembled || !c->x) return fail(c, HFEM_E_STATE, "assemble and solve before update");
+    axpy_kernel<<<sms(c->device) * 4, 256, 0, c->stream>>>(nvec(c), alpha, c->x, c->uh);
+    if ((rc = check_launch(c, "uh update"))) return rc;
+    if ((rc = launch_getq(c, c->x, alpha))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    flush_timer(c);
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
+    if (!dims || !out) return HFEM_E_ARG;
+    *out = nullptr;
+    hfem_ctx* c = new hfem_ctx();
+    c->dims = *dims;
+    c->device = device;
+    const hfem_dims& d = *dims;
+    if (d.nd < 2 || d.nd > 3 || d.nfe != d.nd + 1 || d.ne <= 0 || d.nf <= 0 || d.nblocks < d.nf) {
+        delete c;
+        return HFEM_E_ARG;
+    }
+    for (const Launch& L : launches())
+        if (L.nd == d.nd && L.npv == d.npv && L.npf == d.npf && L.ngv == d.ngv && L.ngf == d.ngf) c->L = &L;
+    if (!c->L) {
+        delete c;
+        return HFEM_E_UNSUPPORTED;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete c;
+        return HFEM_E_CUDA;
+    }
+    c->ncu = d.nd + 2;
+    c->nc = c->ncu * (d.nd + 1);
+    c->nch = c->ncu;
+    c->ndf = d.npf * d.nfe;
+    c->n = d.npv * c->ncu;
+    c->nb = c->nch * c->ndf;
+    c->bsz = c->nch * d.npf;
+    if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return HFEM_E_CUDA;
+    }
+    c->stream = c->own;
+    const Launch& L = *c->L;
+    cudaFuncSetAttribute(L.elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
+    cudaFuncSetAttribute(L.schur_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.schur_smem);
+    cudaFuncSetAttribute(L.q_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.q_smem);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn, NT, L.elem_smem);
+    c->grid_elem = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
+    occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.schur_fn, NT, L.schur_smem);
+    c->grid_schur = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
+    if (cudaMalloc(&c->rnorm, sizeof(double)) != cudaSuccess) {
+        cudaStreamDestroy(c->own);
+        delete c;
+        return HFEM_E_NOMEM;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->own);
+        delete c;
+        return HFEM_E_CUDA;
+    }
+    *out = c;
+    return 0;
+}
+
+int hfem_destroy(hfem_ctx* c) {
+    if (!c) return HFEM_E_ARG;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    void* ptrs[] = {c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm, c->dgnodes, c->elcon,
+                    c->rowstart, c->colidx, c->blk_src, c->face_src, c->rowface, c->colface, c->udg, c->uh, c->sh,
+                    c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws,
+                    c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& p : c->timer.pending) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    if (c->own) cudaStreamDestroy(c->own);
+    delete c;
+    return 0;
+}
+
+const char* hfem_last_error(const hfem_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int hfem_set_stream(hfem_ctx* c, void* stream) {
+    if (!c) return HFEM_E_ARG;
+    c->stream = stream ? (cudaStream_t)stream : c->own;
+    return 0;
+}
+
+int hfem_set_master(hfem_ctx* c, const double* shapvt, const double* shapvg, const double* svsv, const double* shapft,
+                    const double* shapfg, const double* sfsf, const int* perm) {
+    if (!c || !shapvt || !shapvg || !svsv || !shapft || !shapfg || !sfsf || !perm) return HFEM_E_ARG;
+    const hfem_dims& d = c->dims;
+    for (int i = 0; i < d.npf * d.nfe; i++)
+        if (perm[i] < 0 || perm[i] >= d.npv) return fail(c, HFEM_E_ARG, "perm[%d] = %d out of range", i, perm[i]);
+    int rc;
+    CK(cudaSetDevice(c->device));
+    const size_t v1 = (size_t)d.ngv * d.npv * (d.nd + 1), v2 = (size_t)d.npv * d.npv * d.ngv * (d.nd + 1);
+    const size_t f1 = (size_t)d.ngf * d.npf * d.nd, f2 = (size_t)d.npf * d.npf * d.ngf * d.nd;
+    if ((rc = upload(c, &c->shapvt, shapvt, v1)) || (rc = upload(c, &c->shapvg, shapvg, v1)) ||
+        (rc = upload(c, &c->svsv, svsv, v2)) || (rc = upload(c, &c->shapft, shapft, f1)) ||
+        (rc = upload(c, &c->shapfg, shapfg, f1)) || (rc = upload(c, &c->sfsf, sfsf, f2)) ||
+        (rc = upload(c, &c->perm, perm, (size_t)d.npf * d.nfe)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_master = true;
+    return 0;
+}
+
+int hfem_set_mesh(hfem_ctx* c, const double* dgnodes, const int* elcon, const int* t2f, const int* rowstart,
+                  const int* colidx) {
+    if (!c || !dgnodes || !elcon || !t2f || !rowstart || !colidx) return HFEM_E_ARG;
+    const hfem_dims& d = c->dims;
+    const int ne = d.ne, nf = d.nf, nfe = d.nfe, npf = d.npf, ndf = c->ndf, nblk = d.nblocks;
+    // connectivity checks (the reference's own invariants: digasopre.m:80-88, globalassembly.cpp:69-75)
+    if (rowstart[0] != 0 || rowstart[nf] != nblk) return fail(c, HFEM_E_MESH, "ent2entStart must run from 0 to nblocks");
+    for (int i = 0; i < nf; i++) {
+        if (rowstart[i + 1] <= rowstart[i]) return fail(c, HFEM_E_MESH, "empty CSR row %d", i);
+        if (colidx[rowstart[i]] != i) return fail(c, HFEM_E_MESH, "row %d does not start with its diagonal block", i);
+    }
+    for (int k = 0; k < nblk; k++)
+        if (colidx[k] < 0 || colidx[k] >= nf) return fail(c, HFEM_E_MESH, "ent2ent[%d] out of range", k);
+    std::vector<int> rowface(nblk), blk((size_t)nblk * 6, -1), fsrc((size_t)nf * 4, -1), fcount(nf, 0), bcount(nblk, 0);
+    for (int i = 0; i < nf; i++)
+        for (int k = rowstart[i]; k < rowstart[i + 1]; k++) rowface[k] = i;
+    for (int e = 0; e < ne; e++) {
+        for (int a = 0; a < nfe; a++) {
+            const int i = t2f[e * nfe + a];
+            if (i < 0 || i >= nf) return fail(c, HFEM_E_MESH, "t2f of element %d out of range", e);
+            for (int m = 0; m < npf; m++) {
+                const int g = elcon[(size_t)e * ndf + a * npf + m];
+                if (g < i * npf || g >= (i + 1) * npf)
+                    return fail(c, HFEM_E_MESH, "elcon of element %d face %d does not lie on face %d", e, a, i);
+            }
+            if (fcount[i] >= 2) return fail(c, HFEM_E_MESH, "face %d has more than two elements", i);
+            fsrc[(i * 2 + fcount[i]) * 2 + 0] = e;
+            fsrc[(i * 2 + fcount[i]) * 2 + 1] = a;
+            fcount[i]++;
+            for (int b = 0; b < nfe; b++) {
+                const int j = t2f[e * nfe + b];
+                int k = -1;
+                for (int kk = rowstart[i]; kk < rowstart[i + 1]; kk++)
+                    if (colidx[kk] == j) { k = kk; break; }
+                if (k < 0) return fail(c, HFEM_E_MESH, "block (%d, %d) of element %d missing from the CSR", i, j, e);
+                if (bcount[k] >= 2)
+                    return fail(c, HFEM_E_MESH, "block (%d, %d) receives more than two element contributions", i, j);
+                blk[(k * 2 + bcount[k]) * 3 + 0] = e;
+                blk[(k * 2 + bcount[k]) * 3 + 1] = a;
+                blk[(k * 2 + bcount[k]) * 3 + 2] = b;
+                bcount[k]++;
+            }
+        }
+    }
+    int rc;
+    CK(cudaSetDevice(c->device));
+    std::vector<int> colface(colidx, colidx + nblk);
+    if ((rc = upload(c, &c->dgnodes, dgnodes, (size_t)ne * d.npv * d.nd)) ||
+        (rc = upload(c, &c->elcon, elcon, (size_t)ne * ndf)) || (rc = upload(c, &c->rowstart, rowstart, (size_t)nf + 1)) ||
+        (rc = upload(c, &c->colidx, colidx, (size_t)nblk)) || (rc = upload(c, &c->blk_src, blk.data(), blk.size())) ||
+        (rc = upload(c, &c->face_src, fsrc.data(), fsrc.size())) ||
+        (rc = upload(c, &c->rowface, rowface.data(), rowface.size())) ||
+        (rc = upload(c, &c->colface, colface.data(), colface.size())))
+        return rc;
+    if ((rc = dalloc(c, &c->Hg, (size_t)nblk * c->bsz * c->bsz)) || (rc = dalloc(c, &c->Rg, (size_t)nf * c->bsz)) ||
+        (rc = dalloc(c, &c->Rr, (size_t)nf * c->bsz)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->h_rowstart.assign(rowstart, rowstart + nf + 1);
+    c->h_colidx.assign(colidx, colidx + nblk);
+    c->have_mesh = true;
+    return 0;
+}
+
+int hfem_set_physics(hfem_ctx* c, const double* param, int tdep, double fc_u, double fc_q, double time) {
+    if (!c || !param) return HFEM_E_ARG;
+    if (!(param[0] > 1.0) || !(param[2] > 0.0) || !(param[3] > 0.0))
+        return fail(c, HFEM_E_ARG, "physicsparam needs gamma > 1, Re > 0, Pr > 0");
+    for (int i = 0; i < 6; i++) c->param[i] = param[i];
+    c->tdep = tdep;
+    c->fc_u = fc_u;
+    c->fc_q = fc_q;
+    c->time = time;
+    c->have_phys = true;
+    return 0;
+}
+
+static int set_solution_common(hfem_ctx* c, const double* udg, const double* uh, const double* sh, cudaMemcpyKind kind) {
+    if (!c || !udg || !uh) return HFEM_E_ARG;
+    const hfem_dims& d = c->dims;
+    const size_t nudg = (size_t)d.ne * d.npv * c->nc, nuh = (size_t)d.nf * c->bsz;
+    int rc;
+    CK(cudaSetDevice(c->device));
+    if (!c->udg) {
+        if ((rc = dalloc(c, &c->udg, nudg)) || (rc = dalloc(c, &c->uh, nuh)) || (rc = dalloc(c, &c->sh, nudg))) return rc;
+    }
+    CK(cudaMemcpyAsync(c->udg, udg, sizeof(double) * nudg, kind, c->stream));
+    CK(cudaMemcpyAsync(c->uh, uh, sizeof(double) * nuh, kind, c->stream));
+    if (sh) CK(cudaMemcpyAsync(c->sh, sh, sizeof(double) * nudg, kind, c->stream));
+    else CK(cudaMemsetAsync(c->sh, 0, sizeof(double) * nudg, c->stream));
+    c->have_sol = true;
+    c->assembled = false;
+    return 0;
+}
+
+int hfem_set_solution(hfem_ctx* c, const double* udg, const double* uh, const double* sh) {
+    int rc = set_solution_common(c, udg, uh, sh, cudaMemcpyHostToDevice);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int hfem_set_solution_device(hfem_ctx* c, const double* udg, const double* uh, const double* sh) {
+    return set_solution_common(c, udg, uh, sh, cudaMemcpyDeviceToDevice);
+}
+
+int hfem_get_solution(hfem_ctx* c, double* udg, double* uh) {
+    if (!c || !c->have_sol) return c ? fail(c, HFEM_E_STATE, "no solution set") : HFEM_E_ARG;
+    const size_t nudg = (size_t)c->dims.ne * c->dims.npv * c->nc, nuh = (size_t)c->dims.nf * c->bsz;
+    if (udg) CK(cudaMemcpyAsync(udg, c->udg, sizeof(double) * nudg, cudaMemcpyDeviceToHost, c->stream));
+    if (uh) CK(cudaMemcpyAsync(uh, c->uh, sizeof(double) * nuh, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int hfem_getq(hfem_ctx* c) {
+    int rc = ready(c);
+    if (rc) return rc;
+    if ((rc = launch_getq(c, nullptr, 0.0))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    flush_timer(c);
+    c->assembled = false;
+    return 0;
+}
+
+int hfem_assemble(hfem_ctx* c, double* rnorm) { return run_assembly(c, true, rnorm); }
+
+int hfem_residual(hfem_ctx* c, double* rnorm) { return run_assembly(c, false, rnorm); }
+
+int hfem_gmres(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters, double* hist,
+               int hist_len) {
+    if (!c) return HFEM_E_ARG;
+    return gmres_impl(c, precond, restart, tol, maxit, conv, iters, hist, hist_len);
+}
+
+int hfem_update(hfem_ctx* c, double alpha) {
+    if (!c) return HFEM_E_ARG;
+    return update_impl(c, alpha);
+}
+
+// solveNonlinearProblem (solvers/dgsolvers.cpp:106-205), damped Newton with the
+// reference's line search: halve alpha (stepping back from the previous trial)
+// while the residual grows, down to alphaMin = 1e-4.
+int hfem_newton(hfem_ctx* c, double newton_tol, int newton_maxiter, int precond, int restart, double gmres_tol,
+                int gmres_maxit, double* hist, int hist_len, int* niter, int* converged) {
+    if (!c) return HFEM_E_ARG;
+    int rc = ready(c);
+    if (rc) return rc;
+    const double alphaMin = 1.0e-4;
+    double rNorm = newton_tol + 1.0;
+    int iter = 0, nh = 0, robust = 0;
+    while (rNorm > newton_tol && iter < newton_maxiter) {
+        iter++;
+        double oldNorm = 0.0;
+        if ((rc = run_assembly(c, true, &oldNorm))) return rc;
+        if (hist && nh < hist_len) hist[nh++] = oldNorm;
+        if (std::isnan(oldNorm) || std::isinf(oldNorm))
+            return fail(c, HFEM_E_SINGULAR, "residual norm of Newton iterate %d is NaN or Inf", iter);
+        int conv = 0, its = 0;
+        if ((rc = gmres_impl(c, precond, restart, gmres_tol, gmres_maxit, &conv, &its, nullptr, 0))) return rc;
+        if (conv == -1) break;
+        if (iter == 1 && oldNorm < newton_tol) {
+            rNorm = oldNorm;
+            break;
+        }
+        double alpha = 1.0;
+        while (true) {
+            if ((rc = update_impl(c, alpha))) return rc;
+            if ((rc = run_assembly(c, false, &rNorm))) return rc;
+            if (std::isnan(rNorm) || std::isinf(rNorm) || (rNorm > oldNorm && rNorm > newton_tol)) {
+                const double a = std::fabs(alpha / 2);
+                alpha = -a;
+                if (a < alphaMin) {
+                    if (robust == 0) {
+                        robust = 1;
+                        alpha = -2.0 * std::fabs(alpha);
+                        if ((rc = update_impl(c, alpha))) return rc;
+                    }
+                    break;
+                }
+            } else {
+                break;
+            }
+        }
+    }
+    if (hist && nh < hist_len) hist[nh++] = rNorm;
+    if (niter) *niter = iter;
+    if (converged) *converged = rNorm < newton_tol ? 1 : 0;
+    return 0;
+}
+
+int hfem_download(hfem_ctx* c, int what, double* host, size_t count) {
+    if (!c || !host) return HFEM_E_ARG;
+    const hfem_dims& d = c->dims;
+    const double* src = nullptr;
+    size_t need = 0;
+    switch (what) {
+        case 0: src = c->Hg; need = (size_t)d.nblocks * c->bsz * c->bsz; break;
+        case 1: src = c->Rg; need = (size_t)d.nf * c->bsz; break;
+        case 2: src = c->Rr; need = (size_t)d.nf * c->bsz; break;
+        case 3: src = c->Ru; need = (size_t)d.ne * c->n; break;
+        case 4: src = c->F; need = (size_t)d.ne * c->n * c->nb; break;
+        case 5: src = c->H; need = (size_t)d.ne * c->nb * c->nb; break;
+        case 6: src = c->Rh; need = (size_t)d.ne * c->nb; break;
+        case 7: src = c->x; need = (size_t)d.nf * c->bsz; break;
+        default: return fail(c, HFEM_E_ARG, "unknown download target %d", what);
+    }
+    if (!src) return fail(c, HFEM_E_STATE, "nothing computed for target %d yet", what);
+    if (count < need) return fail(c, HFEM_E_ARG, "buffer of %zu < %zu entries", count, need);
+    CK(cudaMemcpyAsync(host, src, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int hfem_set_timing(hfem_ctx* c, int on) {
+    if (!c) return HFEM_E_ARG;
+    flush_timer(c);
+    c->timer.on = on != 0;
+    c->timer.acc.clear();
+    return 0;
+}
+
+int hfem_kernel_times(hfem_ctx* c, char* names, size_t names_len, double* ms, int* counts, int max_kernels) {
+    if (!c || !names || !ms) return HFEM_E_ARG;
+    flush_timer(c);
+    std::string s;
+    int i = 0;
+    for (auto& kv : c->timer.acc) {
+        if (i >= max_kernels) break;
+        if (i) s += ";";
+        s += kv.first;
+        ms[i] = kv.second.first;
+        if (counts) counts[i] = kv.second.second;
+        i++;
+    }
+    if (s.size() + 1 > names_len) return fail(c, HFEM_E_ARG, "names buffer too small");
+    std::memcpy(names, s.c_str(), s.size() + 1);
+    return i;
+}
+
+}  // extern "C"

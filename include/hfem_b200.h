@@ -1,0 +1,134 @@
+/*
+ * hfem_b200: C ABI of the B200 (sm_100a) HDG element hot path.
+ *
+ * Drop-in for the serial hot path of exapde/hfem (the reference).  The
+ * reference composes this path at compile/link time rather than through a
+ * plugin ABI; each entry point below names the reference routine it replaces.
+ * All arrays use the reference's layouts (column-major; element-major arrays
+ * are npv x nc x ne etc.), all integers are 0-based int32, all reals float64.
+ * Host pointers are only read/written during the call; device buffers belong
+ * to the context.  Every call returns 0 on success or a negative HFEM_E_* code;
+ * hfem_last_error() gives the message.  Nothing calls exit().
+ */
+#ifndef HFEM_B200_H
+#define HFEM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hfem_ctx hfem_ctx;
+
+enum {
+    HFEM_OK = 0,
+    HFEM_E_ARG = -1,         /* invalid argument or size */
+    HFEM_E_UNSUPPORTED = -2, /* element shape / order without a compiled kernel */
+    HFEM_E_CUDA = -3,        /* CUDA runtime error */
+    HFEM_E_STATE = -4,       /* call made before the data it needs was set */
+    HFEM_E_MESH = -5,        /* connectivity inconsistent (missing CSR block, bad index) */
+    HFEM_E_SINGULAR = -6,    /* singular local matrix */
+    HFEM_E_NOMEM = -7        /* device allocation failed */
+};
+
+/* Sizes of one problem: element (nd, npv nodes, npf nodes per face, nfe faces,
+ * ngv volume and ngf face quadrature points) and mesh (ne elements, nf faces,
+ * nblocks = entries of the face-to-face block CSR). */
+typedef struct {
+    int nd, npv, npf, nfe, ngv, ngf;
+    int ne, nf, nblocks;
+} hfem_dims;
+
+/* Context on CUDA device `device`.  Replaces the struct set-up of
+ * preprocessing/initializestructs.cpp:45-930 (initializeStructs). */
+int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out);
+int hfem_destroy(hfem_ctx* ctx);
+const char* hfem_last_error(const hfem_ctx* ctx);
+
+/* Work on an existing CUDA stream (cudaStream_t passed as void*); NULL = the
+ * context's own stream. */
+int hfem_set_stream(hfem_ctx* ctx, void* stream);
+
+/* Master element tables, as masterstruct holds them
+ * (preprocessing/digasopre.h:109-229, written by mkmasterelement.m):
+ *   shapvt ngv x npv x (nd+1), shapvg npv x ngv x (nd+1),
+ *   shapvgdotshapvl npv^2 x ngv x (nd+1), shapft ngf x npf x nd,
+ *   shapfg npf x ngf x nd, shapfgdotshapfc npf^2 x ngf x nd, perm npf x nfe. */
+int hfem_set_master(hfem_ctx* ctx, const double* shapvt, const double* shapvg, const double* shapvgdotshapvl,
+                    const double* shapft, const double* shapfg, const double* shapfgdotshapfc, const int* perm);
+
+/* Mesh (meshstruct, digasopre.h:231-300) and the face-block CSR (sysstruct
+ * ent2entStart/ent2ent, diagonal block first in every row; produced by the
+ * reference's dmdserial, preprocessing/preprocessing.cpp:14):
+ *   dgnodes npv x nd x ne, elcon (npf*nfe) x ne, t2f nfe x ne,
+ *   ent2entStart nf+1, ent2ent nblocks.
+ * Checks the connectivity the reference asserts (globalassembly.cpp:69-75). */
+int hfem_set_mesh(hfem_ctx* ctx, const double* dgnodes, const int* elcon, const int* t2f,
+                  const int* ent2entStart, const int* ent2ent);
+
+/* Physics: physicsparam = [gamma, eps, Re, Pr, Mach, tau] (compressible
+ * Navier-Stokes, constant tau, constant viscosity), tdep/fc_u/fc_q/time as
+ * appstruct (digasopre.h:7-91).  appname 1 (NS) is the one supported. */
+int hfem_set_physics(hfem_ctx* ctx, const double* physicsparam, int tdep, double fc_u, double fc_q, double time);
+
+/* Solution state sol.UDG (npv x nc x ne), sol.UH (nch x nf*npf) and the time
+ * source sol.SH (npv x nc x ne; may be NULL = zero).  Host pointers. */
+int hfem_set_solution(hfem_ctx* ctx, const double* udg, const double* uh, const double* sh);
+int hfem_get_solution(hfem_ctx* ctx, double* udg, double* uh);
+/* Same, with device pointers already on the context's device. */
+int hfem_set_solution_device(hfem_ctx* ctx, const double* udg, const double* uh, const double* sh);
+
+/* q from (u, uh) on every element.  Replaces getQ
+ * (assembly/elementassembly.cpp:1414-1479) as called by solveProblem
+ * (solvers/dgsolvers.cpp:464-474). */
+int hfem_getq(hfem_ctx* ctx);
+
+/* Element assembly, static condensation and scatter into the face-block
+ * system Hg x = Rg; stores D^-1 Ru and D^-1 F per element.  Replaces
+ * assembleLinearSystem (assembly/globalassembly.cpp:423-556) with
+ * assembleElementMatrixVector (elementassembly.cpp:1481-1499),
+ * schurElementMatrixVector (elementschur.cpp:331-343) and
+ * mapElement2LinearSystem (globalassembly.cpp:8-161).  rnorm (may be NULL)
+ * receives sqrt(sum ||Ru_e||^2 + ||sum Rh_e||^2) as sol.rNorm. */
+int hfem_assemble(hfem_ctx* ctx, double* rnorm);
+
+/* Residual norm only.  Replaces computeResidualNorm (globalassembly.cpp:618-678). */
+int hfem_residual(hfem_ctx* ctx, double* rnorm);
+
+/* Restarted GMRES on Hg x = Rg (x starts at 0), left preconditioning:
+ * precond -1 none, 2 entity-wise block Jacobi (kernel/mkBlockJacobi.m).
+ * Replaces computeOrdering / computePreconditioner / gmres
+ * (solvers/dgsolvers.cpp:16-20, closed in the reference; spec
+ * kernel/gmres_bilu0.m).  conv: 1 converged, 0 max iterations, -1 breakdown.
+ * hist (may be NULL) receives up to hist_len relative residuals. */
+int hfem_gmres(hfem_ctx* ctx, int precond, int restart, double tol, int maxit, int* conv, int* iters,
+               double* hist, int hist_len);
+
+/* uh += alpha x; u += alpha (D^-1 Ru - D^-1 F x_e); q recomputed.
+ * Replaces updateSol / getU (solvers/solutionupdate.cpp:6-98). */
+int hfem_update(hfem_ctx* ctx, double alpha);
+
+/* Damped Newton with line search on the assembled system.  Replaces
+ * solveNonlinearProblem (solvers/dgsolvers.cpp:106-205).  rnorm_hist
+ * receives the residual before each iteration and the final one
+ * (up to hist_len entries); *niter the number of iterations. */
+int hfem_newton(hfem_ctx* ctx, double newton_tol, int newton_maxiter, int precond, int restart, double gmres_tol,
+                int gmres_maxit, double* rnorm_hist, int hist_len, int* niter, int* converged);
+
+/* Download device results for inspection (host buffers of the given length):
+ * what = 0 Hg (nblocks*bsz^2), 1 Rg (nf*bsz), 2 Rr = sum of uncondensed Rh
+ * (nf*bsz), 3 DinvRu (n*ne), 4 DinvF (n*nb*ne), 5 condensed element H
+ * (nb*nb*ne), 6 condensed element Rh (nb*ne), 7 GMRES solution x (nf*bsz). */
+int hfem_download(hfem_ctx* ctx, int what, double* host, size_t count);
+
+/* Per-kernel device time (ms) accumulated since the last reset, when timing
+ * is on.  names receives a ';'-separated list matching ms[]. */
+int hfem_set_timing(hfem_ctx* ctx, int on);
+int hfem_kernel_times(hfem_ctx* ctx, char* names, size_t names_len, double* ms, int* counts, int max_kernels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HFEM_B200_H */
