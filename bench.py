@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Benchmark of the HDG element hot path on B200 (one JSON line on rank 0).
+
+Workload (default): 3D compressible Navier-Stokes HDG, periodic unit cube,
+20^3 hexes split into 6 tetrahedra = 48,000 elements, p = 3 (20 nodes, 5
+conserved variables + gradients), FP64.  One step = one full pass of element
+assembly + static condensation + scatter into the face-block system
+(assembleLinearSystem), with the solution resident on the device.
+
+  metric  assembly+Schur elements/s (FP64), whole job (sum over GPUs)
+  e2e     the same step through the C ABI with the state copied from pinned
+          host memory every step and the residual norm read back
+  roofline of the dominant kernel against the measured FP64 roof
+  cpu_baseline  the reference's own C++ (oracle/_ref/hfem_ref, built from the
+          reference sources) on the host cores, as a reported baseline
+
+``--impl reference`` times only the reference CPU path (all host cores).
+Multi-GPU runs are independent replicas (the path has no data exchange in
+this single-GPU design): one process per GPU, weak scaling, max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "ns3d_p3_48k": dict(kind="ns3d_fourier", n=20, porder=3,
+                        label="3D NS HDG, periodic unit cube 20^3x6 tets = 48000 elements, p=3, Re 400, Mach 0.3"),
+    "ns3d_p3_6k": dict(kind="ns3d_fourier", n=10, porder=3,
+                       label="3D NS HDG, periodic unit cube 10^3x6 tets = 6000 elements, p=3 (profiling size)"),
+    "ns2d_p2_2k": dict(kind="ns2d_vortex", n=32, porder=2,
+                       label="2D NS HDG, periodic [0,10]^2 32x32x2 tris = 2048 elements, p=2, Re 100, Mach 0.5"),
+}
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "hfem_ref")
+
+
+def flops_per_element(prob):
+    """Algorithmic FLOPs of assembly + Schur per element (GEMM and LU structure of the reference)."""
+    m = prob.master
+    nd, npv, npf, nfe, ngv, ngf = m.nd, m.npv, m.npf, m.nfe, m.ngv, m.ngf
+    ncu = nch = nd + 2
+    ndf = npf * nfe
+    n, nb = npv * ncu, nch * ndf
+    vol = (2 * npv * ncu * ngv * (nd + 1) + 2 * npv * (ncu * npv * ncu) * ngv * (nd + 1)
+           + 2 * npv * (ncu * ncu * ndf) * ngv * (nd + 1))
+    face = (2 * npf * npf * (nfe * nch * ncu) * ngf + 2 * npf * npf * (nfe * nch * nch) * ngf
+            + 2 * npf * (nfe * ncu * npv * ncu) * ngf + 2 * npf * (nfe * ncu * ncu * ndf) * ngf)
+    schur = (2.0 / 3.0) * n ** 3 + 2 * n * n * nb + 2 * nb * nb * n + 2 * n * n + 2 * nb * n
+    return dict(element=float(vol + face), schur=float(schur))
+
+
+def bytes_per_element(prob):
+    """Algorithmic HBM bytes per element: inputs read, condensed outputs written (FP64)."""
+    m = prob.master
+    nd, npv, npf, nfe = m.nd, m.npv, m.npf, m.nfe
+    ncu = nch = nd + 2
+    nc = ncu * (nd + 1)
+    n, nb = npv * ncu, nch * npf * nfe
+    return 8.0 * (npv * nc + npv * nd + npf * nfe * nch) + 8.0 * (nb * nb + nb + n * nb + n)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU legs
+def _write_ref_inputs(tmpdir, kind, porder, n):
+    from hfem_b200.gen.problem import make_problem
+    from hfem_b200.gen.refio import write_inputs
+    prob = make_problem(kind, n=n, porder=porder)
+    prefix = os.path.join(tmpdir, "in_")
+    write_inputs(prefix, prob)
+    return prefix, prob.mesh.ne
+
+
+def _run_ref_timing(prefix, nelem, reps):
+    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+    out = subprocess.run([REF_BIN, "timing", prefix, str(nelem), str(reps)], check=True, capture_output=True,
+                         text=True, env=env).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
+def reference_cpu(workload, seconds_per_proc=10.0, procs=None, reps=None):
+    """Reference C++ assembleLinearSystem on the host cores: P independent processes
+    (the reference's MPI driver cannot be built here; its OpenMP is disabled)."""
+    if not os.path.exists(REF_BIN):
+        return None
+    w = WORKLOADS[workload]
+    sample_n = 3
+    procs = procs or max(1, os.cpu_count() or 1)
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix, ne = _write_ref_inputs(tmp, w["kind"], w["porder"], sample_n)
+        calib = _run_ref_timing(prefix, ne, 1)
+        if reps is None:
+            reps = max(1, int(seconds_per_proc / max(calib["seconds"], 1e-3)))
+        results = [None] * procs
+
+        def worker(i):
+            results[i] = _run_ref_timing(prefix, ne, reps)
+
+        th = [threading.Thread(target=worker, args=(i,)) for i in range(procs)]
+        t0 = time.time()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.time() - t0
+    total = sum(r["elems_per_s"] for r in results)
+    return {"value": total, "unit": "elements/s", "cores": procs, "kind": "reference",
+            "single_core_elems_per_s": calib["elems_per_s"],
+            "sample": f"{w['kind']} p={w['porder']} on a {sample_n}^3x6={ne}-element periodic mesh, "
+                      f"{reps} assembleLinearSystem passes in each of {procs} processes ({wall:.1f} s wall)"}
+
+
+# ---------------------------------------------------------------- GPU leg
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    from hfem_b200.core import HDGSolver
+    from hfem_b200.gen.problem import make_problem
+    from hfem_b200.hwpeak import fp64_peak_tflops
+
+    torch.cuda.set_device(local_rank)
+    dev = local_rank
+    w = WORKLOADS[args.workload]
+    prob = make_problem(w["kind"], n=w["n"], porder=w["porder"], **({"seed": rank} if w["kind"] != "ns3d_tgv" else {}))
+    ne = prob.mesh.ne
+    solver = HDGSolver(prob, device=dev)
+    stream = torch.cuda.current_stream()
+    solver.set_stream(stream.cuda_stream)
+    solver.getQ()
+    udg_q, uh0 = solver.get_solution()
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        solver.assembleLinearSystem()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(dev) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    solver.set_timing(True)
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        rnorm = solver.assembleLinearSystem()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    ktimes = solver.kernel_times()
+    solver.set_timing(False)
+    clocks = sampler.stop() if sampler else None
+
+    # e2e: state from pinned host memory every step, residual norm back
+    h_udg = torch.from_numpy(np.ascontiguousarray(udg_q)).pin_memory()
+    h_uh = torch.from_numpy(np.ascontiguousarray(uh0)).pin_memory()
+    h_sh = torch.from_numpy(np.ascontiguousarray(prob.sh)).pin_memory()
+    import ctypes as C
+    lib = solver.lib
+    dp = C.POINTER(C.c_double)
+
+    def e2e_step():
+        rc = lib.hfem_set_solution(solver.h, C.cast(h_udg.data_ptr(), dp), C.cast(h_uh.data_ptr(), dp),
+                                   C.cast(h_sh.data_ptr(), dp))
+        if rc != 0:
+            raise RuntimeError(lib.hfem_last_error(solver.h).decode())
+        return solver.assembleLinearSystem()
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+
+    if dist is not None:
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    solver.close()
+    if rank != 0:
+        return None
+
+    fl = flops_per_element(prob)
+    peak = fp64_peak_tflops(dev)
+    dom = max(("element", "schur"), key=lambda k: ktimes.get(k, (0.0, 1))[0])
+    kms, kcnt = ktimes[dom]
+    avg_launch_s = kms / kcnt * 1e-3
+    achieved = fl[dom] * ne / avg_launch_s / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        tr = json.load(open(tfile)).get(args.workload, {}).get(dom)
+        if tr:
+            traffic = tr["bytes_per_element"] * ne
+    launches = sum(v[1] for v in ktimes.values()) + args.steps   # + the rnorm reduction per step
+    value = world * ne * args.steps / (ms * 1e-3)
+    e2e_value = world * ne * args.steps / (e2e_ms * 1e-3)
+    bpe = bytes_per_element(prob)
+    line = {
+        "metric": "assembly+Schur elements/s (FP64)",
+        "value": value,
+        "unit": "elements/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Fourier-mode flow on a generated periodic tetrahedral mesh)",
+        "config": {"workload": w["label"], "elements_per_gpu": ne, "porder": prob.master.porder,
+                   "local_dofs_D": prob.n_local, "trace_dofs_H": prob.n_trace,
+                   "flops_per_element": fl["element"] + fl["schur"],
+                   "l2": "inputs larger than L2 (UDG 154 MB, 48 GB of per-pass outputs); no flush needed",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "fp64", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "measured in this run: FP64 FMA burst kernel (hfem_fp64_peak)",
+                     "flops_per_launch": fl[dom] * ne, "avg_launch_ms": avg_launch_s * 1e3,
+                     "hbm_view": {"algorithmic_bytes_per_step": bpe * ne,
+                                  "achieved_gbs": bpe * ne / (ms * 1e-3 / args.steps) / 1e9}},
+        "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
+        "e2e": {"value": e2e_value, "unit": "elements/s", "ms_per_step": e2e_ms / args.steps,
+                "h2d_bytes_per_step": int(h_udg.numel() * 8 + h_uh.numel() * 8 + h_sh.numel() * 8),
+                "d2h_bytes_per_step": 8 + 4 * ne},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "rnorm": rnorm,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_cpu(args.workload, seconds_per_proc=args.cpu_seconds)
+    return line
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    if not os.path.exists(REF_BIN):
+        return {"impl": "reference", "unavailable": "oracle/_ref/hfem_ref not built (needs the reference sources)"}
+    w = WORKLOADS[args.workload]
+    procs = max(1, os.cpu_count() or 1)
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix, ne = _write_ref_inputs(tmp, w["kind"], w["porder"], 3)
+        for _ in range(args.warmup):
+            _run_ref_timing(prefix, ne, 1)
+        results = [None] * procs
+
+        def worker(i):
+            results[i] = _run_ref_timing(prefix, ne, args.steps)
+
+        th = [threading.Thread(target=worker, args=(i,)) for i in range(procs)]
+        t0 = time.time()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.time() - t0
+    value = sum(r["elems_per_s"] for r in results)
+    sample = (f"{w['kind']} p={w['porder']} on a 3^3x6={ne}-element periodic mesh, {args.steps} "
+              f"assembleLinearSystem passes per process, {procs} processes")
+    return {"metric": "assembly+Schur elements/s (FP64)", "value": value, "unit": "elements/s", "impl": "reference",
+            "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": w["label"], "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "elements/s", "cores": procs, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hfem", choices=["hfem", "reference"])
+    ap.add_argument("--workload", default="ns3d_p3_48k", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "hfem" else args.warmup
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        line = run_gpu(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -232,7 +232,7 @@ struct ElemSmem {
 };
 
 template <class S>
-__global__ void __launch_bounds__(NT) element_kernel(ElemArgs A) {
+__global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
     constexpr int ND = S::ND, NPV = S::NPV, NPF = S::NPF, NGV = S::NGV, NGF = S::NGF, NFE = S::NFE;
     constexpr int NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, ND1 = S::ND1, N = S::N, NB = S::NB;
     constexpr int NA = S::NA, NQ = S::NQ, NPF2 = NPF * NPF;

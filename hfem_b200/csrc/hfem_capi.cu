@@ -822,4 +822,48 @@ int hfem_kernel_times(hfem_ctx* c, char* names, size_t names_len, double* ms, in
     return i;
 }
 
+// FP64 FMA burst: the compute roof of the FP64 element path on this device.
+__global__ void fp64_burst_kernel(int iters, double seed, double* out) {
+    double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+           a7 = a0 + 7;
+    const double b = 0.999999, c = 1e-7;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+            a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+        }
+    }
+    const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 12345.678) out[0] = s;
+}
+
+int hfem_fp64_peak(int device, double* tflops) {
+    if (!tflops) return HFEM_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return HFEM_E_CUDA;
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double)) != cudaSuccess) return HFEM_E_NOMEM;
+    const int blocks = sms(device) * 8, threads = 256, iters = 2048;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    double best = 0.0;
+    for (int r = 0; r < 5; r++) {
+        cudaEventRecord(a);
+        fp64_burst_kernel<<<blocks, threads>>>(iters, 1.0 + r, d);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+        if (r > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
+    *tflops = best;
+    return 0;
+}
+
 }  // extern "C"

@@ -123,9 +123,14 @@ int hfem_newton(hfem_ctx* ctx, double newton_tol, int newton_maxiter, int precon
 int hfem_download(hfem_ctx* ctx, int what, double* host, size_t count);
 
 /* Per-kernel device time (ms) accumulated since the last reset, when timing
- * is on.  names receives a ';'-separated list matching ms[]. */
+ * is on (measurement helper, no counterpart in the reference).  names
+ * receives a ';'-separated list matching ms[]; returns the number of kernels. */
 int hfem_set_timing(hfem_ctx* ctx, int on);
 int hfem_kernel_times(hfem_ctx* ctx, char* names, size_t names_len, double* ms, int* counts, int max_kernels);
+
+/* Measurement helper (no counterpart in the reference): FP64 FMA throughput of
+ * `device` in TFLOP/s from a burst kernel, the compute roof of this FP64 path. */
+int hfem_fp64_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }

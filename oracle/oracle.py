@@ -189,7 +189,8 @@ def run_reference(prob, mode="assemble", ndump=0, newton=None, workdir=None):
     else:
         cmd = [REF_BIN, "newton", inp, out, str(newton["maxiter"]), str(newton["precond"]),
                str(newton["restart"]), repr(newton["tol"])]
-    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
+    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, env=env)
 
     def ld(name):
         return np.fromfile(out + name + ".bin", dtype=np.float64)
