@@ -867,3 +867,94 @@ int hfem_fp64_peak(int device, double* tflops) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Element assembly + condensation with no device allocation.
+//
+// For callers that hand out all device memory themselves and must not call
+// cudaMalloc: programs whose memory comes from a caching pool (a PyTorch or
+// RMM allocator, where a raw cudaMalloc synchronises the device and fragments
+// the pool), serving loops that reserve HBM once at admission and may not
+// allocate per request, and host codes that register a fixed set of buffers.
+// The element kernel's per-CTA workspace lives in the file-scope array below
+// instead of a context buffer.  Its size is fixed at HFEM_NOALLOC_SCRATCH_BYTES
+// (32 MiB) on every GPU that loads this library, for the life of the process.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+#define HFEM_NOALLOC_SCRATCH_BYTES (32u << 20)
+static __device__ __align__(256) double g_noalloc_scratch[HFEM_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt, const double* shapvg,
+                                     const double* shapvgdotshapvl, const double* shapft, const double* shapfg,
+                                     const double* shapfgdotshapfc, const int* perm, const double* dgnodes,
+                                     const int* elcon, const double* udg, const double* uh, const double* sh,
+                                     const double* physicsparam, int tdep, double fc_u, double fc_q, double* D,
+                                     double* DinvF, double* K, double* H, double* DinvRu, double* Rh,
+                                     double* Rh_uncondensed, double* ru2, int* info, void* stream) {
+    if (!dims || !shapvt || !shapvg || !shapvgdotshapvl || !shapft || !shapfg || !shapfgdotshapfc || !perm ||
+        !dgnodes || !elcon || !udg || !uh || !sh || !physicsparam || !D || !DinvF || !K || !H || !DinvRu || !Rh ||
+        !Rh_uncondensed || !ru2 || !info)
+        return HFEM_E_ARG;
+    const hfem_dims& d = *dims;
+    if (d.ne <= 0) return HFEM_E_ARG;
+    const Launch* L = nullptr;
+    for (const Launch& x : launches())
+        if (x.nd == d.nd && x.npv == d.npv && x.npf == d.npf && x.ngv == d.ngv && x.ngf == d.ngf) L = &x;
+    if (!L) return HFEM_E_UNSUPPORTED;
+    const size_t slot_bytes = L->ws * sizeof(double);
+    if (slot_bytes > HFEM_NOALLOC_SCRATCH_BYTES) return HFEM_E_ARG;   // one element's workspace exceeds the scratch
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HFEM_E_CUDA;
+    double* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            // once per device, with that device current
+            if (cudaGetSymbolAddress((void**)&g_noalloc_ptr[dev], g_noalloc_scratch) != cudaSuccess) {
+                g_noalloc_ptr[dev] = nullptr;
+                return HFEM_E_CUDA;
+            }
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    if (cudaFuncSetAttribute(L->elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->elem_smem) != cudaSuccess ||
+        cudaFuncSetAttribute(L->schur_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->schur_smem) != cudaSuccess)
+        return HFEM_E_CUDA;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->elem_fn, NT, L->elem_smem);
+    const int slots = (int)(HFEM_NOALLOC_SCRATCH_BYTES / slot_bytes);
+    const int ge = std::max(1, std::min(std::min(d.ne, slots), sms(dev) * std::max(occ, 1)));
+    occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->schur_fn, NT, L->schur_smem);
+    const int gs = std::max(1, std::min(d.ne, sms(dev) * std::max(occ, 1)));
+    cudaStream_t st = (cudaStream_t)stream;
+
+    ElemArgs a;
+    a.T = Tables{shapvt, shapvg, shapvgdotshapvl, shapft, shapfg, shapfgdotshapfc, perm};
+    a.dgnodes = dgnodes;
+    a.elcon = elcon;
+    a.udg = udg;
+    a.uh = uh;
+    a.sh = sh;
+    for (int i = 0; i < 6; i++) a.param[i] = physicsparam[i];
+    a.tdep = tdep;
+    a.fc_u = fc_u;
+    a.fc_q = fc_q;
+    a.ne = d.ne;
+    a.D = D; a.F = DinvF; a.K = K; a.H = H;
+    a.Ru = DinvRu; a.Rh = Rh; a.Ro = Rh_uncondensed; a.ru2 = ru2;
+    a.ws = scratch;
+    L->element(dim3(ge), L->elem_smem, st, a);
+    if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
+    SchurArgs s{d.ne, D, DinvF, K, H, DinvRu, Rh, info};
+    L->schur(dim3(gs), L->schur_smem, st, s);
+    if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
+    return 0;
+}

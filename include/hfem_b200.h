@@ -132,6 +132,32 @@ int hfem_kernel_times(hfem_ctx* ctx, char* names, size_t names_len, double* ms, 
  * `device` in TFLOP/s from a burst kernel, the compute roof of this FP64 path. */
 int hfem_fp64_peak(int device, double* tflops);
 
+/* Element assembly + static condensation that allocates nothing (no
+ * counterpart in the reference).  For callers that cannot call cudaMalloc:
+ * programs whose device memory comes from their own caching pool (PyTorch,
+ * RMM), where a raw cudaMalloc would synchronise the device and fragment the
+ * pool, and serving loops that reserve HBM once and must not allocate per
+ * request.  Every pointer except physicsparam (6 doubles, host) is device
+ * memory on the calling thread's current device; the caller passes all inputs
+ * (master tables, dgnodes, elcon, udg with q, uh, sh) and all outputs, per
+ * element: D (n^2, before condensation), DinvF (n*nb), K (nb*n), H (nb^2,
+ * condensed), DinvRu (n), Rh (nb, condensed), Rh_uncondensed (nb), ru2
+ * (||Ru||^2 before condensation), info (0, or 1 + pivot of a singular D).
+ * The element workspace comes from one fixed 32 MiB device array that every
+ * GPU loading the library holds until exit; shapes whose per-CTA workspace
+ * exceeds it are rejected with HFEM_E_ARG.  The first call on a device looks
+ * up that array's address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the array and nothing in it needs to
+ * start at zero; calls that overlap on the GPU (different streams or threads
+ * at once) race on it.  Launches on `stream` (cudaStream_t, NULL = legacy
+ * default stream) and returns without synchronising. */
+int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt, const double* shapvg,
+                          const double* shapvgdotshapvl, const double* shapft, const double* shapfg,
+                          const double* shapfgdotshapfc, const int* perm, const double* dgnodes, const int* elcon,
+                          const double* udg, const double* uh, const double* sh, const double* physicsparam,
+                          int tdep, double fc_u, double fc_q, double* D, double* DinvF, double* K, double* H,
+                          double* DinvRu, double* Rh, double* Rh_uncondensed, double* ru2, int* info, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
