@@ -18,6 +18,7 @@
 #include "../../include/hfem_b200.h"
 #include "elem_kernels.cuh"
 #include "krylov_kernels.cuh"
+#include "schur_kernels.cuh"
 
 using namespace hfem;
 
@@ -39,6 +40,42 @@ struct KernelTimer {
     X(3, 10, 6, 14, 6)          \
     X(3, 20, 10, 24, 12)
 
+// GEMM tile choices per shape (m-tiles, n-tiles per warp, warps): g1 for D^-1 F
+// (n x nb, K = n), g2 for H - K D^-1 F (nb x nb, K = n).
+template <class S> struct SchurCfg;
+template <> struct SchurCfg<Shape<2, 3, 2, 3, 2>> { using g1 = GemmCfg<2, 3, 1>; using g2 = GemmCfg<3, 3, 1>; };
+template <> struct SchurCfg<Shape<2, 6, 3, 6, 3>> { using g1 = GemmCfg<3, 5, 1>; using g2 = GemmCfg<5, 5, 1>; };
+template <> struct SchurCfg<Shape<2, 10, 4, 12, 4>> { using g1 = GemmCfg<5, 3, 2>; using g2 = GemmCfg<6, 3, 2>; };
+template <> struct SchurCfg<Shape<2, 15, 5, 16, 5>> { using g1 = GemmCfg<4, 4, 2>; using g2 = GemmCfg<4, 4, 2>; };
+template <> struct SchurCfg<Shape<3, 4, 3, 4, 3>> { using g1 = GemmCfg<3, 4, 2>; using g2 = GemmCfg<4, 4, 2>; };
+template <> struct SchurCfg<Shape<3, 10, 6, 14, 6>> { using g1 = GemmCfg<7, 3, 5>; using g2 = GemmCfg<5, 3, 5>; };
+template <> struct SchurCfg<Shape<3, 20, 10, 24, 12>> { using g1 = GemmCfg<5, 5, 5>; using g2 = GemmCfg<5, 5, 5>; };
+
+struct GemmLaunch {
+    int bm, bn, threads;
+    size_t smem;
+    const void* fn;
+    void (*run)(cudaStream_t, int, int, int, int, double, const double*, int, long long, const double*, int,
+                long long, double, double*, int, long long);
+};
+
+template <class G, int MT, int WN, int NW>
+void run_gemm(cudaStream_t st, int batch, int M, int N, int K, double alpha, const double* A, int lda, long long sA,
+              const double* B, int ldb, long long sB, double beta, double* C, int ldc, long long sC) {
+    const int tiles = ((M + G::BM - 1) / G::BM) * ((N + G::BN - 1) / G::BN);
+    batched_dgemm_kernel<MT, WN, NW><<<(unsigned)(tiles * batch), G::THREADS, G::SMEM, st>>>(
+        M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
+}
+
+template <class G> struct GemmParams;
+template <int MT, int WN, int NW> struct GemmParams<GemmCfg<MT, WN, NW>> {
+    static GemmLaunch make() {
+        using G = GemmCfg<MT, WN, NW>;
+        return GemmLaunch{G::BM, G::BN, G::THREADS, G::SMEM, (const void*)batched_dgemm_kernel<MT, WN, NW>,
+                          run_gemm<G, MT, WN, NW>};
+    }
+};
+
 struct Launch {
     int nd, npv, npf, ngv, ngf;
     size_t ws;                  // workspace doubles per CTA slot
@@ -46,8 +83,16 @@ struct Launch {
     void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
     void (*schur)(dim3, size_t, cudaStream_t, const SchurArgs&);
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
-    const void *elem_fn, *schur_fn, *q_fn;
+    void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
+    int inv_threads;
+    const void *elem_fn, *schur_fn, *q_fn, *inv_fn;
+    GemmLaunch g1, g2;
 };
+
+template <int N>
+void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info) {
+    inverse_kernel<N><<<g, InvThreads<N>::value, 0, st>>>(ne, D, Ru, info);
+}
 
 template <class S>
 void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel<S><<<g, NT, sm, st>>>(a); }
@@ -70,6 +115,11 @@ Launch make_launch() {
     L.elem_fn = (const void*)element_kernel<S>;
     L.schur_fn = (const void*)schur_kernel<S::N, S::NB>;
     L.q_fn = (const void*)getq_kernel<S>;
+    L.inverse = launch_inverse<S::N>;
+    L.inv_threads = InvThreads<S::N>::value;
+    L.inv_fn = (const void*)inverse_kernel<S::N>;
+    L.g1 = GemmParams<typename SchurCfg<S>::g1>::make();
+    L.g2 = GemmParams<typename SchurCfg<S>::g2>::make();
     return L;
 }
 
@@ -92,7 +142,7 @@ struct hfem_ctx {
     cudaStream_t own = nullptr, stream = nullptr;
     std::string err;
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
-    int grid_elem = 0, grid_schur = 0;
+    int grid_elem = 0, grid_schur = 0, grid_inv = 0;
     // master tables
     double *shapvt = nullptr, *shapvg = nullptr, *svsv = nullptr, *shapft = nullptr, *shapfg = nullptr, *sfsf = nullptr;
     int* perm = nullptr;
@@ -109,6 +159,7 @@ struct hfem_ctx {
     double *udg = nullptr, *uh = nullptr, *sh = nullptr;
     // assembly outputs and workspace
     double *D = nullptr, *F = nullptr, *K = nullptr, *H = nullptr, *Ru = nullptr, *Rh = nullptr, *Ro = nullptr;
+    double* DinvF = nullptr;
     double *ru2 = nullptr, *Hg = nullptr, *Rg = nullptr, *Rr = nullptr, *rnorm = nullptr, *ws = nullptr;
     int* info = nullptr;
     // Krylov
@@ -207,6 +258,7 @@ int ensure_assembly_buffers(hfem_ctx* c) {
     int rc = 0;
     if ((rc = dalloc(c, &c->D, ne * n * n))) return rc;
     if ((rc = dalloc(c, &c->F, ne * n * nb))) return rc;
+    if ((rc = dalloc(c, &c->DinvF, ne * n * nb))) return rc;
     if ((rc = dalloc(c, &c->K, ne * nb * n))) return rc;
     if ((rc = dalloc(c, &c->H, ne * nb * nb))) return rc;
     if ((rc = dalloc(c, &c->Ru, ne * n))) return rc;
@@ -259,7 +311,7 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
     int rc = ready(c);
     if (rc) return rc;
     if ((rc = ensure_assembly_buffers(c))) return rc;
-    const dim3 ge(c->grid_elem), gs(c->grid_schur);
+    const dim3 ge(c->grid_elem);
     {
         Timed t(c, "element");
         c->L->element(ge, c->L->elem_smem, c->stream, elem_args(c));
@@ -267,11 +319,29 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
     }
     ScatterArgs sa = scatter_args(c);
     if (matrix) {
-        SchurArgs s{c->dims.ne, c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->info};
+        const int ne = c->dims.ne, n = c->n, nb = c->nb;
         {
-            Timed t(c, "schur");
-            c->L->schur(gs, c->L->schur_smem, c->stream, s);
-            if ((rc = check_launch(c, "schur"))) return rc;
+            Timed t(c, "inverse");
+            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
+            if ((rc = check_launch(c, "inverse"))) return rc;
+        }
+        {
+            Timed t(c, "gemm_DinvF");
+            c->L->g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb, 0.0,
+                         c->DinvF, n, (long long)n * nb);
+            if ((rc = check_launch(c, "gemm_DinvF"))) return rc;
+        }
+        {
+            Timed t(c, "gemm_schur");
+            c->L->g2.run(c->stream, ne, nb, nb, n, -1.0, c->K, nb, (long long)nb * n, c->DinvF, n, (long long)n * nb,
+                         1.0, c->H, nb, (long long)nb * nb);
+            if ((rc = check_launch(c, "gemm_schur"))) return rc;
+        }
+        {
+            Timed t(c, "gemv_Rh");
+            batched_dgemv_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(ne, nb, n, -1.0, c->K, (long long)nb * n,
+                                                                           c->Ru, n, c->Rh, nb);
+            if ((rc = check_launch(c, "gemv_Rh"))) return rc;
         }
         {
             Timed t(c, "scatter_H");
@@ -315,7 +385,7 @@ int launch_getq(hfem_ctx* c, const double* duh, double alpha) {
     q.fc_q = c->fc_q;
     q.ne = c->dims.ne;
     q.DinvRu = duh ? c->Ru : nullptr;
-    q.DinvF = duh ? c->F : nullptr;
+    q.DinvF = duh ? c->DinvF : nullptr;
     q.duh = duh;
     q.alpha = alpha;
     Timed t(c, duh ? "update" : "getq");
@@ -520,6 +590,11 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.schur_fn, NT, L.schur_smem);
     c->grid_schur = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
+    cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
+    cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
+    occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.inv_fn, L.inv_threads, 0);
+    c->grid_inv = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
     if (cudaMalloc(&c->rnorm, sizeof(double)) != cudaSuccess) {
         cudaStreamDestroy(c->own);
         delete c;
@@ -541,7 +616,7 @@ int hfem_destroy(hfem_ctx* c) {
     cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm, c->dgnodes, c->elcon,
                     c->rowstart, c->colidx, c->blk_src, c->face_src, c->rowface, c->colface, c->udg, c->uh, c->sh,
-                    c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws,
+                    c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -783,7 +858,7 @@ int hfem_download(hfem_ctx* c, int what, double* host, size_t count) {
         case 1: src = c->Rg; need = (size_t)d.nf * c->bsz; break;
         case 2: src = c->Rr; need = (size_t)d.nf * c->bsz; break;
         case 3: src = c->Ru; need = (size_t)d.ne * c->n; break;
-        case 4: src = c->F; need = (size_t)d.ne * c->n * c->nb; break;
+        case 4: src = c->DinvF; need = (size_t)d.ne * c->n * c->nb; break;
         case 5: src = c->H; need = (size_t)d.ne * c->nb * c->nb; break;
         case 6: src = c->Rh; need = (size_t)d.ne * c->nb; break;
         case 7: src = c->x; need = (size_t)d.nf * c->bsz; break;

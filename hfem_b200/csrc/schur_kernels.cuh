@@ -1,0 +1,205 @@
+// Static condensation on sm_100a, FP64 (restating elementschur.cpp:6-329):
+//   1. inverse_kernel: D^-1 and D^-1 Ru by Gauss-Jordan with partial pivoting,
+//      register-resident (one thread owns one row of [D | Ru]);
+//   2. batched_dgemm: D^-1 F and H - K (D^-1 F) on the FP64 tensor cores
+//      (mma.sync m8n8k4 f64), one CTA per 40-row stripe of one element;
+//   3. batched_dgemv: Rh - K (D^-1 Ru).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hfem {
+
+// ------------------------------------------------------------ inverse
+// Gauss-Jordan on the rows of [D | Ru] with the pivot column rotated into
+// register 0 after every step, so each thread only ever indexes its row with
+// compile-time constants.  Row pivot[k] is chosen at step k (first row of
+// maximal |.| among rows not yet used, the LAPACK idamax rule).  With X the
+// in-place result, D^-1(k, l) = X(pivot[k], pivot[l]) and (D^-1 Ru)(k) is the
+// extra column of row pivot[k].  Writes D^-1 over D and D^-1 Ru over Ru.
+template <int N>
+struct InvThreads {
+    static constexpr int value = ((N + 31) / 32) * 32;
+};
+
+template <int N>
+__global__ void __launch_bounds__(InvThreads<N>::value) inverse_kernel(int ne, double* __restrict__ D,
+                                                                       double* __restrict__ Ru, int* __restrict__ info) {
+    constexpr int NTH = InvThreads<N>::value;
+    constexpr int NW = NTH / 32;
+    __shared__ double prow[N + 1];
+    __shared__ double wv[NW];
+    __shared__ int wi[NW];
+    __shared__ int kstep[N];
+    __shared__ int s_q;
+    const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
+    for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+        double r[N + 1];
+        double* De = D + (size_t)e * N * N;
+        if (i < N) {
+#pragma unroll
+            for (int j = 0; j < N; j++) r[j] = De[i + N * j];
+            r[N] = Ru[(size_t)e * N + i];
+        }
+        bool used = i >= N;
+        int mystep = -1;
+        int bad = 0;
+        for (int k = 0; k < N; k++) {
+            double v = used ? -1.0 : fabs(r[0]);
+            int vi = used ? N : i;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, v, o);
+                const int oi = __shfl_down_sync(0xffffffffu, vi, o);
+                if (ov > v || (ov == v && oi < vi)) { v = ov; vi = oi; }
+            }
+            if (lane == 0) { wv[warp] = v; wi[warp] = vi; }
+            __syncthreads();
+            if (i == 0) {
+                double b = wv[0];
+                int q = wi[0];
+                for (int w = 1; w < NW; w++)
+                    if (wv[w] > b || (wv[w] == b && wi[w] < q)) { b = wv[w]; q = wi[w]; }
+                s_q = (b > 0.0) ? q : -1;
+            }
+            __syncthreads();
+            const int q = s_q;
+            if (q < 0) { bad = k + 1; break; }
+            if (i == q) {
+                const double inv = 1.0 / r[0];
+#pragma unroll
+                for (int j = 0; j < N - 1; j++) r[j] = r[j + 1] * inv;
+                r[N - 1] = inv;
+                r[N] *= inv;
+#pragma unroll
+                for (int j = 0; j <= N; j++) prow[j] = r[j];
+                used = true;
+                mystep = k;
+                kstep[i] = k;
+            }
+            __syncthreads();
+            if (i != q && i < N) {
+                const double f = r[0];
+#pragma unroll
+                for (int j = 0; j < N - 1; j++) r[j] = fma(-f, prow[j], r[j + 1]);
+                r[N - 1] = -f * prow[N - 1];
+                r[N] = fma(-f, prow[N], r[N]);
+            }
+        }
+        if (bad) {
+            if (i == 0) info[e] = bad;
+            __syncthreads();
+            continue;
+        }
+        __syncthreads();
+        if (i < N) {
+            // row i of X is row mystep of D^-1; column m of X is column kstep[m]
+#pragma unroll
+            for (int m = 0; m < N; m++) De[mystep + N * kstep[m]] = r[m];
+            Ru[(size_t)e * N + mystep] = r[N];
+        }
+        if (i == 0) info[e] = 0;
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ FP64 mma GEMM
+// D(8x8) += A(8x4, row) * B(4x8, col); lane l holds A(l/4, l%4), B(l%4, l/4),
+// C(l/4, 2(l%4)) and C(l/4, 2(l%4)+1).
+__device__ __forceinline__ void dmma8x8x4(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+// C_e = beta C_e + alpha A_e B_e for e in [0, batch), column-major, batch strides
+// sA, sB, sC.  CTA: NW warps, tile BM = 8*MT rows x BN = 8*WN*NW columns; warp w
+// owns n-tiles [w*WN, (w+1)*WN) of all MT m-tiles.  K staged 20 deep; shared
+// leading dimensions (A: 8*MT padded to 4 mod 16 doubles, B: 20) make the
+// fragment loads bank-conflict free.  Grid: ceil(M/BM) * ceil(N/BN) * batch CTAs,
+// element-major (the tiles of one element run together and share it in L2).
+template <int MT, int WN, int NW>
+struct GemmCfg {
+    static constexpr int BM = 8 * MT, BN = 8 * WN * NW, BK = 20;
+    static constexpr int LDA = ((BM + 11) / 16) * 16 + 4;     // >= BM, == 4 (mod 16)
+    static constexpr int LDB = BK;
+    static constexpr int THREADS = 32 * NW;
+    static constexpr size_t SMEM = sizeof(double) * ((size_t)LDA * BK + (size_t)LDB * BN);
+};
+
+template <int MT, int WN, int NW>
+__global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, int K, double alpha,
+                                                                const double* __restrict__ A, int lda, long long sA,
+                                                                const double* __restrict__ B, int ldb, long long sB,
+                                                                double beta, double* __restrict__ C, int ldc,
+                                                                long long sC) {
+    using G = GemmCfg<MT, WN, NW>;
+    extern __shared__ __align__(16) double gsm[];
+    double* As = gsm;                       // As[m + LDA * k]
+    double* Bs = gsm + G::LDA * G::BK;      // Bs[k + LDB * n]
+    const int tilesM = (M + G::BM - 1) / G::BM, tilesN = (N + G::BN - 1) / G::BN;
+    const int e = blockIdx.x / (tilesM * tilesN), tile = blockIdx.x % (tilesM * tilesN);
+    const int m0 = (tile % tilesM) * G::BM, n0 = (tile / tilesM) * G::BN;
+    const double* Ae = A + (size_t)e * sA;
+    const double* Be = B + (size_t)e * sB;
+    double* Ce = C + (size_t)e * sC;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gr = lane >> 2, gc = lane & 3;
+    double acc[MT][WN][2];
+#pragma unroll
+    for (int a = 0; a < MT; a++)
+#pragma unroll
+        for (int b = 0; b < WN; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += G::BK) {
+        __syncthreads();
+        for (int t = tid; t < G::BM * G::BK; t += G::THREADS) {
+            const int m = t % G::BM, k = t / G::BM;
+            As[m + G::LDA * k] = (m0 + m < M && k0 + k < K) ? Ae[(m0 + m) + (size_t)lda * (k0 + k)] : 0.0;
+        }
+        for (int t = tid; t < G::BK * G::BN; t += G::THREADS) {
+            const int k = t % G::BK, n = t / G::BK;
+            Bs[k + G::LDB * n] = (n0 + n < N && k0 + k < K) ? Be[(k0 + k) + (size_t)ldb * (n0 + n)] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < G::BK; ks += 4) {
+            double af[MT], bf[WN];
+#pragma unroll
+            for (int a = 0; a < MT; a++) af[a] = As[(8 * a + gr) + G::LDA * (ks + gc)];
+#pragma unroll
+            for (int b = 0; b < WN; b++) bf[b] = Bs[(ks + gc) + G::LDB * (8 * (warp * WN + b) + gr)];
+#pragma unroll
+            for (int a = 0; a < MT; a++)
+#pragma unroll
+                for (int b = 0; b < WN; b++) dmma8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < MT; a++)
+#pragma unroll
+        for (int b = 0; b < WN; b++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int m = m0 + 8 * a + gr, n = n0 + 8 * (warp * WN + b) + 2 * gc + h;
+                if (m < M && n < N) {
+                    double* c = &Ce[m + (size_t)ldc * n];
+                    *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[a][b][h];
+                }
+            }
+}
+
+// y_e = y_e + alpha A_e x_e   (A_e: M x K column-major)
+__global__ void batched_dgemv_kernel(int batch, int M, int K, double alpha, const double* __restrict__ A,
+                                     long long sA, const double* __restrict__ x, long long sx, double* __restrict__ y,
+                                     long long sy) {
+    const long long total = (long long)batch * M;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int e = (int)(t / M), r = (int)(t % M);
+        const double* Ae = A + (size_t)e * sA;
+        const double* xe = x + (size_t)e * sx;
+        double s = 0.0;
+        for (int k = 0; k < K; k++) s += Ae[r + (size_t)M * k] * xe[k];
+        y[(size_t)e * sy + r] += alpha * s;
+    }
+}
+
+}  // namespace hfem
