@@ -13,9 +13,12 @@ namespace hfem {
 // Gauss-Jordan on the rows of [D | Ru] with the pivot column rotated into
 // register 0 after every step, so each thread only ever indexes its row with
 // compile-time constants.  Row pivot[k] is chosen at step k (first row of
-// maximal |.| among rows not yet used, the LAPACK idamax rule).  With X the
-// in-place result, D^-1(k, l) = X(pivot[k], pivot[l]) and (D^-1 Ru)(k) is the
-// extra column of row pivot[k].  Writes D^-1 over D and D^-1 Ru over Ru.
+// maximal |.| among rows not yet used, the LAPACK idamax rule).  Slot k of the
+// in-place result X holds the augmented column of row pivot[k], so with
+// P e_k = e_pivot[k]:  X = P D^-1 P, i.e. D^-1(k, l) = X(pivot[k], step(l)) where
+// step(l) is the step at which row l pivoted; the thread of row pivot[k] writes
+// its register m to D^-1(k, pivot[m]).  (D^-1 Ru)(k) is the extra column of row
+// pivot[k].  Writes D^-1 over D and D^-1 Ru over Ru.
 template <int N>
 struct InvThreads {
     static constexpr int value = ((N + 31) / 32) * 32;
@@ -29,7 +32,7 @@ __global__ void __launch_bounds__(InvThreads<N>::value) inverse_kernel(int ne, d
     __shared__ double prow[N + 1];
     __shared__ double wv[NW];
     __shared__ int wi[NW];
-    __shared__ int kstep[N];
+    __shared__ int qrow[N];
     __shared__ int s_q;
     const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
     for (int e = blockIdx.x; e < ne; e += gridDim.x) {
@@ -74,7 +77,7 @@ __global__ void __launch_bounds__(InvThreads<N>::value) inverse_kernel(int ne, d
                 for (int j = 0; j <= N; j++) prow[j] = r[j];
                 used = true;
                 mystep = k;
-                kstep[i] = k;
+                qrow[k] = i;
             }
             __syncthreads();
             if (i != q && i < N) {
@@ -92,9 +95,9 @@ __global__ void __launch_bounds__(InvThreads<N>::value) inverse_kernel(int ne, d
         }
         __syncthreads();
         if (i < N) {
-            // row i of X is row mystep of D^-1; column m of X is column kstep[m]
+            // row i of X is row mystep of D^-1; column m of X is column qrow[m]
 #pragma unroll
-            for (int m = 0; m < N; m++) De[mystep + N * kstep[m]] = r[m];
+            for (int m = 0; m < N; m++) De[mystep + N * qrow[m]] = r[m];
             Ru[(size_t)e * N + mystep] = r[N];
         }
         if (i == 0) info[e] = 0;
