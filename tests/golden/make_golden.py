@@ -1,0 +1,65 @@
+"""Generates the golden fixtures in this folder from the reference's own C++.
+
+Runs oracle/_ref/hfem_ref (the reference's serial hot path compiled from its
+sources by oracle/Makefile; needs the reference tree) on small seeded problems
+and stores its outputs next to the generated inputs:
+
+    python tests/golden/make_golden.py
+
+Each fixture holds the inputs (so the CPU tests also pin the generator) and
+the reference outputs: q from getQ, Hg / Rg / Rr, D^-1 Ru, D^-1 F, rNorm and the
+pre-condensation blocks of the first elements; large 3D arrays are stored as
+fixed random projections instead of in full.  The Newton fixture holds the
+reference driver's residual history and GMRES iteration counts.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from hfem_b200.gen.problem import ns2d_vortex, ns3d_fourier  # noqa: E402
+from oracle import run_reference  # noqa: E402
+
+CASES = {
+    "ns2d_p1_n3": lambda: ns2d_vortex(n=3, porder=1),
+    "ns2d_p2_n3": lambda: ns2d_vortex(n=3, porder=2),
+    "ns2d_p3_n3": lambda: ns2d_vortex(n=3, porder=3),
+    "ns3d_p1_n3": lambda: ns3d_fourier(n=3, porder=1),
+    "ns3d_p3_n3": lambda: ns3d_fourier(n=3, porder=3),
+}
+FULL_LIMIT = 400_000          # store arrays up to this many entries in full
+
+
+
+def squeeze(name, a):
+    a = np.asarray(a)
+    if a.size <= FULL_LIMIT:
+        return {name: a}
+    p = np.random.default_rng(20261203).standard_normal((8, a.size))
+    return {name + "_proj": p @ a.ravel(), name + "_absmax": np.array([np.max(np.abs(a))])}
+
+
+def main():
+    for key, make in CASES.items():
+        prob = make()
+        ref = run_reference(prob, ndump=2)
+        out = dict(udg_in=prob.udg, uh_in=prob.uh, dgnodes=prob.mesh.dgnodes, elcon=prob.mesh.elcon,
+                   rnorm=np.array([ref["rnorm"]]))
+        for k in ("udg", "Hg", "Rg", "Rr", "DinvRu", "DinvF", "eD", "eF", "eK", "eH", "eRu", "eRh"):
+            out.update(squeeze(k, ref[k]))
+        np.savez_compressed(os.path.join(HERE, key + ".npz"), **out)
+        print(key, {k: v.shape for k, v in out.items()})
+    prob = ns2d_vortex(n=4, porder=2)
+    ref = run_reference(prob, mode="newton", newton=dict(maxiter=2, precond=2, restart=50, tol=1e-10))
+    np.savez_compressed(os.path.join(HERE, "ns2d_p2_n4_newton.npz"), rnorm_hist=ref["rnorm_hist"],
+                        gmres_iters=ref["gmres_iters"], udg=ref["udg"], uh=ref["uh"])
+    print("newton", ref["rnorm_hist"], ref["gmres_iters"])
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,102 @@
+"""CPU: the oracle restatement against fixtures made by the reference's own C++.
+
+The fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py with
+oracle/_ref/hfem_ref) hold seeded inputs and the reference's outputs.  These
+tests pin (1) the input generator: regenerated inputs equal the stored ones, and
+(2) the oracle: on the stored inputs it reproduces the reference's q, element
+blocks, Hg, Rg, Rr, D^-1 Ru, D^-1 F and rNorm within 1e-12 relative (residual
+vectors: 1e-12 of the scale of the terms that cancel in them).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from hfem_b200.gen.problem import ns2d_vortex, ns3d_fourier
+from oracle import Oracle
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = {
+    "ns2d_p1_n3": lambda: ns2d_vortex(n=3, porder=1),
+    "ns2d_p2_n3": lambda: ns2d_vortex(n=3, porder=2),
+    "ns2d_p3_n3": lambda: ns2d_vortex(n=3, porder=3),
+    "ns3d_p1_n3": lambda: ns3d_fourier(n=3, porder=1),
+    "ns3d_p3_n3": lambda: ns3d_fourier(n=3, porder=3),
+}
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.ravel(a) - np.ravel(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+def compare(name, got, g, tol=1e-12, scale=None):
+    if name in g:
+        ref = g[name]
+        if scale is None:
+            assert rel(got, ref) < tol, (name, rel(got, ref))
+        else:
+            assert np.max(np.abs(np.ravel(got) - ref)) <= tol * scale, name
+    else:
+        p = np.random.default_rng(20261203).standard_normal((8, np.size(got)))
+        proj = p @ np.ravel(got)
+        assert np.max(np.abs(proj - g[name + "_proj"])) <= tol * g[name + "_absmax"][0] * np.sqrt(np.size(got)) * 8, name
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request):
+    g = dict(np.load(os.path.join(HERE, request.param + ".npz")))
+    prob = CASES[request.param]()
+    return request.param, prob, g
+
+
+def test_generator_reproduces_inputs(case):
+    name, prob, g = case
+    assert rel(prob.udg, g["udg_in"]) < 1e-13
+    assert rel(prob.uh, g["uh_in"]) < 1e-13
+    assert rel(prob.mesh.dgnodes, g["dgnodes"]) < 1e-13
+    assert np.array_equal(prob.mesh.elcon, g["elcon"])
+
+
+def test_oracle_matches_reference(case):
+    name, prob, g = case
+    o = Oracle(prob)
+    udg_q = o.getq(g["udg_in"], g["uh_in"])
+    assert rel(udg_q, g["udg"]) < 1e-12
+    ref_udg = g["udg"].reshape(udg_q.shape)
+    for ie in range(2):
+        e = o.element(ref_udg, g["uh_in"], ie)
+        for k in ("D", "F", "K", "H", "Rh"):
+            blk = g["e" + k].reshape(2, -1)[ie]
+            assert rel(e[k], blk) < 1e-12, (k, ie)
+        ru = g["eRu"].reshape(2, -1)[ie]
+        assert np.max(np.abs(e["Ru"] - ru)) <= 1e-12 * max(np.max(np.abs(e["Rh"])), np.max(np.abs(ru)))
+    a = o.assemble(ref_udg, g["uh_in"])
+    compare("Hg", a["Hg"], g)
+    compare("DinvF", a["DinvF"], g)
+    scale = max(np.max(np.abs(g["Rr"])), np.max(np.abs(g["Rg"])))
+    compare("Rg", a["Rg"], g, scale=scale)
+    compare("Rr", a["Rr"], g, scale=scale)
+    compare("DinvRu", a["DinvRu"], g, scale=max(np.max(np.abs(g["DinvRu"])), 1.0))
+    assert abs(a["rnorm"] - g["rnorm"][0]) <= 1e-12 * g["rnorm"][0]
+
+
+def test_newton_history_matches_reference():
+    g = dict(np.load(os.path.join(HERE, "ns2d_p2_n4_newton.npz")))
+    prob = ns2d_vortex(n=4, porder=2)
+    o = Oracle(prob)
+    udg = o.getq(prob.udg, prob.uh)
+    uh = prob.uh.copy()
+    hist, iters = [], []
+    for _ in range(2):
+        a = o.assemble(udg, uh)
+        hist.append(a["rnorm"])
+        x, flag, gh = o.gmres(a["Hg"], a["Rg"], Minv=o.bj_inverse(a["Hg"]), restart=50, tol=1e-10)
+        assert flag == 0
+        iters.append(len(gh))
+        udg, uh = o.update(udg, uh, x, a["DinvRu"], a["DinvF"], 1.0)
+    hist.append(o.residual(udg, uh))
+    r0 = g["rnorm_hist"][0]
+    assert np.max(np.abs(np.array(hist) - g["rnorm_hist"])) <= 1e-12 * r0
+    assert iters == [int(v) for v in g["gmres_iters"]]
+    assert rel(udg.ravel(), g["udg"]) < 1e-12
+    assert rel(uh.ravel(), g["uh"]) < 1e-12
