@@ -19,6 +19,7 @@
 #include "elem_kernels.cuh"
 #include "krylov_kernels.cuh"
 #include "schur_kernels.cuh"
+#include "elem_kernel_v2.cuh"
 
 using namespace hfem;
 
@@ -84,6 +85,9 @@ struct Launch {
     void (*schur)(dim3, size_t, cudaStream_t, const SchurArgs&);
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
     void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
+    void (*element2)(dim3, size_t, cudaStream_t, const ElemArgs&);
+    size_t elem2_smem;
+    const void* elem2_fn;
     int inv_threads;
     const void *elem_fn, *schur_fn, *q_fn, *inv_fn;
     GemmLaunch g1, g2;
@@ -96,6 +100,8 @@ void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int*
 
 template <class S>
 void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel<S><<<g, NT, sm, st>>>(a); }
+template <class S>
+void launch_element2(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel_v2<S><<<g, NT, sm, st>>>(a); }
 template <class S>
 void launch_schur(dim3 g, size_t sm, cudaStream_t st, const SchurArgs& a) { schur_kernel<S::N, S::NB><<<g, NT, sm, st>>>(a); }
 template <class S>
@@ -116,6 +122,9 @@ Launch make_launch() {
     L.schur_fn = (const void*)schur_kernel<S::N, S::NB>;
     L.q_fn = (const void*)getq_kernel<S>;
     L.inverse = launch_inverse<S::N>;
+    L.element2 = launch_element2<S>;
+    L.elem2_smem = sizeof(ElemSmemV2<S>);
+    L.elem2_fn = (const void*)element_kernel_v2<S>;
     L.inv_threads = InvThreads<S::N>::value;
     L.inv_fn = (const void*)inverse_kernel<S::N>;
     L.g1 = GemmParams<typename SchurCfg<S>::g1>::make();
@@ -314,7 +323,7 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
     const dim3 ge(c->grid_elem);
     {
         Timed t(c, "element");
-        c->L->element(ge, c->L->elem_smem, c->stream, elem_args(c));
+        c->L->element2(ge, c->L->elem2_smem, c->stream, elem_args(c));
         if ((rc = check_launch(c, "element"))) return rc;
     }
     ScatterArgs sa = scatter_args(c);
@@ -582,10 +591,11 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     c->stream = c->own;
     const Launch& L = *c->L;
     cudaFuncSetAttribute(L.elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
+    cudaFuncSetAttribute(L.elem2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem2_smem);
     cudaFuncSetAttribute(L.schur_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.schur_smem);
     cudaFuncSetAttribute(L.q_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.q_smem);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn, NT, L.elem_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem2_fn, NT, L.elem2_smem);
     c->grid_elem = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.schur_fn, NT, L.schur_smem);
