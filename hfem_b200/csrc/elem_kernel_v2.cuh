@@ -200,71 +200,71 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * Em[sm.perm[fc * NPF + m] + NPV * fd];
             sMiEf[t] = s;
         }
-        if (tid < NGV + NA) {
-            using DD = Dual<NC>;
+        // pointwise fluxes: one work item per (point, differentiated variable k);
+        // a one-derivative dual pass gives f and df/dw_k at that point.
+        for (int t = tid; t < (NGV + NA) * NC; t += NT) {
+            using DD = Dual<1>;
+            const int p = t % (NGV + NA), k = t / (NGV + NA);
+            const bool vol = p < NGV;
+            const int g = vol ? p : p - NGV;
             DD w[NC], f[ND * NCU];
-            const bool vol = tid < NGV;
-            const int g = vol ? tid : tid - NGV;
 #pragma unroll
-            for (int k = 0; k < NC; k++) {
-                double val;
-                if (vol) val = ug[g + NGV * k];
-                else val = (k < NCU) ? uhg[g + NA * k] : ugf[g + NA * k];
-                w[k] = dc<NC>(val);
-                w[k].d[k] = 1.0;
+            for (int c = 0; c < NC; c++) {
+                const double val = vol ? ug[g + NGV * c] : ((c < NCU) ? uhg[g + NA * c] : ugf[g + NA * c]);
+                w[c].v = val;
+                w[c].d[0] = (c == k) ? 1.0 : 0.0;
             }
             ns_flux_dual<ND>(A.param, w, f);
             if (vol) {
                 const double jg = sm.jac[g];
 #pragma unroll
                 for (int j = 0; j < NCU; j++) {
-                    double s = 0.0;
-                    if (A.tdep) {
-                        double t = 0.0;
-                        for (int a = 0; a < NPV; a++) t += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
-                        s = t - ug[g + NGV * j] * A.fc_u;
-                    }
-                    sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
-#pragma unroll
-                    for (int m = 0; m < ND; m++) {
-                        double fx = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
-                        sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
-                    }
-#pragma unroll
-                    for (int k = 0; k < NC; k++) {
-                        const double su = (A.tdep && k == j) ? -A.fc_u : 0.0;
-                        wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
+                    if (k == 0) {
+                        double s = 0.0;
+                        if (A.tdep) {
+                            double tt = 0.0;
+                            for (int a = 0; a < NPV; a++) tt += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
+                            s = tt - ug[g + NGV * j] * A.fc_u;
+                        }
+                        sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
 #pragma unroll
                         for (int m = 0; m < ND; m++) {
-                            double t = 0.0;
+                            double fx = 0.0;
 #pragma unroll
-                            for (int d = 0; d < ND; d++) t += f[d * NCU + j].d[k] * sm.Xx[g + NGV * (d + ND * m)];
-                            wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -t;
+                            for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
+                            sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
                         }
+                    }
+                    const double su = (A.tdep && k == j) ? -A.fc_u : 0.0;
+                    wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
+#pragma unroll
+                    for (int m = 0; m < ND; m++) {
+                        double tt = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) tt += f[d * NCU + j].d[0] * sm.Xx[g + NGV * (d + ND * m)];
+                        wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -tt;
                     }
                 }
             } else {
+                // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
                 const double tau = A.param[5];
                 const double jf = sm.jacf[g];
 #pragma unroll
                 for (int j = 0; j < NCU; j++) {
-                    double t = tau * (ugf[g + NA * j] - uhg[g + NA * j]);
+                    if (k == 0) {
+                        double tt = tau * (ugf[g + NA * j] - uhg[g + NA * j]);
 #pragma unroll
-                    for (int d = 0; d < ND; d++) t += f[d * NCU + j].v * sm.nl[g + NA * d];
-                    sm.fn[g + NA * j] = t * jf;
+                        for (int d = 0; d < ND; d++) tt += f[d * NCU + j].v * sm.nl[g + NA * d];
+                        sm.fn[g + NA * j] = tt * jf;
+                    }
+                    double dn = 0.0;
 #pragma unroll
-                    for (int k = 0; k < NC; k++) {
-                        double dn = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[k] * sm.nl[g + NA * d];
-                        if (k < NCU) {
-                            fnuh[g + NA * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
-                            fnu[g + NA * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
-                        } else {
-                            fnu[g + NA * (j + NCH * k)] = dn * jf;
-                        }
+                    for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[0] * sm.nl[g + NA * d];
+                    if (k < NCU) {
+                        fnuh[g + NA * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
+                        fnu[g + NA * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
+                    } else {
+                        fnu[g + NA * (j + NCH * k)] = dn * jf;
                     }
                 }
             }

@@ -12,8 +12,7 @@
 // tau_ij = (1/Re)(dv_i/dx_j + dv_j/dx_i - 2/3 delta_ij div v).
 // Variables: w = [rho, m_1..m_nd, E, q_1 (ncu comps), .., q_nd].
 //
-// The Jacobian is exact forward-mode differentiation (dual numbers carrying
-// all nc partial derivatives).
+// The Jacobian is exact forward-mode differentiation (dual numbers).
 #pragma once
 
 namespace hfem {
@@ -74,13 +73,13 @@ __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, const Dual<N>& b)
     return r;
 }
 
-// f[d*ncu + c] for one point; w has ND+2 + (ND+2)*ND entries.
-template <int ND>
-__device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, const Dual<(ND + 2) * (ND + 1)>* w,
-                                             Dual<(ND + 2) * (ND + 1)>* f) {
+// f[d*ncu + c] for one point; w has ND+2 + (ND+2)*ND entries, each carrying M
+// partial derivatives (M = nc for the full Jacobian, 1 for one column of it).
+template <int ND, int M>
+__device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, const Dual<M>* w, Dual<M>* f) {
     constexpr int NCU = ND + 2;
-    constexpr int NC = NCU * (ND + 1);
-    using D = Dual<NC>;
+    constexpr int NC = M;
+    using D = Dual<M>;
     const double gam = param[0], Re = param[2], Pr = param[3];
     const double iRe = 1.0 / Re;
     const D& rho = w[0];
