@@ -122,12 +122,25 @@ __device__ __forceinline__ void dmma8x8x4(double& c0, double& c1, double a, doub
 // element-major (the tiles of one element run together and share it in L2).
 template <int MT, int WN, int NW>
 struct GemmCfg {
-    static constexpr int BM = 8 * MT, BN = 8 * WN * NW, BK = 20;
+    static constexpr int BM = 8 * MT, BN = 8 * WN * NW, BK = 20, STAGES = 2;
     static constexpr int LDA = ((BM + 11) / 16) * 16 + 4;     // >= BM, == 4 (mod 16)
     static constexpr int LDB = BK;
     static constexpr int THREADS = 32 * NW;
-    static constexpr size_t SMEM = sizeof(double) * ((size_t)LDA * BK + (size_t)LDB * BN);
+    static constexpr int ASZ = LDA * BK, BSZ = LDB * BN;
+    static constexpr size_t SMEM = sizeof(double) * (size_t)STAGES * (ASZ + BSZ);
 };
+
+// 8-byte asynchronous global->shared copy; with valid == false nothing is read
+// (src-size 0) and the shared word is zero-filled.  gmem must always be a valid
+// global address (callers pass the operand's base when the element is outside).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
 
 template <int MT, int WN, int NW>
 __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, int K, double alpha,
@@ -137,8 +150,6 @@ __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, in
                                                                 long long sC) {
     using G = GemmCfg<MT, WN, NW>;
     extern __shared__ __align__(16) double gsm[];
-    double* As = gsm;                       // As[m + LDA * k]
-    double* Bs = gsm + G::LDA * G::BK;      // Bs[k + LDB * n]
     const int tilesM = (M + G::BM - 1) / G::BM, tilesN = (N + G::BN - 1) / G::BN;
     const int e = blockIdx.x / (tilesM * tilesN), tile = blockIdx.x % (tilesM * tilesN);
     const int m0 = (tile % tilesM) * G::BM, n0 = (tile / tilesM) * G::BN;
@@ -147,22 +158,43 @@ __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, in
     double* Ce = C + (size_t)e * sC;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int gr = lane >> 2, gc = lane & 3;
+
+    auto stage_a = [&](int st) { return gsm + st * (G::ASZ + G::BSZ); };
+    auto stage_b = [&](int st) { return gsm + st * (G::ASZ + G::BSZ) + G::ASZ; };
+    auto load = [&](int st, int k0) {
+        double* As = stage_a(st);
+        double* Bs = stage_b(st);
+        for (int t = tid; t < G::BM * G::BK; t += G::THREADS) {
+            const int m = t % G::BM, k = t / G::BM;
+            const bool ok = (m0 + m < M) && (k0 + k < K);
+            cp_async8(&As[m + G::LDA * k], Ae + (ok ? (m0 + m) + (size_t)lda * (k0 + k) : 0), ok);
+        }
+        for (int t = tid; t < G::BK * G::BN; t += G::THREADS) {
+            const int k = t % G::BK, n = t / G::BK;
+            const bool ok = (n0 + n < N) && (k0 + k < K);
+            cp_async8(&Bs[k + G::LDB * n], Be + (ok ? (k0 + k) + (size_t)ldb * (n0 + n) : 0), ok);
+        }
+    };
+
     double acc[MT][WN][2];
 #pragma unroll
     for (int a = 0; a < MT; a++)
 #pragma unroll
         for (int b = 0; b < WN; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
-    for (int k0 = 0; k0 < K; k0 += G::BK) {
-        __syncthreads();
-        for (int t = tid; t < G::BM * G::BK; t += G::THREADS) {
-            const int m = t % G::BM, k = t / G::BM;
-            As[m + G::LDA * k] = (m0 + m < M && k0 + k < K) ? Ae[(m0 + m) + (size_t)lda * (k0 + k)] : 0.0;
+    const int nk = (K + G::BK - 1) / G::BK;
+    load(0, 0);
+    cp_async_commit();
+    for (int kt = 0; kt < nk; kt++) {
+        if (kt + 1 < nk) {
+            load((kt + 1) & 1, (kt + 1) * G::BK);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
-        for (int t = tid; t < G::BK * G::BN; t += G::THREADS) {
-            const int k = t % G::BK, n = t / G::BK;
-            Bs[k + G::LDB * n] = (n0 + n < N && k0 + k < K) ? Be[(k0 + k) + (size_t)ldb * (n0 + n)] : 0.0;
-        }
         __syncthreads();
+        const double* As = stage_a(kt & 1);
+        const double* Bs = stage_b(kt & 1);
 #pragma unroll
         for (int ks = 0; ks < G::BK; ks += 4) {
             double af[MT], bf[WN];
@@ -175,6 +207,7 @@ __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, in
 #pragma unroll
                 for (int b = 0; b < WN; b++) dmma8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
         }
+        __syncthreads();
     }
 #pragma unroll
     for (int a = 0; a < MT; a++)
