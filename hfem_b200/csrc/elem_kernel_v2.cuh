@@ -1,18 +1,19 @@
 // Element assembly on the FP64 tensor cores (sm_100a, mma.sync m8n8k4 f64).
 //
 // Same outputs and phases as element_kernel up to the pointwise fluxes; every
-// contraction after that is a small GEMM whose B operand is generated on the
-// fly into shared memory (restating elementassembly.cpp elementint 307-572 and
-// faceint 717-1321):
-//   K_fc = shapfg (npf x ngf) * T_k,  T_k(q; j,m,a) = [a on fc] phi_kk(a)(q) fhn_u(q; j,m)
-//                                               + sum_d fhn_u(q; j, q_dm) (phi M^-1 C_d)(q; a)
-//   H_fc = shapfg * T_h,  T_h(q; j,m,f2) = [f2 on fc] phi_f2(q) fhn_uh(q; j,m)
-//                                        - sum_d fhn_u(q; j, q_dm) (phi M^-1 E_d)(q; f2)
-//   D_vol = shapvg (npv x ngv(nd+1)) * W,  W(g,r; j,a,k) = wrl(g,r; j,k) phi_a(g)
-//                                               + sum_d wrl(g,r; j, q_dk) (phi M^-1 C_d)(g; a)
-//   F_vol = shapvg * W_f,  W_f(g,r; j,k,f2) = sum_d wrl(g,r; j, q_dk) (-phi M^-1 E_d)(g; f2)
-// followed by the lifted trace terms D = D_vol + P K, F = F_vol + P H.  The
-// face mass product uses shapfgdotshapfc = shapfg .* shapfc (its definition,
+// contraction after that is a GEMM with rows over (test node, equation,
+// variable) and a small B operand resident in shared memory (restating
+// elementassembly.cpp elementint 307-572 and faceint 717-1321):
+//   K_fc[(ip,j,m), a]  = sum_{q,d'} shapfg(ip,q) fhn(q; j, (d',m)) Phi_fc[(q,d'), a],
+//        Phi_fc[(q,0),a] = [a on fc] phi_pos(a)(q),  Phi_fc[(q,d+1),a] = (phi M^-1 C_d)(q; a)
+//   H_fc[(ip,j,m), f2] = sum_{q,d'} shapfg(ip,q) fhn'(q; j, (d',m)) Psi_fc[(q,d'), f2],
+//        d' = 0 uses fhn_uh and Psi_fc[(q,0),f2] = [f2 on fc] phi_f2(q); d' > 0 uses
+//        fhn_u(q; j, q_dm) and Psi_fc = -(phi M^-1 E_d)(q; f2)
+//   Y(i,g,j,c) = sum_r shapvg(i,(g,r)) wrl((g,r), j, c)       (the derivative index r)
+//   D_vol[(i,j,k), a]  = sum_{g,d'} Y(i,g,j,(d',k)) Phi[(g,d'), a],  Phi = [phi_a(g); (phi M^-1 C_d)(g;a)]
+//   F_vol[(i,j,k), f2] = sum_{g,d} Y(i,g,j,(d+1,k)) (-phi M^-1 E_d)(g; f2)
+// followed by the lifted trace terms D = D_vol + P K, F = F_vol + P H.  The face
+// mass product uses shapfgdotshapfc = shapfg .* shapfc (its definition,
 // mkmasterelement.m:113-115) in factored form.
 #pragma once
 #include <cuda_runtime.h>
@@ -21,23 +22,35 @@
 
 namespace hfem {
 
+// Tile parameters of the row-major element GEMMs (K/H per face, D/F volume).
+template <class S>
+struct C3 {
+    static constexpr int NKP = ((S::NPV + 7) / 8) * 8;             // K columns (a), padded
+    static constexpr int NHP = ((S::NDF + 7) / 8) * 8;             // H columns (f2), padded
+    static constexpr int NTK = NKP / 8, NTH = NHP / 8;             // n-tiles
+    static constexpr int KFD = ((S::NGF * (S::ND + 1) + 3) / 4) * 4;  // face k = (q, d')
+    static constexpr int KV3 = ((S::NGV * (S::ND + 1) + 3) / 4) * 4;  // volume k = (g, d')
+    static constexpr int KQ3 = ((S::NGV * S::ND + 3) / 4) * 4;        // volume k = (g, d)
+    static constexpr int LDBK = ((KFD + 11) / 16) * 16 + 4;
+    static constexpr int LDBD = ((KV3 + 11) / 16) * 16 + 4;
+    static constexpr int BKH = LDBK * (NKP + NHP);
+    static constexpr int BDF = LDBD * (NKP + NHP);
+    static constexpr int WY = S::NPV * S::NGV * S::NCU * S::NC;       // Y workspace
+};
+
 template <class S>
 struct V2 {
     static constexpr int MTV = (S::NPV + 7) / 8;              // m-tiles of shapvg
     static constexpr int MTF = (S::NPF + 7) / 8;              // m-tiles of shapfg
-    static constexpr int KV = ((S::NQ + 3) / 4) * 4;          // padded k of volume GEMMs
-    static constexpr int KF = ((S::NGF + 3) / 4) * 4;         // padded k of face GEMMs
+    static constexpr int KV = ((S::NQ + 3) / 4) * 4;          // padded k of shapvg
+    static constexpr int KF = ((S::NGF + 3) / 4) * 4;         // padded k of shapfg
     static constexpr int LDAV = ((8 * MTV + 11) / 16) * 16 + 4;
     static constexpr int LDAF = ((8 * MTF + 11) / 16) * 16 + 4;
-    static constexpr int LDBV = ((KV + 11) / 16) * 16 + 4;    // >= KV, == 4 (mod 16)
-    static constexpr int LDBF = ((KF + 11) / 16) * 16 + 4;
-    static constexpr int NTWV = 1, NTWF = 5;                  // n-tiles per warp (8 warps)
-    static constexpr int CWV = 8 * NTWV * (NT / 32);          // chunk width, volume jobs
-    static constexpr int CWF = 8 * NTWF * (NT / 32);          // chunk width, face jobs
     static constexpr int QSZ = S::NPV * S::NPV * (1 + S::ND) + S::NPV * S::NDF * S::ND + S::NGV * S::NC +
                                S::NA * (S::NC + S::NCH);
-    static constexpr int BSZV = LDBV * CWV, BSZF = LDBF * CWF;
-    static constexpr int UN = (QSZ > BSZV ? (QSZ > BSZF ? QSZ : BSZF) : (BSZV > BSZF ? BSZV : BSZF));
+    static constexpr int UN = QSZ > C3<S>::BKH ? (QSZ > C3<S>::BDF ? QSZ : C3<S>::BDF)
+                                               : (C3<S>::BKH > C3<S>::BDF ? C3<S>::BKH : C3<S>::BDF);
+    static constexpr int WS = S::WS + C3<S>::WY;              // workspace doubles per CTA slot
 };
 
 template <class S>
@@ -54,32 +67,12 @@ struct ElemSmemV2 {
     double Af[V2<S>::LDAF * V2<S>::KF];   // shapfg, zero padded: Af[ip + LDAF*q]
     double sfc[S::NGF * S::NPF];          // face basis values shapfc(kk, q) = shapft[q + NGF*kk]
     double red[NT / 32];
-    double un[V2<S>::UN];                 // q-phase matrices, then the generated B chunks
+    double un[V2<S>::UN];                 // q-phase matrices, then the B operands
     int perm[S::NDF];
     int inc_n[S::NPV];
     int inc_f[S::NPV * S::MAXINC];
     int pos[S::NFE * S::NPV];             // position of element node a on face fc, or -1
 };
-
-// acc(MT x NTW tiles) += A(8MT x 4KST, smem col-major lda) * B(4KST x 8 NTW*warps, smem col-major ldb)
-template <int MT, int NTW, int KST>
-__device__ __forceinline__ void chunk_mma(const double* As, int lda, const double* Bs, int ldb,
-                                          double (&acc)[MT][NTW][2]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int gr = lane >> 2, gc = lane & 3;
-#pragma unroll 4
-    for (int ks = 0; ks < KST; ks++) {
-        double af[MT], bf[NTW];
-#pragma unroll
-        for (int a = 0; a < MT; a++) af[a] = As[(8 * a + gr) + lda * (4 * ks + gc)];
-#pragma unroll
-        for (int b = 0; b < NTW; b++) bf[b] = Bs[(4 * ks + gc) + ldb * (8 * (warp * NTW + b) + gr)];
-#pragma unroll
-        for (int a = 0; a < MT; a++)
-#pragma unroll
-            for (int b = 0; b < NTW; b++) dmma8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
-    }
-}
 
 template <class S>
 __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
@@ -93,7 +86,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int gr = lane >> 2, gc = lane & 3;
 
-    double* ws = A.ws + (size_t)blockIdx.x * S::WS;
+    double* ws = A.ws + (size_t)blockIdx.x * V2<S>::WS;
     double* wrl = ws;
     double* sMiC = wrl + S::W_WRL;
     double* sMiE = sMiC + S::W_SMIC;
@@ -275,6 +268,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         double* He = A.H + (size_t)e * NB * NB;
         double* Rhe = A.Rh + (size_t)e * NB;
         double* Roe = A.Ro + (size_t)e * NB;
+        double* Ys = fnuh + S::W_FNUH;      // Y(i,g,j,c) = sum_r shapvg(i,(g,r)) wrl((g,r), j, c)
         for (int t = tid; t < NB; t += NT) {
             const int j = t % NCH, fdof = t / NCH, fc = fdof / NPF, ip = fdof % NPF;
             double s = 0.0;
@@ -282,117 +276,193 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             Rhe[t] = -s;
             Roe[t] = -s;
         }
-        // ---- K and H, face by face: columns (j, m, a) and (j, m, f2), chunks of CWF
-        constexpr int NCOLK = NCH * NCU * NPV, NCOLH = NCH * NCU * NDF;
-        for (int job = 0; job < NFE * 2; job++) {
-            const int fc = job % NFE;
-            const bool isH = job >= NFE;
-            const int ncol = isH ? NCOLH : NCOLK;
-            for (int c0 = 0; c0 < ncol; c0 += C2::CWF) {
-                __syncthreads();
-                for (int t = tid; t < C2::KF * C2::CWF; t += NT) {
-                    const int q = t % C2::KF, cl = t / C2::KF, c = c0 + cl;
-                    double v = 0.0;
-                    if (q < NGF && c < ncol) {
-                        const int gg = q + NGF * fc;
-                        const int j = c % NCH, m = (c / NCH) % NCU, z = c / (NCH * NCU);
-                        double s = 0.0;
+        // Y, stored so that row (i,j,k) and column (g,d') of the volume GEMMs are
+        // separable: Ys[(i + NPV j) + N (g + NGV (NCU d' + k))]
+        for (int t = tid; t < NGV * NCU * NC; t += NT) {
+            const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
+            double w[ND1];
 #pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            s += fnu[gg + NA * (j + NCH * (NCU * (1 + d) + m))] *
-                                 (isH ? sMiEf[gg + NA * (z + NDF * d)] : sMiCf[gg + NA * (z + NPV * d)]);
-                        if (isH) {
-                            v = -s;
-                            if (z / NPF == fc) v += sm.sfc[q + NGF * (z % NPF)] * fnuh[gg + NA * (j + NCH * m)];
-                        } else {
-                            v = s;
-                            const int p = sm.pos[fc * NPV + z];
-                            if (p >= 0) v += sm.sfc[q + NGF * p] * fnu[gg + NA * (j + NCH * m)];
-                        }
-                    }
-                    Bs[q + C2::LDBF * cl] = v;
-                }
-                __syncthreads();
-                double acc[C2::MTF][C2::NTWF][2];
+            for (int r = 0; r < ND1; r++) w[r] = wrl[g + NGV * (r + ND1 * (j + NCU * c))];
+#pragma unroll 4
+            for (int i = 0; i < NPV; i++) {
+                double y = 0.0;
 #pragma unroll
-                for (int a = 0; a < C2::MTF; a++)
-#pragma unroll
-                    for (int b = 0; b < C2::NTWF; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
-                chunk_mma<C2::MTF, C2::NTWF, C2::KF / 4>(sm.Af, C2::LDAF, Bs, C2::LDBF, acc);
-#pragma unroll
-                for (int a = 0; a < C2::MTF; a++)
-#pragma unroll
-                    for (int b = 0; b < C2::NTWF; b++)
-#pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            const int ip = 8 * a + gr, c = c0 + 8 * (warp * C2::NTWF + b) + 2 * gc + h;
-                            if (ip < NPF && c < ncol) {
-                                const int j = c % NCH, m = (c / NCH) % NCU, z = c / (NCH * NCU);
-                                const int row = j + NCH * (fc * NPF + ip);
-                                if (isH) He[row + (size_t)NB * (m + NCH * z)] = acc[a][b][h];
-                                else Ke[row + (size_t)NB * (z + NPV * m)] = acc[a][b][h];
+                for (int r = 0; r < ND1; r++) y += sm.Av[i + C2::LDAV * (g + NGV * r)] * w[r];
+                Ys[(i + NPV * j) + (size_t)N * (g + NGV * c)] = y;
+            }
+        }
+        // ---- K and H face by face: rows (ip, j, m), k = (q, d'), generated A = shapfg(ip,q) x fhn
+        for (int fc = 0; fc < NFE; fc++) {
+            __syncthreads();
+            double* BK = Bs;                              // KFD x NPV  (ld C3::LDBK)
+            double* BH = Bs + C3<S>::LDBK * C3<S>::NKP;   // KFD x NDF  (ld C3::LDBK)
+            for (int t = tid; t < C3<S>::KFD * (C3<S>::NKP + C3<S>::NHP); t += NT) {
+                const int k = t % C3<S>::KFD, n = t / C3<S>::KFD;
+                const int q = k % NGF, dp = k / NGF, gg = q + NGF * fc;
+                double v = 0.0;
+                if (dp <= ND && k < NGF * ND1) {
+                    if (n < C3<S>::NKP) {                 // K columns a
+                        const int a = n;
+                        if (a < NPV) {
+                            if (dp == 0) {
+                                const int p = sm.pos[fc * NPV + a];
+                                v = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
+                            } else {
+                                v = sMiCf[gg + NA * (a + NPV * (dp - 1))];
                             }
                         }
+                        BK[k + C3<S>::LDBK * a] = v;
+                    } else {                              // H columns f2
+                        const int f2 = n - C3<S>::NKP;
+                        if (f2 < NDF) {
+                            if (dp == 0) v = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
+                            else v = -sMiEf[gg + NA * (f2 + NDF * (dp - 1))];
+                        }
+                        BH[k + C3<S>::LDBK * f2] = v;
+                    }
+                } else {
+                    if (n < C3<S>::NKP) BK[k + C3<S>::LDBK * n] = 0.0;
+                    else BH[k + C3<S>::LDBK * (n - C3<S>::NKP)] = 0.0;
+                }
+            }
+            __syncthreads();
+            constexpr int MTK = (NPF * NCH * NCU + 7) / 8;
+            for (int mt = warp; mt < MTK; mt += NT / 32) {
+                const int r = 8 * mt + gr;
+                const bool rv = r < NPF * NCH * NCU;
+                const int ip = r % NPF, j = (r / NPF) % NCH, m = r / (NPF * NCH);
+                double aK[C3<S>::KFD / 4], aH[C3<S>::KFD / 4];
+#pragma unroll
+                for (int ks = 0; ks < C3<S>::KFD / 4; ks++) {
+                    const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF, gg = q + NGF * fc;
+                    double vK = 0.0, vH = 0.0;
+                    if (rv && k < NGF * ND1) {
+                        const double sf = sm.Af[ip + C2::LDAF * q];
+                        if (dp == 0) {
+                            vK = sf * fnu[gg + NA * (j + NCH * m)];
+                            vH = sf * fnuh[gg + NA * (j + NCH * m)];
+                        } else {
+                            vK = sf * fnu[gg + NA * (j + NCH * (NCU * dp + m))];
+                            vH = vK;
+                        }
+                    }
+                    aK[ks] = vK;
+                    aH[ks] = vH;
+                }
+                double acc[C3<S>::NTK][2];
+#pragma unroll
+                for (int b = 0; b < C3<S>::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < C3<S>::KFD / 4; ks++)
+#pragma unroll
+                    for (int b = 0; b < C3<S>::NTK; b++)
+                        dmma8x8x4(acc[b][0], acc[b][1], aK[ks], BK[(4 * ks + gc) + C3<S>::LDBK * (8 * b + gr)]);
+#pragma unroll
+                for (int b = 0; b < C3<S>::NTK; b++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int a = 8 * b + 2 * gc + h;
+                        if (rv && a < NPV) Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = acc[b][h];
+                    }
+                double acch[C3<S>::NTH][2];
+#pragma unroll
+                for (int b = 0; b < C3<S>::NTH; b++) acch[b][0] = acch[b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < C3<S>::KFD / 4; ks++)
+#pragma unroll
+                    for (int b = 0; b < C3<S>::NTH; b++)
+                        dmma8x8x4(acch[b][0], acch[b][1], aH[ks], BH[(4 * ks + gc) + C3<S>::LDBK * (8 * b + gr)]);
+#pragma unroll
+                for (int b = 0; b < C3<S>::NTH; b++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int f2 = 8 * b + 2 * gc + h;
+                        if (rv && f2 < NDF) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[b][h];
+                    }
             }
         }
         __syncthreads();
-        // ---- D and F: volume GEMMs, then the lifted trace rows of K and H
-        double* De = A.D + (size_t)e * N * N;
-        double* Fe = A.F + (size_t)e * N * NB;
-        constexpr int NCOLD = NCU * NPV * NCU, NCOLF = NCU * NCU * NDF;
-        for (int job = 0; job < 2; job++) {
-            const bool isF = job == 1;
-            const int ncol = isF ? NCOLF : NCOLD;
-            for (int c0 = 0; c0 < ncol; c0 += C2::CWV) {
-                __syncthreads();
-                for (int t = tid; t < C2::KV * C2::CWV; t += NT) {
-                    const int q = t % C2::KV, cl = t / C2::KV, c = c0 + cl;
+        // ---- D_vol = Y' Phi and F_vol = Y'_q Psi, B operands in shared memory
+        {
+            double* Phi = Bs;                              // KV x NPV   (ld LDBD)
+            double* Psi = Bs + C3<S>::LDBD * C3<S>::NKP;   // KQ x NDF   (ld LDBD)
+            for (int t = tid; t < C3<S>::KV3 * (C3<S>::NKP + C3<S>::NHP); t += NT) {
+                const int k = t % C3<S>::KV3, n = t / C3<S>::KV3;
+                const int g = k % NGV, dp = k / NGV;
+                if (n < C3<S>::NKP) {
                     double v = 0.0;
-                    if (q < NQ && c < ncol) {
-                        const int g = q % NGV, r = q / NGV;
-                        if (!isF) {                 // column (j, a, k)
-                            const int j = c % NCU, a = (c / NCU) % NPV, k = c / (NCU * NPV);
-                            v = wrl[g + NGV * (r + ND1 * (j + NCU * k))] * T.shapvt[g + NGV * a];
-#pragma unroll
-                            for (int d = 0; d < ND; d++)
-                                v += wrl[g + NGV * (r + ND1 * (j + NCU * (NCU * (1 + d) + k)))] * sMiC[g + NGV * (a + NPV * d)];
-                        } else {                    // column (j, k, f2)
-                            const int j = c % NCU, k = (c / NCU) % NCU, f2 = c / (NCU * NCU);
-#pragma unroll
-                            for (int d = 0; d < ND; d++)
-                                v += wrl[g + NGV * (r + ND1 * (j + NCU * (NCU * (1 + d) + k)))] * sMiE[g + NGV * (f2 + NDF * d)];
-                        }
-                    }
-                    Bs[q + C2::LDBV * cl] = v;
+                    if (n < NPV && k < NGV * ND1)
+                        v = (dp == 0) ? T.shapvt[g + NGV * n] : sMiC[g + NGV * (n + NPV * (dp - 1))];
+                    Phi[k + C3<S>::LDBD * n] = v;
+                } else {
+                    const int f2 = n - C3<S>::NKP;
+                    double v = 0.0;
+                    if (f2 < NDF && k < NGV * ND) v = sMiE[g + NGV * (f2 + NDF * dp)];
+                    Psi[k + C3<S>::LDBD * f2] = v;
                 }
-                __syncthreads();
-                double acc[C2::MTV][C2::NTWV][2];
+            }
+            __syncthreads();
+            double* De = A.D + (size_t)e * N * N;
+            double* Fe = A.F + (size_t)e * N * NB;
+            constexpr int MTD = (NPV * NCU * NCU + 7) / 8;
+            for (int mt = warp; mt < MTD; mt += NT / 32) {
+                const int r = 8 * mt + gr;
+                const bool rv = r < NPV * NCU * NCU;
+                const int i = r % NPV, j = (r / NPV) % NCU, k = r / (NPV * NCU);
+                const double* yrow = Ys + (i + NPV * j) + (size_t)N * NGV * k;
+                double acc[C3<S>::NTK][2];
 #pragma unroll
-                for (int a = 0; a < C2::MTV; a++) acc[a][0][0] = acc[a][0][1] = 0.0;
-                chunk_mma<C2::MTV, C2::NTWV, C2::KV / 4>(sm.Av, C2::LDAV, Bs, C2::LDBV, acc);
+                for (int b = 0; b < C3<S>::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
+#pragma unroll 8
+                for (int ks = 0; ks < C3<S>::KV3 / 4; ks++) {
+                    const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
+                    const double a = (rv && kk < NGV * ND1) ? yrow[(size_t)N * (g + NGV * NCU * dp)] : 0.0;
 #pragma unroll
-                for (int a = 0; a < C2::MTV; a++)
+                    for (int b = 0; b < C3<S>::NTK; b++)
+                        dmma8x8x4(acc[b][0], acc[b][1], a, Phi[kk + C3<S>::LDBD * (8 * b + gr)]);
+                }
+                double accf[C3<S>::NTH][2];
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int i = 8 * a + gr, c = c0 + 8 * warp + 2 * gc + h;
-                        if (i < NPV && c < ncol) {
-                            double s = acc[a][0][h];
-                            const int j = c % NCU;
-                            if (!isF) {
-                                const int kcol = c / NCU;       // a + NPV*k
+                for (int b = 0; b < C3<S>::NTH; b++) accf[b][0] = accf[b][1] = 0.0;
+#pragma unroll 8
+                for (int ks = 0; ks < C3<S>::KQ3 / 4; ks++) {
+                    const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
+                    const double a = (rv && kk < NGV * ND) ? yrow[(size_t)N * (g + NGV * NCU * (d + 1))] : 0.0;
+#pragma unroll
+                    for (int b = 0; b < C3<S>::NTH; b++)
+                        dmma8x8x4(accf[b][0], accf[b][1], a, Psi[kk + C3<S>::LDBD * (8 * b + gr)]);
+                }
+                if (rv) {
+#pragma unroll
+                    for (int b = 0; b < C3<S>::NTK; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int a = 8 * b + 2 * gc + h;
+                            if (a < NPV) {
+                                const int kcol = a + NPV * k;
+                                double v = acc[b][h];
                                 for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
-                                    s += Ke[j + NCH * sm.inc_f[i * S::MAXINC + c2] + (size_t)NB * kcol];
-                                De[i + NPV * c] = s;
-                            } else {
-                                const int hcol = c / NCU;       // k + NCH*f2
-                                for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
-                                    s += He[j + NCH * sm.inc_f[i * S::MAXINC + c2] + (size_t)NB * hcol];
-                                Fe[i + NPV * c] = s;
+                                    v += Ke[j + NCH * sm.inc_f[i * S::MAXINC + c2] + (size_t)NB * kcol];
+                                De[i + NPV * (j + NCU * kcol)] = v;
                             }
                         }
-                    }
+#pragma unroll
+                    for (int b = 0; b < C3<S>::NTH; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int f2 = 8 * b + 2 * gc + h;
+                            if (f2 < NDF) {
+                                const int hcol = k + NCH * f2;
+                                double v = accf[b][h];
+                                for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
+                                    v += He[j + NCH * sm.inc_f[i * S::MAXINC + c2] + (size_t)NB * hcol];
+                                Fe[i + NPV * (j + NCU * hcol)] = v;
+                            }
+                        }
+                }
             }
         }
+        __syncthreads();
         double ru2 = 0.0;
         for (int t = tid; t < N; t += NT) {
             const int i = t % NPV, j = t / NPV;

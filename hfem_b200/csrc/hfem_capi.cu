@@ -79,7 +79,8 @@ template <int MT, int WN, int NW> struct GemmParams<GemmCfg<MT, WN, NW>> {
 
 struct Launch {
     int nd, npv, npf, ngv, ngf;
-    size_t ws;                  // workspace doubles per CTA slot
+    size_t ws;                  // workspace doubles per CTA slot (element_kernel)
+    size_t ws2;                 // workspace doubles per CTA slot (element_kernel_v2)
     size_t elem_smem, schur_smem, q_smem;
     void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
     void (*schur)(dim3, size_t, cudaStream_t, const SchurArgs&);
@@ -112,6 +113,7 @@ Launch make_launch() {
     Launch L;
     L.nd = S::ND; L.npv = S::NPV; L.npf = S::NPF; L.ngv = S::NGV; L.ngf = S::NGF;
     L.ws = S::WS;
+    L.ws2 = V2<S>::WS;
     L.elem_smem = sizeof(ElemSmem<S>);
     L.schur_smem = sizeof(double) * ((size_t)S::N * S::N + (size_t)S::N * 32 + 2 * 16 * 64 + S::N);
     L.q_smem = sizeof(QSmem<S>);
@@ -275,7 +277,7 @@ int ensure_assembly_buffers(hfem_ctx* c) {
     if ((rc = dalloc(c, &c->Ro, ne * nb))) return rc;
     if ((rc = dalloc(c, &c->ru2, ne))) return rc;
     if ((rc = dalloc(c, &c->info, ne))) return rc;
-    if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws))) return rc;
+    if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws2))) return rc;
     return 0;
 }
 
