@@ -63,6 +63,8 @@ def load_library(path: str = LIB):
     lib.hfem_newton.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, _dp,
                                 C.c_int, _ip, _ip]
     lib.hfem_download.argtypes = [C.c_void_p, C.c_int, _dp, C.c_size_t]
+    lib.hfem_dirk_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                   C.c_double, C.c_int, _ip]
     lib.hfem_set_timing.argtypes = [C.c_void_p, C.c_int]
     lib.hfem_kernel_times.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, _dp, _ip, C.c_int]
     _lib = lib
@@ -192,6 +194,14 @@ class HDGSolver:
         self._chk(self.lib.hfem_newton(self.h, newton_tol, maxiter, precond, restart, gmres_tol, gmres_maxit, _d(hist),
                                        hist.size, C.byref(nit), C.byref(conv)), "solveNonlinearProblem")
         return conv.value, hist[:nit.value + 1]
+
+    def solveUnsteadyStep(self, dt, stages=3, order=3, newton_tol=1e-10, newton_maxiter=10, precond=2, restart=50,
+                          gmres_tol=1e-10, gmres_maxit=1000):
+        """One DIRK time step (solveUnsteadyProblem's step loop body); returns Newton iterations."""
+        it = C.c_int(0)
+        self._chk(self.lib.hfem_dirk_step(self.h, float(dt), stages, order, newton_tol, newton_maxiter, precond,
+                                          restart, gmres_tol, gmres_maxit, C.byref(it)), "solveUnsteadyStep")
+        return it.value
 
     def set_timing(self, on=True):
         self._chk(self.lib.hfem_set_timing(self.h, 1 if on else 0), "set_timing")

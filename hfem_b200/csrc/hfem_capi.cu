@@ -177,6 +177,7 @@ struct hfem_ctx {
     double *Minv = nullptr, *V = nullptr, *w = nullptr, *x = nullptr, *pb = nullptr, *scal = nullptr, *part = nullptr;
     int* binfo = nullptr;
     int krylov_restart = 0;
+    double* udgi = nullptr;     // state at the start of the current time step
     KernelTimer timer;
 };
 
@@ -554,6 +555,60 @@ int update_impl(hfem_ctx* c, double alpha) {
     return 0;
 }
 
+// DIRK(s, q) tableaus (solvers/DIRKcoeff.cpp:6-118 lists the same methods):
+// d = A^-1 column-major (d[i + s*j]), t = stage times c_i.  The tableaus are the
+// published ones: backward Euler, implicit midpoint, the 2-stage L-stable SDIRK
+// (gamma = 1 - 1/sqrt 2), the 2-stage 3rd-order SDIRK (gamma = (3 + sqrt 3)/6) and
+// Alexander's 3-stage L-stable SDIRK (gamma the root of g^3 - 3g^2 + 3g/2 - 1/6 in (0,1)).
+bool dirk_table(int stages, int order, double* d, double* t) {
+    double A[9] = {0};
+    if (stages == 1 && order == 1) { A[0] = 1.0; t[0] = 1.0; }
+    else if (stages == 1 && order == 2) { A[0] = 0.5; t[0] = 0.5; }
+    else if (stages == 2 && order == 2) {
+        const double g = 1.0 - 1.0 / std::sqrt(2.0);
+        A[0] = g; A[1] = 1.0 - g; A[3] = g;            // A[i + 2j]
+        t[0] = g; t[1] = 1.0;
+    } else if (stages == 2 && order == 3) {
+        const double g = (3.0 + std::sqrt(3.0)) / 6.0;
+        A[0] = g; A[1] = 1.0 - 2.0 * g; A[3] = g;
+        t[0] = g; t[1] = 1.0 - g;
+    } else if (stages == 3 && order == 3) {
+        double g = 0.4358665;                             // Newton on g^3 - 3g^2 + 3g/2 - 1/6
+        for (int it = 0; it < 50; it++) g -= (g * g * g - 3 * g * g + 1.5 * g - 1.0 / 6.0) / (3 * g * g - 6 * g + 1.5);
+        const double t2 = 0.5 * (1.0 + g);
+        const double b1 = -(6 * g * g - 16 * g + 1) / 4.0, b2 = (6 * g * g - 20 * g + 5) / 4.0;
+        A[0] = g; A[1] = t2 - g; A[2] = b1;               // A[i + 3j]
+        A[4] = g; A[5] = b2; A[8] = g;
+        t[0] = g; t[1] = t2; t[2] = 1.0;
+    } else {
+        return false;
+    }
+    // inverse of the lower-triangular A, column by column
+    const int s = stages;
+    for (int j = 0; j < s; j++)
+        for (int i = 0; i < s; i++) {
+            double v = 0.0;
+            if (i == j) v = 1.0 / A[i + s * i];
+            else if (i > j) {
+                double acc = 0.0;
+                for (int k = j; k < i; k++) acc += A[i + s * k] * d[k + s * j];
+                v = -acc / A[i + s * i];
+            }
+            d[i + s * j] = v;
+        }
+    return true;
+}
+
+// sh = cu_i udgi + cu udg + cs sh on the u components, 0 on the q components.
+__global__ void dirk_source_kernel(long long n, int npv, int nc, int ncu, double ci, double cu, double cs,
+                                   const double* __restrict__ udgi, const double* __restrict__ udg,
+                                   double* __restrict__ sh) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int comp = (int)((i / npv) % nc);
+        sh[i] = (comp < ncu) ? ci * udgi[i] + cu * udg[i] + cs * sh[i] : 0.0;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -629,7 +684,7 @@ int hfem_destroy(hfem_ctx* c) {
     void* ptrs[] = {c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm, c->dgnodes, c->elcon,
                     c->rowstart, c->colidx, c->blk_src, c->face_src, c->rowface, c->colface, c->udg, c->uh, c->sh,
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
-                    c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo};
+                    c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& p : c->timer.pending) {
@@ -857,6 +912,62 @@ int hfem_newton(hfem_ctx* c, double newton_tol, int newton_maxiter, int precond,
     if (hist && nh < hist_len) hist[nh++] = rNorm;
     if (niter) *niter = iter;
     if (converged) *converged = rNorm < newton_tol ? 1 : 0;
+    return 0;
+}
+
+// One time step of solveUnsteadyProblem (solvers/dgsolvers.cpp:221-444): for
+// each DIRK stage set time = t + dt c_i, fc_u = d_ii/dt, fc_q = 1, form the
+// stage source SH from the step's initial state and the previous stage
+// (dgsolvers.cpp:319-348, q part zeroed) and solve the stage with the Newton
+// driver.  A stage that does not converge returns HFEM_E_SINGULAR (the
+// reference calls error() and exits).
+int hfem_dirk_step(hfem_ctx* c, double dt, int stages, int order, double newton_tol, int newton_maxiter,
+                   int precond, int restart, double gmres_tol, int gmres_maxit, int* newton_iters) {
+    if (!c) return HFEM_E_ARG;
+    int rc = ready(c);
+    if (rc) return rc;
+    double d[9], t[3];
+    if (!(dt > 0.0) || !dirk_table(stages, order, d, t))
+        return fail(c, HFEM_E_ARG, "unsupported DIRK(%d,%d) or dt <= 0", stages, order);
+    const hfem_dims& dm = c->dims;
+    const long long n = (long long)dm.ne * dm.npv * c->nc;
+    if (!c->udgi && (rc = dalloc(c, &c->udgi, (size_t)n))) return rc;
+    CK(cudaMemcpyAsync(c->udgi, c->udg, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    const int S = stages;
+    const double t0 = c->time;
+    int total_iters = 0;
+    for (int s = 0; s < S; s++) {
+        double ci = 0.0, cu = 0.0, cs = 0.0;
+        if (s == 0) {
+            ci = d[0] / dt;
+        } else if (s == 1) {
+            ci = (d[1] + d[S + 1]) / dt;
+            cu = -d[1] / dt;
+        } else {
+            const double r = d[2] / d[1];
+            ci = (d[2] + d[S + 2] + d[2 * S + 2]) / dt - r * (d[1] + d[S + 1]) / dt;
+            cs = r;
+            cu = -d[S + 2] / dt;
+        }
+        dirk_source_kernel<<<sms(c->device) * 4, 256, 0, c->stream>>>(n, dm.npv, c->nc, c->ncu, ci, cu, cs, c->udgi,
+                                                                      c->udg, c->sh);
+        if ((rc = check_launch(c, "dirk_source"))) return rc;
+        c->time = t0 + dt * t[s];
+        c->fc_u = d[s + S * s] / dt;
+        c->fc_q = 1.0;
+        c->tdep = 1;
+        int it = 0, conv = 0;
+        if ((rc = hfem_newton(c, newton_tol, newton_maxiter, precond, restart, gmres_tol, gmres_maxit, nullptr, 0,
+                              &it, &conv)))
+            return rc;
+        total_iters += it;
+        if (!conv) {
+            c->time = t0;
+            return fail(c, HFEM_E_SINGULAR, "DIRK stage %d did not converge in %d Newton iterations", s + 1, it);
+        }
+    }
+    c->time = t0 + dt;
+    if (newton_iters) *newton_iters = total_iters;
     return 0;
 }
 

@@ -116,6 +116,14 @@ int hfem_update(hfem_ctx* ctx, double alpha);
 int hfem_newton(hfem_ctx* ctx, double newton_tol, int newton_maxiter, int precond, int restart, double gmres_tol,
                 int gmres_maxit, double* rnorm_hist, int hist_len, int* niter, int* converged);
 
+/* One DIRK(stages, order) time step of size dt (stages 1-3; (1,1) (1,2) (2,2)
+ * (2,3) (3,3) as solvers/DIRKcoeff.cpp), each stage solved by hfem_newton.
+ * Replaces one iteration of solveUnsteadyProblem (solvers/dgsolvers.cpp:221-444);
+ * the context's time advances by dt.  *newton_iters (may be NULL) receives the
+ * Newton iterations of all stages. */
+int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newton_tol, int newton_maxiter,
+                   int precond, int restart, double gmres_tol, int gmres_maxit, int* newton_iters);
+
 /* Download device results for inspection (host buffers of the given length):
  * what = 0 Hg (nblocks*bsz^2), 1 Rg (nf*bsz), 2 Rr = sum of uncondensed Rh
  * (nf*bsz), 3 DinvRu (n*ne), 4 DinvF (n*nb*ne), 5 condensed element H

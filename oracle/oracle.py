@@ -171,6 +171,83 @@ class Oracle:
         return x, flag, hist[:it.value]
 
 
+def dirk_table(stages, order):
+    """(d = A^-1, t) of the DIRK(s, q) tableaus solvers/DIRKcoeff.cpp lists."""
+    if (stages, order) == (1, 1):
+        A, t = np.array([[1.0]]), [1.0]
+    elif (stages, order) == (2, 2):
+        g = 1 - 1 / np.sqrt(2)
+        A, t = np.array([[g, 0], [1 - g, g]]), [g, 1.0]
+    elif (stages, order) == (3, 3):
+        g = 0.4358665
+        for _ in range(50):
+            g -= (g ** 3 - 3 * g * g + 1.5 * g - 1 / 6) / (3 * g * g - 6 * g + 1.5)
+        t2 = (1 + g) / 2
+        b1, b2 = -(6 * g * g - 16 * g + 1) / 4, (6 * g * g - 20 * g + 5) / 4
+        A, t = np.array([[g, 0, 0], [t2 - g, g, 0], [b1, b2, g]]), [g, t2, 1.0]
+    else:
+        raise ValueError((stages, order))
+    return np.linalg.inv(A), t
+
+
+def newton_solve(o, udg, uh, sh, tol, maxiter, restart=50, gmres_tol=1e-10):
+    """solveNonlinearProblem (solvers/dgsolvers.cpp:106-205) on the oracle."""
+    rnorm, it, robust = tol + 1.0, 0, 0
+    hist = []
+    while rnorm > tol and it < maxiter:
+        it += 1
+        a = o.assemble(udg, uh, sh=sh)
+        old = a["rnorm"]
+        hist.append(old)
+        x, flag, _ = o.gmres(a["Hg"], a["Rg"], Minv=o.bj_inverse(a["Hg"]), restart=restart, tol=gmres_tol)
+        if flag == -1:
+            break
+        if it == 1 and old < tol:
+            rnorm = old
+            break
+        alpha = 1.0
+        while True:
+            udg, uh = o.update(udg, uh, x, a["DinvRu"], a["DinvF"], alpha, sh=sh)
+            rnorm = o.residual(udg, uh, sh=sh)
+            if not np.isfinite(rnorm) or (rnorm > old and rnorm > tol):
+                alpha = -abs(alpha / 2)
+                if abs(alpha) < 1e-4:
+                    if robust == 0:
+                        robust = 1
+                        alpha = -2 * abs(alpha)
+                        udg, uh = o.update(udg, uh, x, a["DinvRu"], a["DinvF"], alpha, sh=sh)
+                    break
+            else:
+                break
+    hist.append(rnorm)
+    return udg, uh, rnorm < tol, hist
+
+
+def dirk_step(prob, udg, uh, sh, dt, stages=3, order=3, tol=1e-10, maxiter=10):
+    """One step of solveUnsteadyProblem (solvers/dgsolvers.cpp:280-420) on the oracle."""
+    d, t = dirk_table(stages, order)
+    ncu = prob.ncu
+    udgi = udg.copy()
+    for s in range(stages):
+        if s == 0:
+            sh = (d[0, 0] / dt) * udgi
+        elif s == 1:
+            sh = ((d[1, 0] + d[1, 1]) / dt) * udgi - udg * d[1, 0] / dt
+        else:
+            sh = (((d[2, 0] + d[2, 1] + d[2, 2]) / dt) * udgi
+                  - (d[2, 0] / d[1, 0]) * ((d[1, 0] + d[1, 1]) * udgi / dt - sh) - udg * d[2, 1] / dt)
+        sh = sh.copy()
+        sh[:, ncu:, :] = 0.0
+        prob.fc_u = d[s, s] / dt
+        prob.fc_q = 1.0
+        prob.tdep = 1
+        o = Oracle(prob)
+        udg, uh, conv, _ = newton_solve(o, udg, uh, sh, tol, maxiter)
+        if not conv:
+            raise RuntimeError(f"DIRK stage {s + 1} did not converge")
+    return udg, uh, sh
+
+
 def run_reference(prob, mode="assemble", ndump=0, newton=None, workdir=None):
     """Run the compiled reference on ``prob`` and load its dumps."""
     from hfem_b200.gen.refio import write_inputs
