@@ -343,6 +343,87 @@ def run_reference(args, rank):
             "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# ------------------------------------------------------------- other tasks
+def run_newton_task(args):
+    """Config 1: one Newton step (assembly, BJ-GMRES(50) to 1e-10, update, residual) on
+    the 2D p=2 vortex, repeated to the converged state; GPU vs the reference driver."""
+    import torch
+    from hfem_b200.core import HDGSolver
+    from hfem_b200.gen.problem import ns2d_vortex
+    prob = ns2d_vortex(n=32, porder=2)
+    s = HDGSolver(prob)
+    st = torch.cuda.current_stream()
+    s.set_stream(st.cuda_stream)
+    s.getQ()
+    u0, h0 = s.get_solution()
+    for _ in range(args.warmup):
+        s.set_solution(u0, h0, prob.sh)
+        s.solveNonlinearProblem(newton_tol=1e-10, maxiter=1)
+    times, hist = [], None
+    for _ in range(args.steps):
+        s.set_solution(u0, h0, prob.sh)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=1)
+        e1.record(st)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    _, gh = s.gmres(precond=2, restart=50, tol=1e-10)
+    s.close()
+    ms = float(np.median(times))
+    line = {"metric": "Newton steps/s (2D NS p=2, 2048 elements, BJ-GMRES(50) tol 1e-10)", "value": 1e3 / ms,
+            "unit": "steps/s", "impl": "hfem", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+            "dtype": "f64", "rnorm_history": [float(v) for v in hist], "gmres_iterations": int(len(gh)),
+            "higher_is_better": True}
+    if os.path.exists(REF_BIN):
+        from hfem_b200.gen.refio import write_inputs
+        with tempfile.TemporaryDirectory() as tmp:
+            prefix = os.path.join(tmp, "in_")
+            write_inputs(prefix, prob, newton_maxiter=1, gmres_tol=1e-10)
+            env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
+            t0 = time.time()
+            subprocess.run([REF_BIN, "newton", prefix, os.path.join(tmp, "out_"), "1", "2", "50", "1e-10"],
+                           check=True, capture_output=True, env=env)
+            wall = time.time() - t0
+            rh = np.fromfile(os.path.join(tmp, "out_rnorm_hist.bin"))
+        line["cpu_baseline"] = {"value": 1.0 / wall, "unit": "steps/s", "cores": 1, "kind": "reference",
+                                "sample": "the same Newton step by oracle/_ref/hfem_ref (reference driver, one "
+                                          "process, includes its set-up)",
+                                "rnorm_history": [float(v) for v in rh]}
+    return line
+
+
+def run_dirk_task(args):
+    """Config 4: Taylor-Green 16^3 x 6 tets, p = 3, Re 1600, Mach 0.1, DIRK(3,3), dt = 0.01."""
+    import torch
+    from hfem_b200.core import HDGSolver
+    from hfem_b200.diagnostics import kinetic_energy
+    from hfem_b200.gen.problem import ns3d_tgv
+    prob = ns3d_tgv(n=args.tgv_n, porder=3, dt=0.01)
+    s = HDGSolver(prob)
+    st = torch.cuda.current_stream()
+    s.set_stream(st.cuda_stream)
+    s.getQ()
+    u, _ = s.get_solution()
+    ke = [kinetic_energy(prob, u)]
+    iters, times = [], []
+    for _ in range(args.dirk_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        iters.append(s.solveUnsteadyStep(0.01, stages=3, order=3, newton_tol=args.dirk_tol))
+        e1.record(st)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        u, _ = s.get_solution()
+        ke.append(kinetic_energy(prob, u))
+    s.close()
+    return {"metric": f"DIRK(3,3) time steps/s (3D TGV {args.tgv_n}^3x6 tets = {prob.mesh.ne} elements, p=3)",
+            "value": 1e3 / float(np.mean(times)), "unit": "steps/s", "impl": "hfem", "dtype": "f64",
+            "ms_per_step": float(np.mean(times)), "steps": args.dirk_steps, "newton_iterations": iters,
+            "kinetic_energy": ke, "higher_is_better": True}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,7 +433,15 @@ def main():
     ap.add_argument("--workload", default="ns3d_p3_48k", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk"])
+    ap.add_argument("--tgv-n", type=int, default=16)
+    ap.add_argument("--dirk-steps", type=int, default=20)
+    ap.add_argument("--dirk-tol", type=float, default=1e-9)
     args = ap.parse_args()
+    if args.task != "assembly":
+        line = run_newton_task(args) if args.task == "newton" else run_dirk_task(args)
+        print(json.dumps(line), flush=True)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "hfem" else args.warmup
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
