@@ -186,3 +186,71 @@ def write_inputs(prefix: str, prob: Problem, **kw):
     write_master(prefix + "master.bin", prob)
     write_mesh(prefix + "mesh.bin", prob)
     write_sol(prefix + "sol.bin", prob)
+
+
+# ------------------------------------------------------------------ readers
+def _rd(f, n):
+    a = np.fromfile(f, dtype=np.float64, count=n)
+    if a.size != n:
+        raise ValueError("file shorter than its header says")
+    return a
+
+
+def read_sol(path, ne=None, npv=None, nc=None):
+    """sol.bin (readbinaryfiles.cpp readsolstruct, serial branch): UDG, UH, PDG as flat arrays."""
+    with open(path, "rb") as f:
+        nd = _rd(f, 10).astype(np.int64)
+        udg, uh, pdg = _rd(f, int(nd[0])), _rd(f, int(nd[1])), _rd(f, int(nd[2]))
+    if ne is not None:
+        udg = udg.reshape(ne, nc, npv)
+    return udg, uh, pdg
+
+
+def read_mesh(path):
+    """mesh.bin (readmeshstruct, serial branch) as a dict of element-major arrays."""
+    with open(path, "rb") as f:
+        nd = _rd(f, 30).astype(np.int64)
+        dim, ncd, nfe, nve, nvf, ne, nf = (int(v) for v in nd[:7])
+        npe, npf = int(nd[9]), int(nd[10])
+        out = dict(ndims=nd)
+        out["elementtype"] = _rd(f, ne).astype(np.int64)
+        out["t"] = _rd(f, nve * ne).reshape(ne, nve).astype(np.int64)
+        out["dgnodes"] = _rd(f, npe * ncd * ne).reshape(ne, ncd, npe)
+        out["elcon"] = _rd(f, npf * nfe * ne).reshape(ne, npf * nfe).astype(np.int64)
+        out["bf"] = _rd(f, nfe * ne).reshape(ne, nfe).astype(np.int64)
+        out["t2f"] = _rd(f, nfe * ne).reshape(ne, nfe).astype(np.int64)
+        out["t2t"] = _rd(f, nfe * ne).reshape(ne, nfe).astype(np.int64)
+        out["f"] = _rd(f, (nvf + 3) * nf).reshape(nf, nvf + 3).astype(np.int64)
+        out["isEDGface"] = _rd(f, nf).astype(np.int64)
+    return out
+
+
+def write_checkpoint(path, udg, uh, ncu=None, with_q=True):
+    """Solution file of solstruct::writeSol2File (preprocessing/ioutilities.cpp:256-300):
+    [n_udg, n_uh, UDG (u only when with_q is False), UH], float64."""
+    udg = np.ascontiguousarray(udg)
+    if not with_q:
+        udg = np.ascontiguousarray(udg[:, :ncu, :])
+    with open(path, "wb") as f:
+        np.array([udg.size, np.size(uh)], dtype=np.float64).tofile(f)
+        udg.astype(np.float64).tofile(f)
+        np.ascontiguousarray(uh, dtype=np.float64).tofile(f)
+
+
+def read_checkpoint(path):
+    with open(path, "rb") as f:
+        n = _rd(f, 2).astype(np.int64)
+        return _rd(f, int(n[0])), _rd(f, int(n[1]))
+
+
+def problem_from_files(prefix, prob_template):
+    """State of a problem read back from the reference's input files: UDG/UH from
+    sol.bin and dgnodes/elcon/t2f checked against the template's mesh."""
+    udg, uh, _ = read_sol(prefix + "sol.bin")
+    me = read_mesh(prefix + "mesh.bin")
+    p = prob_template
+    if not (np.array_equal(me["elcon"], p.mesh.elcon) and np.array_equal(me["t2f"], p.mesh.t2f)):
+        raise ValueError("mesh file does not match the problem's connectivity")
+    p.udg = udg.reshape(p.udg.shape)
+    p.uh = uh.reshape(p.uh.shape)
+    return p
