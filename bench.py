@@ -424,6 +424,35 @@ def run_dirk_task(args):
             "kinetic_energy": ke, "higher_is_better": True}
 
 
+def run_serve_task(args):
+    """Config 5: a stream of independent 2D NS solve requests (Poisson arrivals,
+    256-16,384 elements log-uniform, p in {1,2,3}, Re in [50,500], Mach in
+    [0.2,0.7], Newton residual 1e-10), served with continuous batching and, on
+    the same stream, by sequential plain FP64 solves."""
+    import torch
+    from hfem_b200.serve import build_problem, make_requests, sequential, serve
+    torch.cuda.init()
+    out = {"metric": "HDG solves/s with p50/p99 latency (2D NS request stream)", "unit": "solves/s",
+           "impl": "hfem", "dtype": "f64", "higher_is_better": True, "data": "synthetic", "rates": []}
+    for rate in args.serve_rates:
+        reqs = make_requests(args.serve_requests, rate, seed=args.serve_seed)
+        for r in reqs:
+            build_problem(r)
+        # warm the kernels and contexts of every order once, outside the timing
+        serve([r for r in make_requests(6, 1e6, seed=999, max_el=512)], hbm_budget=None)
+        st = serve(reqs, tol=1e-10, gmres_tol=args.serve_gmres_tol)
+        seq_reqs = make_requests(args.serve_requests, rate, seed=args.serve_seed)[:args.serve_seq_requests]
+        for a, b in zip(seq_reqs, reqs):
+            a.prob = b.prob
+        sq = sequential(seq_reqs, tol=1e-10, gmres_tol=args.serve_gmres_tol)
+        out["rates"].append({"rate": rate, "requests": len(reqs), "served": st.as_dict(),
+                             "sequential": dict(sq.as_dict(), requests=len(seq_reqs))})
+    best = out["rates"][-1]
+    out["value"] = best["served"]["solves_per_s"]
+    out["sequential_value"] = best["sequential"]["solves_per_s"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,13 +462,18 @@ def main():
     ap.add_argument("--workload", default="ns3d_p3_48k", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk"])
+    ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve"])
     ap.add_argument("--tgv-n", type=int, default=16)
     ap.add_argument("--dirk-steps", type=int, default=20)
     ap.add_argument("--dirk-tol", type=float, default=1e-9)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[50.0])
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-seq-requests", type=int, default=200)
+    ap.add_argument("--serve-seed", type=int, default=0)
+    ap.add_argument("--serve-gmres-tol", type=float, default=1e-10)
     args = ap.parse_args()
     if args.task != "assembly":
-        line = run_newton_task(args) if args.task == "newton" else run_dirk_task(args)
+        line = {"newton": run_newton_task, "dirk": run_dirk_task, "serve": run_serve_task}[args.task](args)
         print(json.dumps(line), flush=True)
         return
     args.warmup = max(args.warmup, 3) if args.impl == "hfem" else args.warmup

@@ -193,6 +193,9 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * Em[sm.perm[fc * NPF + m] + NPV * fd];
             sMiEf[t] = s;
         }
+        const double* P = A.pparam ? A.pparam + 8 * A.eprob[e] : A.param;
+        const int tdep = A.pparam ? (int)P[6] : A.tdep;
+        const double fc_u = A.pparam ? P[7] : A.fc_u;
         // pointwise fluxes: one work item per (point, differentiated variable k);
         // a one-derivative dual pass gives f and df/dw_k at that point.
         for (int t = tid; t < (NGV + NA) * NC; t += NT) {
@@ -207,17 +210,17 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 w[c].v = val;
                 w[c].d[0] = (c == k) ? 1.0 : 0.0;
             }
-            ns_flux_dual<ND>(A.param, w, f);
+            ns_flux_dual<ND>(P, w, f);
             if (vol) {
                 const double jg = sm.jac[g];
 #pragma unroll
                 for (int j = 0; j < NCU; j++) {
                     if (k == 0) {
                         double s = 0.0;
-                        if (A.tdep) {
+                        if (tdep) {
                             double tt = 0.0;
                             for (int a = 0; a < NPV; a++) tt += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
-                            s = tt - ug[g + NGV * j] * A.fc_u;
+                            s = tt - ug[g + NGV * j] * fc_u;
                         }
                         sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
 #pragma unroll
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                             sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
                         }
                     }
-                    const double su = (A.tdep && k == j) ? -A.fc_u : 0.0;
+                    const double su = (tdep && k == j) ? -fc_u : 0.0;
                     wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
 #pragma unroll
                     for (int m = 0; m < ND; m++) {
@@ -240,7 +243,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 }
             } else {
                 // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
-                const double tau = A.param[5];
+                const double tau = P[5];
                 const double jf = sm.jacf[g];
 #pragma unroll
                 for (int j = 0; j < NCU; j++) {

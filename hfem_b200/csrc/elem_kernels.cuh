@@ -54,6 +54,10 @@ struct ElemArgs {
     int ne;
     double *D, *F, *K, *H, *Ru, *Rh, *Ro, *ru2;
     double* ws;                 // gridDim.x slots of Shape::WS doubles
+    // several problems in one mesh (NULL = the uniform values above): element ->
+    // problem, and per problem [gamma, eps, Re, Pr, Mach, tau, tdep, fc_u]
+    const int* eprob;
+    const double* pparam;
 };
 
 constexpr int NT = 256;         // threads per CTA for element kernels
@@ -789,6 +793,8 @@ struct QArgs {
     // optional update before the q solve: u += alpha (DinvRu - DinvF duh_e)
     const double *DinvRu, *DinvF, *duh;
     double alpha;
+    const int* eprob;           // per-problem step lengths (NULL: alpha for all)
+    const double* palpha;
 };
 
 template <class S>
@@ -823,14 +829,15 @@ __global__ void __launch_bounds__(NT) getq_kernel(QArgs A) {
             if (A.DinvF) sm.de[fn * NCH + c] = A.duh[(size_t)gd * NCH + c];
         }
         __syncthreads();
+        const double alpha = A.palpha ? A.palpha[A.eprob[e]] : A.alpha;
         for (int t = tid; t < N; t += NT) {
             double v = ue[t];
             if (A.DinvF) {
                 const double* df = A.DinvF + (size_t)e * N * NB;
                 double s = 0.0;
                 for (int c = 0; c < NB; c++) s += df[t + (size_t)N * c] * sm.de[c];
-                v += -A.alpha * s;
-                v += A.alpha * A.DinvRu[(size_t)e * N + t];
+                v += -alpha * s;
+                v += alpha * A.DinvRu[(size_t)e * N + t];
                 ue[t] = v;
             }
             sm.u[t] = v;
@@ -863,6 +870,13 @@ __global__ void __launch_bounds__(NT) getq_kernel(QArgs A) {
 __global__ void axpy_kernel(long long n, double alpha, const double* x, double* y) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         y[i] += alpha * x[i];
+}
+
+// y += alpha[prob[i / per]] x  (per-problem step lengths on the trace unknowns)
+__global__ void axpy_prob_kernel(long long n, int per, const int* __restrict__ prob, const double* __restrict__ alpha,
+                                 const double* x, double* y) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] += alpha[prob[i / per]] * x[i];
 }
 
 }  // namespace hfem

@@ -18,6 +18,7 @@
 #include "../../include/hfem_b200.h"
 #include "elem_kernels.cuh"
 #include "krylov_kernels.cuh"
+#include "krylov_seg.cuh"
 #include "schur_kernels.cuh"
 #include "elem_kernel_v2.cuh"
 
@@ -178,6 +179,19 @@ struct hfem_ctx {
     int* binfo = nullptr;
     int krylov_restart = 0;
     double* udgi = nullptr;     // state at the start of the current time step
+    // several problems in one mesh
+    int nprob = 0;
+    bool palpha_on = false;
+    int *eprob = nullptr, *fprob = nullptr;
+    double *pparam = nullptr, *palpha = nullptr;
+    // per-problem Krylov segments (faces of each problem contiguous)
+    int npieces = 0;
+    long long* seg_pstart = nullptr;
+    int *seg_pseg = nullptr, *seg_p0 = nullptr, *seg_ticket = nullptr;
+    double *seg_part = nullptr, *seg_h = nullptr, *seg_y = nullptr, *seg_nrm = nullptr;
+    unsigned char* seg_act = nullptr;
+    int* seg_k = nullptr;
+    int seg_restart = 0;
     KernelTimer timer;
 };
 
@@ -298,6 +312,8 @@ ElemArgs elem_args(hfem_ctx* c) {
     a.D = c->D; a.F = c->F; a.K = c->K; a.H = c->H;
     a.Ru = c->Ru; a.Rh = c->Rh; a.Ro = c->Ro; a.ru2 = c->ru2;
     a.ws = c->ws;
+    a.eprob = c->nprob ? c->eprob : nullptr;
+    a.pparam = c->nprob ? c->pparam : nullptr;
     return a;
 }
 
@@ -400,6 +416,8 @@ int launch_getq(hfem_ctx* c, const double* duh, double alpha) {
     q.DinvF = duh ? c->DinvF : nullptr;
     q.duh = duh;
     q.alpha = alpha;
+    q.eprob = c->eprob;
+    q.palpha = (duh && c->nprob && c->palpha_on) ? c->palpha : nullptr;
     Timed t(c, duh ? "update" : "getq");
     c->L->getq(dim3(c->grid_elem), c->L->q_smem, c->stream, q);
     return check_launch(c, "getq");
@@ -544,6 +562,204 @@ int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int
     return 0;
 }
 
+// z = M^-1 Hg x (M^-1 omitted when !prec) by the warp-per-row kernel, rows
+// of problems with act[p] == 0 skipped.
+int matvec_warp(hfem_ctx* c, const double* x, double* z, bool prec, const unsigned char* act) {
+    Timed t(c, "matvec_warp");
+    const int grid = std::max(1, std::min((c->dims.nf + 7) / 8, sms(c->device) * 8));
+    const double* M = prec ? c->Minv : nullptr;
+    const int* rseg = act ? c->fprob : nullptr;
+    switch (c->bsz) {
+#define HFEM_MV(B)                                                                                               \
+    case B:                                                                                                      \
+        bsr_matvec_warp_kernel<B><<<grid, 256, 0, c->stream>>>(c->dims.nf, c->rowstart, c->colidx, c->Hg, M, x, z, \
+                                                                 rseg, act);                                     \
+        break;
+        HFEM_MV(8) HFEM_MV(12) HFEM_MV(15) HFEM_MV(16) HFEM_MV(20) HFEM_MV(30) HFEM_MV(50)
+#undef HFEM_MV
+        default: return fail(c, HFEM_E_UNSUPPORTED, "no block matvec for block size %d", c->bsz);
+    }
+    return check_launch(c, "matvec_warp");
+}
+
+// Restarted, left-preconditioned GMRES with modified Gram-Schmidt run for
+// every problem of the context at once (kernel/gmres_bilu0.m:17-105 per
+// problem).  Each problem has its own Krylov basis (its segment of the
+// vectors), Hessenberg matrix, Givens rotations and stopping test, so it takes
+// exactly the iterations it takes alone; the launches are shared, and a
+// problem that has stopped is skipped by every kernel.
+int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters) {
+    int rc;
+    if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before gmres");
+    if (!c->nprob || !c->npieces)
+        return fail(c, HFEM_E_STATE, "per-problem GMRES needs a problem map with each problem's faces contiguous");
+    if (restart < 1 || maxit < 1 || !(tol > 0.0)) return fail(c, HFEM_E_ARG, "restart, maxit and tol must be positive");
+    if (precond != -1 && precond != 2) return fail(c, HFEM_E_ARG, "precond must be -1 (none) or 2 (block Jacobi)");
+    if ((rc = ensure_krylov(c, restart))) return rc;
+    const int P = c->nprob;
+    if (c->seg_restart < restart) {
+        if ((rc = dalloc(c, &c->seg_h, (size_t)(restart + 2) * P))) return rc;
+        if ((rc = dalloc(c, &c->seg_y, (size_t)restart * P))) return rc;
+        c->seg_restart = restart;
+    }
+    const long long n = nvec(c);
+    const int g = sms(c->device) * 4;
+    const bool prec = precond == 2;
+    if (prec) {
+        Timed t(c, "bj_inverse");
+        const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
+        bj_inverse_kernel<<<std::min(c->dims.nf, sms(c->device) * 8), 64, smem, c->stream>>>(
+            c->dims.nf, c->bsz, c->rowstart, c->Hg, c->Minv, c->binfo);
+        if ((rc = check_launch(c, "bj_inverse"))) return rc;
+        std::vector<int> bi(c->dims.nf);
+        CK(cudaMemcpyAsync(bi.data(), c->binfo, sizeof(int) * bi.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < c->dims.nf; i++)
+            if (bi[i]) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d is singular", i);
+        bj_apply_kernel<<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv, c->Rg, c->pb);
+    } else {
+        CK(cudaMemcpyAsync(c->pb, c->Rg, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CK(cudaMemsetAsync(c->x, 0, sizeof(double) * n, c->stream));
+    const SegPieces SP{c->npieces, c->seg_pstart, c->seg_pseg, c->seg_p0, c->seg_ticket, c->seg_part, c->seg_act};
+    const int np = c->npieces;
+    double* d_h = c->seg_h;                   // Hessenberg column, entry (i, p) at i * P + p
+    std::vector<unsigned char> act(P, 1);
+    auto set_act = [&]() -> int {
+        CK(cudaMemcpyAsync(c->seg_act, act.data(), P, cudaMemcpyHostToDevice, c->stream));
+        return 0;
+    };
+    auto axpy_dot = [&](const double* hprev, const double* vprev, double* w, const double* b, double* out, int sq) {
+        seg_axpy_dot_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, hprev, vprev, w, b, out, sq);
+    };
+    if ((rc = set_act())) return rc;
+    axpy_dot(nullptr, nullptr, c->pb, c->pb, c->seg_nrm, 1);
+    std::vector<double> nrmb(P), beta(P), hcol((size_t)(restart + 2) * P);
+    CK(cudaMemcpyAsync(nrmb.data(), c->seg_nrm, sizeof(double) * P, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (double& v : nrmb)
+        if (v == 0.0) v = 1.0;
+    const size_t ldh = (size_t)(restart + 1) * restart;
+    std::vector<double> H(ldh * P), cs((size_t)restart * P), sn((size_t)restart * P), gv((size_t)(restart + 1) * P),
+        Y((size_t)restart * P);
+    std::vector<int> state(P, 2), its(P, 0), jc(P, 0);   // state 2 running, 1 converged, 0 maxit, -1 breakdown
+    std::vector<char> incycle(P, 0);
+    while (true) {
+        int running = 0;
+        for (int p = 0; p < P; p++) act[p] = state[p] == 2, running += state[p] == 2;
+        if (!running) break;
+        if ((rc = set_act())) return rc;
+        // r = M^-1 b - M^-1 A x, beta = |r| per problem
+        if ((rc = matvec_warp(c, c->x, c->w, prec, c->seg_act))) return rc;
+        seg_sub_from_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, c->pb, c->w);
+        axpy_dot(nullptr, nullptr, c->w, c->w, c->seg_nrm, 1);
+        CK(cudaMemcpyAsync(beta.data(), c->seg_nrm, sizeof(double) * P, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        int live = 0;
+        for (int p = 0; p < P; p++) {
+            incycle[p] = 0;
+            jc[p] = 0;
+            if (state[p] != 2) continue;
+            if (beta[p] / nrmb[p] <= tol) { state[p] = 1; continue; }
+            incycle[p] = 1;
+            live++;
+            std::fill(gv.begin() + (size_t)p * (restart + 1), gv.begin() + (size_t)(p + 1) * (restart + 1), 0.0);
+            gv[(size_t)p * (restart + 1)] = beta[p];
+        }
+        if (!live) break;
+        for (int p = 0; p < P; p++) act[p] = incycle[p];
+        if ((rc = set_act())) return rc;
+        seg_scale_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, c->seg_nrm, c->w, c->V);
+        for (int j = 0; j < restart && live; j++) {
+            double* vj = c->V + (size_t)j * n;
+            double* vn = c->V + (size_t)(j + 1) * n;
+            if ((rc = matvec_warp(c, vj, vn, prec, c->seg_act))) return rc;
+            {
+                Timed t(c, "orthogonalise_seg");
+                for (int i = 0; i <= j; i++)
+                    axpy_dot(i ? d_h + (size_t)(i - 1) * P : nullptr, i ? c->V + (size_t)(i - 1) * n : nullptr, vn,
+                             c->V + (size_t)i * n, d_h + (size_t)i * P, 0);
+                axpy_dot(d_h + (size_t)j * P, vj, vn, vn, d_h + (size_t)(j + 1) * P, 1);
+                seg_scale_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, d_h + (size_t)(j + 1) * P, vn, vn);
+            }
+            if ((rc = check_launch(c, "arnoldi"))) return rc;
+            CK(cudaMemcpyAsync(hcol.data(), d_h, sizeof(double) * (size_t)(j + 2) * P, cudaMemcpyDeviceToHost,
+                               c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            bool changed = false;
+            for (int p = 0; p < P; p++) {
+                if (!incycle[p]) continue;
+                double* h = H.data() + ldh * p;
+                double* cp = cs.data() + (size_t)restart * p;
+                double* sp = sn.data() + (size_t)restart * p;
+                double* gp = gv.data() + (size_t)(restart + 1) * p;
+                for (int i = 0; i <= j + 1; i++) h[i + (restart + 1) * j] = hcol[(size_t)i * P + p];
+                const double nn = hcol[(size_t)(j + 1) * P + p];
+                for (int i = 0; i < j; i++) {
+                    const double a = h[i + (restart + 1) * j], b = h[i + 1 + (restart + 1) * j];
+                    h[i + (restart + 1) * j] = cp[i] * a + sp[i] * b;
+                    h[i + 1 + (restart + 1) * j] = -sp[i] * a + cp[i] * b;
+                }
+                const double a = h[j + (restart + 1) * j], b = h[j + 1 + (restart + 1) * j];
+                const double rr = std::sqrt(a * a + b * b);
+                cp[j] = a / rr;
+                sp[j] = b / rr;
+                h[j + (restart + 1) * j] = rr;
+                h[j + 1 + (restart + 1) * j] = 0.0;
+                gp[j + 1] = -sp[j] * gp[j];
+                gp[j] = cp[j] * gp[j];
+                its[p]++;
+                jc[p] = j + 1;
+                const double res = std::fabs(gp[j + 1]);
+                int stop = 2;
+                if (res / nrmb[p] <= tol) stop = 1;
+                else if (its[p] >= maxit) stop = 0;
+                else if (nn == 0.0) stop = -1;
+                if (stop != 2) {
+                    state[p] = stop;
+                    incycle[p] = 0;
+                    live--;
+                    changed = true;
+                }
+            }
+            if (changed && live) {
+                for (int p = 0; p < P; p++) act[p] = incycle[p];
+                if ((rc = set_act())) return rc;
+            }
+        }
+        // x += V y for every problem that took part in this cycle
+        std::vector<int> kk(P, 0);
+        std::fill(Y.begin(), Y.end(), 0.0);
+        for (int p = 0; p < P; p++) {
+            const int J = jc[p];
+            act[p] = J > 0;
+            kk[p] = J;
+            if (!J) continue;
+            const double* h = H.data() + ldh * p;
+            const double* gp = gv.data() + (size_t)(restart + 1) * p;
+            double* y = Y.data() + (size_t)restart * p;
+            for (int i = J - 1; i >= 0; i--) {
+                double s = gp[i];
+                for (int k = i + 1; k < J; k++) s -= h[i + (restart + 1) * k] * y[k];
+                y[i] = s / h[i + (restart + 1) * i];
+            }
+        }
+        if ((rc = set_act())) return rc;
+        CK(cudaMemcpyAsync(c->seg_k, kk.data(), sizeof(int) * P, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->seg_y, Y.data(), sizeof(double) * Y.size(), cudaMemcpyHostToDevice, c->stream));
+        seg_combine_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, n, c->seg_k, restart, c->V, c->seg_y, c->x);
+        if ((rc = check_launch(c, "combine_seg"))) return rc;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    flush_timer(c);
+    for (int p = 0; p < P; p++) {
+        if (conv) conv[p] = state[p] == 1 ? 1 : (state[p] == 0 ? 0 : -1);
+        if (iters) iters[p] = its[p];
+    }
+    return 0;
+}
+
 int update_impl(hfem_ctx* c, double alpha) {
     int rc;
     if (!c->assembled || !c->x) return fail(c, HFEM_E_STATE, "assemble and solve before update");
@@ -684,7 +900,9 @@ int hfem_destroy(hfem_ctx* c) {
     void* ptrs[] = {c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm, c->dgnodes, c->elcon,
                     c->rowstart, c->colidx, c->blk_src, c->face_src, c->rowface, c->colface, c->udg, c->uh, c->sh,
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
-                    c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi};
+                    c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
+                    c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
+                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& p : c->timer.pending) {
@@ -971,6 +1189,111 @@ int hfem_dirk_step(hfem_ctx* c, double dt, int stages, int order, double newton_
     return 0;
 }
 
+// Several independent problems packed into this context's mesh (a disjoint
+// union: no face is shared between problems).  eprob: element -> problem,
+// fprob: face -> problem, params: per problem [gamma, eps, Re, Pr, Mach, tau,
+// tdep, fc_u].  The element kernels then read each element's own physics.
+int hfem_set_problem_map(hfem_ctx* c, int nprob, const int* eprob, const int* fprob, const double* params) {
+    if (!c || nprob < 1 || !eprob || !fprob || !params) return HFEM_E_ARG;
+    const hfem_dims& d = c->dims;
+    for (int e = 0; e < d.ne; e++)
+        if (eprob[e] < 0 || eprob[e] >= nprob) return fail(c, HFEM_E_ARG, "eprob[%d] out of range", e);
+    for (int f = 0; f < d.nf; f++)
+        if (fprob[f] < 0 || fprob[f] >= nprob) return fail(c, HFEM_E_ARG, "fprob[%d] out of range", f);
+    int rc;
+    CK(cudaSetDevice(c->device));
+    if ((rc = upload(c, &c->eprob, eprob, (size_t)d.ne)) || (rc = upload(c, &c->fprob, fprob, (size_t)d.nf)) ||
+        (rc = upload(c, &c->pparam, params, (size_t)nprob * 8)) || (rc = dalloc(c, &c->palpha, (size_t)nprob)))
+        return rc;
+    // Krylov segments (hfem_gmres_problems): when fprob is non-decreasing and
+    // every problem owns a face, problem p's slice of the trace vector is one
+    // contiguous segment, cut into pieces of <= SEG_PIECE entries.
+    c->npieces = 0;
+    bool sorted = true;
+    std::vector<int> fcount(nprob, 0);
+    for (int f = 0; f < d.nf; f++) {
+        fcount[fprob[f]]++;
+        if (f && fprob[f] < fprob[f - 1]) sorted = false;
+    }
+    for (int p = 0; p < nprob; p++) sorted = sorted && fcount[p] > 0;
+    if (sorted) {
+        // piece length: a power of two in [1024, SEG_PIECE] giving about 4 CTAs per SM
+        const long long ntot = (long long)d.nf * c->bsz;
+        long long piece = 1024;
+        while (piece < SEG_PIECE && piece * 4 * sms(c->device) < ntot) piece *= 2;
+        std::vector<long long> pstart;
+        std::vector<int> pseg, p0(nprob + 1);
+        long long a = 0;
+        for (int p = 0; p < nprob; p++) {
+            p0[p] = (int)pseg.size();
+            const long long b = a + (long long)fcount[p] * c->bsz;
+            for (long long s = a; s < b; s += piece) {
+                pstart.push_back(s);
+                pseg.push_back(p);
+            }
+            a = b;
+        }
+        p0[nprob] = (int)pseg.size();
+        pstart.push_back(a);
+        c->npieces = (int)pseg.size();
+        if ((rc = upload(c, &c->seg_pstart, pstart.data(), pstart.size())) ||
+            (rc = upload(c, &c->seg_pseg, pseg.data(), pseg.size())) ||
+            (rc = upload(c, &c->seg_p0, p0.data(), p0.size())) || (rc = dalloc(c, &c->seg_ticket, (size_t)nprob)) ||
+            (rc = dalloc(c, &c->seg_part, pseg.size())) || (rc = dalloc(c, &c->seg_nrm, (size_t)2 * nprob)) ||
+            (rc = dalloc(c, &c->seg_act, (size_t)nprob)) || (rc = dalloc(c, &c->seg_k, (size_t)nprob)))
+            return rc;
+        CK(cudaMemsetAsync(c->seg_ticket, 0, sizeof(int) * nprob, c->stream));
+        c->seg_restart = 0;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->nprob = nprob;
+    return 0;
+}
+
+// Per-problem residual norms of the last assembly or residual pass:
+// rnorm[p] = sqrt(sum over p's elements ||Ru_e||^2 + ||Rr restricted to p's faces||^2).
+int hfem_problem_rnorms(hfem_ctx* c, double* rnorm) {
+    if (!c || !rnorm) return HFEM_E_ARG;
+    if (!c->nprob || !c->ru2) return fail(c, HFEM_E_STATE, "no problem map or no residual yet");
+    const hfem_dims& d = c->dims;
+    std::vector<double> ru2(d.ne), rr((size_t)d.nf * c->bsz);
+    std::vector<int> ep(d.ne), fp(d.nf);
+    CK(cudaMemcpyAsync(ru2.data(), c->ru2, sizeof(double) * ru2.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(rr.data(), c->Rr, sizeof(double) * rr.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(ep.data(), c->eprob, sizeof(int) * ep.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(fp.data(), c->fprob, sizeof(int) * fp.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<double> acc(c->nprob, 0.0);
+    for (int e = 0; e < d.ne; e++) acc[ep[e]] += ru2[e];
+    for (int f = 0; f < d.nf; f++)
+        for (int k = 0; k < c->bsz; k++) acc[fp[f]] += rr[(size_t)f * c->bsz + k] * rr[(size_t)f * c->bsz + k];
+    for (int p = 0; p < c->nprob; p++) rnorm[p] = std::sqrt(acc[p]);
+    return 0;
+}
+
+// updateSol with a step length per problem: uh += alpha_p x, u += alpha_p (D^-1 Ru - D^-1 F x_e).
+int hfem_update_problems(hfem_ctx* c, const double* alpha) {
+    if (!c || !alpha) return HFEM_E_ARG;
+    if (!c->nprob) return fail(c, HFEM_E_STATE, "no problem map");
+    if (!c->assembled || !c->x) return fail(c, HFEM_E_STATE, "assemble and solve before update");
+    int rc;
+    CK(cudaMemcpyAsync(c->palpha, alpha, sizeof(double) * c->nprob, cudaMemcpyHostToDevice, c->stream));
+    axpy_prob_kernel<<<sms(c->device) * 4, 256, 0, c->stream>>>(nvec(c), c->bsz, c->fprob, c->palpha, c->x, c->uh);
+    if ((rc = check_launch(c, "uh update"))) return rc;
+    c->palpha_on = true;
+    rc = launch_getq(c, c->x, 0.0);
+    c->palpha_on = false;
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    flush_timer(c);
+    return 0;
+}
+
+int hfem_gmres_problems(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters) {
+    if (!c) return HFEM_E_ARG;
+    return gmres_seg_impl(c, precond, restart, tol, maxit, conv, iters);
+}
+
 int hfem_download(hfem_ctx* c, int what, double* host, size_t count) {
     if (!c || !host) return HFEM_E_ARG;
     const hfem_dims& d = c->dims;
@@ -1149,6 +1472,8 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.D = D; a.F = DinvF; a.K = K; a.H = H;
     a.Ru = DinvRu; a.Rh = Rh; a.Ro = Rh_uncondensed; a.ru2 = ru2;
     a.ws = scratch;
+    a.eprob = nullptr;
+    a.pparam = nullptr;
     L->element(dim3(ge), L->elem_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     SchurArgs s{d.ne, D, DinvF, K, H, DinvRu, Rh, info};

@@ -1,0 +1,218 @@
+// Krylov kernels for several independent systems packed into one vector
+// (sm_100a): each problem's trace unknowns form one contiguous segment, and
+// every reduction is per segment, so one launch advances the GMRES of every
+// problem while each keeps its own Arnoldi basis, Hessenberg matrix and
+// convergence test (the per-problem algorithm of kernel/gmres_bilu0.m:17-105).
+//
+// A segment is cut into pieces of at most SEG_PIECE entries, one CTA each
+// (the host picks the piece length so that there are a few CTAs per SM).
+// Reductions are deterministic: a CTA reduces its piece in a fixed tree, and
+// the last CTA of a segment to finish (counted with an atomic ticket, the
+// threadfence-reduction pattern; nothing waits) sums the segment's piece
+// partials in piece order and resets the ticket.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hfem {
+
+constexpr int SEG_PIECE = 8192;
+constexpr int SEG_THREADS = 256;
+
+struct SegPieces {
+    int npieces;
+    const long long* pstart;   // npieces + 1 entry offsets
+    const int* pseg;           // segment of each piece
+    const int* seg_p0;         // first piece of each segment (nseg + 1)
+    int* ticket;               // per segment, zero between launches
+    double* part;              // per piece partial sums
+    const unsigned char* act;  // per segment: 0 = skip
+};
+
+__device__ __forceinline__ double seg_block_sum(double s, double* red) {
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < SEG_THREADS / 32; w++) t += red[w];
+    return t;   // valid in thread 0
+}
+
+// Finish a per-segment reduction: thread 0 of every CTA holds its piece sum.
+__device__ __forceinline__ void seg_finish(const SegPieces& P, int piece, int seg, double s, double* out, int sq,
+                                           double* red) {
+    __shared__ int last;
+    if (threadIdx.x == 0) {
+        P.part[piece] = s;
+        __threadfence();
+        const int need = P.seg_p0[seg + 1] - P.seg_p0[seg];
+        last = (atomicAdd(&P.ticket[seg], 1) == need - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int p0 = P.seg_p0[seg], p1 = P.seg_p0[seg + 1];
+    double t = 0.0;
+    for (int k = p0 + threadIdx.x; k < p1; k += SEG_THREADS) t += __ldcg(&P.part[k]);
+    t = seg_block_sum(t, red);
+    if (threadIdx.x == 0) {
+        out[seg] = sq ? sqrt(t) : t;
+        P.ticket[seg] = 0;
+    }
+}
+
+// One modified Gram-Schmidt step fused with the next projection:
+//   w -= hprev[seg] * vprev       (skipped when hprev == NULL)
+//   out[seg] = <b, w>             (sqrt when sq; b may alias w for the norm)
+__global__ void __launch_bounds__(SEG_THREADS) seg_axpy_dot_kernel(SegPieces P, const double* __restrict__ hprev,
+                                                                   const double* __restrict__ vprev, double* w,
+                                                                   const double* b, double* __restrict__ out,
+                                                                   int sq) {
+    __shared__ double red[SEG_THREADS / 32];
+    const int piece = blockIdx.x;
+    const int seg = P.pseg[piece];
+    if (P.act && !P.act[seg]) return;
+    const long long i0 = P.pstart[piece], i1 = P.pstart[piece + 1];
+    double s = 0.0;
+    if (hprev) {
+        const double a = hprev[seg];
+        for (long long i = i0 + threadIdx.x; i < i1; i += SEG_THREADS) {
+            const double v = w[i] - a * vprev[i];
+            w[i] = v;
+            s += b[i] * v;
+        }
+    } else {
+        for (long long i = i0 + threadIdx.x; i < i1; i += SEG_THREADS) s += b[i] * w[i];
+    }
+    s = seg_block_sum(s, red);
+    seg_finish(P, piece, seg, s, out, sq, red);
+}
+
+// y = x / nrm[seg] where nrm[seg] != 0 (y may alias x).
+__global__ void __launch_bounds__(SEG_THREADS) seg_scale_kernel(SegPieces P, const double* __restrict__ nrm,
+                                                                const double* x, double* y) {
+    const int piece = blockIdx.x;
+    const int seg = P.pseg[piece];
+    if (P.act && !P.act[seg]) return;
+    const double d = nrm[seg];
+    if (d == 0.0) return;
+    const double inv = 1.0 / d;
+    for (long long i = P.pstart[piece] + threadIdx.x; i < P.pstart[piece + 1]; i += SEG_THREADS) y[i] = x[i] * inv;
+}
+
+// x += sum_{j<kseg[seg]} V_j y[seg * ldy + j]   (columns of stride n)
+__global__ void __launch_bounds__(SEG_THREADS) seg_combine_kernel(SegPieces P, long long n, const int* __restrict__ kseg,
+                                                                  int ldy, const double* __restrict__ V,
+                                                                  const double* __restrict__ y,
+                                                                  double* __restrict__ x) {
+    const int piece = blockIdx.x;
+    const int seg = P.pseg[piece];
+    if (P.act && !P.act[seg]) return;
+    const int k = kseg[seg];
+    const double* ys = y + (size_t)seg * ldy;
+    for (long long i = P.pstart[piece] + threadIdx.x; i < P.pstart[piece + 1]; i += SEG_THREADS) {
+        double s = 0.0;
+        for (int j = 0; j < k; j++) s += V[(size_t)j * n + i] * ys[j];
+        x[i] += s;
+    }
+}
+
+// r = b - r on active segments
+__global__ void __launch_bounds__(SEG_THREADS) seg_sub_from_kernel(SegPieces P, const double* __restrict__ b,
+                                                                   double* __restrict__ r) {
+    const int piece = blockIdx.x;
+    const int seg = P.pseg[piece];
+    if (P.act && !P.act[seg]) return;
+    for (long long i = P.pstart[piece] + threadIdx.x; i < P.pstart[piece + 1]; i += SEG_THREADS) r[i] = b[i] - r[i];
+}
+
+// z = M^-1 (Hg x) with one warp per block row.  A row's blocks are contiguous
+// in Hg, so the row is one column-major BSZ x (nblk * BSZ) matrix; the warp's
+// lanes form G = 32 / BSZ column groups of BSZ rows (R = 2 rows per lane when
+// BSZ > 32), and the groups' partial sums are added in group order.  Rows of
+// inactive segments (act[rseg[i]] == 0) are skipped.
+template <int BSZ>
+__global__ void __launch_bounds__(256) bsr_matvec_warp_kernel(int nrows, const int* __restrict__ rowstart,
+                                                              const int* __restrict__ colidx,
+                                                              const double* __restrict__ Hg,
+                                                              const double* __restrict__ Minv,
+                                                              const double* __restrict__ x, double* __restrict__ z,
+                                                              const int* __restrict__ rseg,
+                                                              const unsigned char* __restrict__ act) {
+    constexpr int G = BSZ <= 32 ? 32 / BSZ : 1;
+    constexpr int R = (BSZ + 31) / 32;
+    constexpr int LDY = R * 32;
+    __shared__ double ys[8][G][LDY];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int g = BSZ <= 32 ? lane / BSZ : 0;
+    const int r0 = BSZ <= 32 ? lane % BSZ : lane;
+    const bool on = g < G;
+    const int nwarps = gridDim.x * 8;
+    for (int i = blockIdx.x * 8 + wib; i < nrows; i += nwarps) {
+        if (act && !act[rseg[i]]) continue;
+        const int k0 = rowstart[i], k1 = rowstart[i + 1];
+        const int ncol = (k1 - k0) * BSZ;
+        const double* A = Hg + (size_t)k0 * BSZ * BSZ;
+        double acc[R];
+#pragma unroll
+        for (int t = 0; t < R; t++) acc[t] = 0.0;
+        if (on) {
+#pragma unroll 4
+            for (int cc = g; cc < ncol; cc += G) {
+                const int kb = cc / BSZ, c = cc - kb * BSZ;
+                const double xv = __ldg(&x[(size_t)colidx[k0 + kb] * BSZ + c]);
+#pragma unroll
+                for (int t = 0; t < R; t++) {
+                    const int r = r0 + 32 * t;
+                    if (r < BSZ) acc[t] += __ldg(&A[(size_t)cc * BSZ + r]) * xv;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < R; t++) {
+                const int r = r0 + 32 * t;
+                if (r < BSZ) ys[wib][g][r] = acc[t];
+            }
+        }
+        __syncwarp();
+        double y[R];
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+            const int r = lane + 32 * t;
+            double s = 0.0;
+            if (r < BSZ)
+#pragma unroll
+                for (int gg = 0; gg < G; gg++) s += ys[wib][gg][r];
+            y[t] = s;
+        }
+        __syncwarp();
+        if (!Minv) {
+#pragma unroll
+            for (int t = 0; t < R; t++) {
+                const int r = lane + 32 * t;
+                if (r < BSZ) z[(size_t)i * BSZ + r] = y[t];
+            }
+            continue;
+        }
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+            const int r = lane + 32 * t;
+            if (r < BSZ) ys[wib][0][r] = y[t];
+        }
+        __syncwarp();
+        const double* m = Minv + (size_t)i * BSZ * BSZ;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+            const int r = lane + 32 * t;
+            if (r < BSZ) {
+                double s = 0.0;
+#pragma unroll 4
+                for (int c = 0; c < BSZ; c++) s += __ldg(&m[(size_t)c * BSZ + r]) * ys[wib][0][c];
+                z[(size_t)i * BSZ + r] = s;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace hfem

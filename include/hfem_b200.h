@@ -124,6 +124,24 @@ int hfem_newton(hfem_ctx* ctx, double newton_tol, int newton_maxiter, int precon
 int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newton_tol, int newton_maxiter,
                    int precond, int restart, double gmres_tol, int gmres_maxit, int* newton_iters);
 
+/* Several independent problems in one context (a disjoint union of meshes, so
+ * element work of many requests runs in one launch; no counterpart in the
+ * reference, which runs one problem per process).  eprob (ne) and fprob (nf)
+ * map elements and faces to problems; params holds per problem
+ * [gamma, eps, Re, Pr, Mach, tau, tdep, fc_u]. */
+int hfem_set_problem_map(hfem_ctx* ctx, int nprob, const int* eprob, const int* fprob, const double* params);
+/* Residual norm of each problem after hfem_assemble / hfem_residual
+ * (computeResidualNorm restricted to the problem's elements and faces). */
+int hfem_problem_rnorms(hfem_ctx* ctx, double* rnorm);
+/* updateSol with one step length per problem (alpha[nprob], host). */
+int hfem_update_problems(hfem_ctx* ctx, const double* alpha);
+/* GMRES for every problem of the context at once: the algorithm of hfem_gmres
+ * (kernel/gmres_bilu0.m:17-105) run per problem, with each problem's own
+ * Krylov basis, Hessenberg matrix and stopping test, sharing the launches.
+ * Needs a problem map whose fprob is non-decreasing with every problem owning
+ * a face.  conv[nprob] and iters[nprob] as in hfem_gmres. */
+int hfem_gmres_problems(hfem_ctx* ctx, int precond, int restart, double tol, int maxit, int* conv, int* iters);
+
 /* Download device results for inspection (host buffers of the given length):
  * what = 0 Hg (nblocks*bsz^2), 1 Rg (nf*bsz), 2 Rr = sum of uncondensed Rh
  * (nf*bsz), 3 DinvRu (n*ne), 4 DinvF (n*nb*ne), 5 condensed element H
