@@ -40,6 +40,8 @@ WORKLOADS = {
                         label="3D NS HDG, periodic unit cube 20^3x6 tets = 48000 elements, p=3, Re 400, Mach 0.3"),
     "ns3d_p3_6k": dict(kind="ns3d_fourier", n=10, porder=3,
                        label="3D NS HDG, periodic unit cube 10^3x6 tets = 6000 elements, p=3 (profiling size)"),
+    "ns3d_p3_3k": dict(kind="ns3d_fourier", n=8, porder=3,
+                       label="3D NS HDG, periodic unit cube 8^3x6 tets = 3072 elements, p=3 (ncu capture size)"),
     "ns2d_p2_2k": dict(kind="ns2d_vortex", n=32, porder=2,
                        label="2D NS HDG, periodic [0,10]^2 32x32x2 tris = 2048 elements, p=2, Re 100, Mach 0.5"),
 }
@@ -247,10 +249,40 @@ def run_gpu(args, rank, world, local_rank):
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
+    # mixed precision leg: the same step with the Schur GEMMs on the tcgen05 tensor cores (TF32)
+    mixed_ms, mixed_k, mixed_err = 0.0, {}, {}
+    if not args.no_mixed:
+        solver.set_solution(udg_q, uh0, prob.sh)
+        solver.assembleLinearSystem()
+        ref = {k: solver.device_tensor(k).clone() for k in ("Hg", "DinvF")}
+        r64 = solver.assembleLinearSystem()
+        solver.set_precision(1)
+        for _ in range(max(3, args.warmup)):
+            solver.assembleLinearSystem()
+        solver.set_timing(True)
+        barrier()
+        torch.cuda.synchronize()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            r32 = solver.assembleLinearSystem()
+        m1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        mixed_ms = m0.elapsed_time(m1)
+        mixed_k = solver.kernel_times()
+        solver.set_timing(False)
+        for k, v in ref.items():
+            cur = solver.device_tensor(k)
+            mixed_err[k] = float((cur - v).abs().max() / v.abs().max())
+        mixed_err["rnorm"] = abs(r32 - r64) / r64
+        del ref
+        solver.set_precision(0)
+
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        t = torch.tensor([ms, e2e_ms, mixed_ms], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+        ms, e2e_ms, mixed_ms = float(t[0]), float(t[1]), float(t[2])
     solver.close()
     if rank != 0:
         return None
@@ -303,6 +335,16 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": launches,
         "rnorm": rnorm,
     }
+    if not args.no_mixed:
+        tc_ms = mixed_k.get("schur_tc", (0.0, 1))
+        line["mixed"] = {
+            "metric": "assembly+Schur elements/s (TF32 tensor-core Schur GEMMs, FP64 LU/residual)",
+            "value": world * ne * args.steps / (mixed_ms * 1e-3), "unit": "elements/s",
+            "ms_per_step": mixed_ms / args.steps, "speedup_vs_fp64": ms / mixed_ms,
+            "error_vs_fp64": mixed_err,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in mixed_k.items()},
+            "schur_tc_tflops": (2.0 * prob.n_local * prob.n_trace * (prob.n_local + prob.n_trace)) * ne
+                               / (tc_ms[0] / tc_ms[1] * 1e-3) / 1e12 if tc_ms[0] > 0 else None}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu(args.workload, seconds_per_proc=args.cpu_seconds)
     return line
@@ -462,6 +504,7 @@ def main():
     ap.add_argument("--workload", default="ns3d_p3_48k", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (TF32 Schur) leg")
     ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve"])
     ap.add_argument("--tgv-n", type=int, default=16)
     ap.add_argument("--dirk-steps", type=int, default=20)

@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhfem_b200.so")
 SOURCES = ["hfem_capi.cu"]
-HEADERS = ["elem_kernels.cuh", "krylov_kernels.cuh", "ns_flux.cuh", "schur_kernels.cuh", "krylov_seg.cuh", "elem_kernel_v2.cuh"]
+HEADERS = ["elem_kernels.cuh", "krylov_kernels.cuh", "ns_flux.cuh", "schur_kernels.cuh", "krylov_seg.cuh", "schur_tc.cuh", "elem_kernel_v2.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "177"]
 

@@ -66,6 +66,8 @@ def load_library(path: str = LIB):
     lib.hfem_dirk_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
                                    C.c_double, C.c_int, _ip]
     lib.hfem_set_timing.argtypes = [C.c_void_p, C.c_int]
+    lib.hfem_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.hfem_device_buffer.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]
     lib.hfem_kernel_times.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, _dp, _ip, C.c_int]
     _lib = lib
     return lib
@@ -163,6 +165,17 @@ class HDGSolver:
         self._chk(self.lib.hfem_download(self.h, DOWNLOAD[what], _d(out), out.size), f"download {what}")
         return out
 
+    def device_tensor(self, what):
+        """A torch view (float64, cuda) of one of the context's device buffers (no copy)."""
+        import torch
+        ptr, cnt = C.c_void_p(), C.c_size_t()
+        self._chk(self.lib.hfem_device_buffer(self.h, DOWNLOAD[what], C.byref(ptr), C.byref(cnt)), f"buffer {what}")
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (cnt.value,), "typestr": "<f8", "data": (ptr.value, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_View(), device=f"cuda:{torch.cuda.current_device()}")
+
     # -- reference surface ---------------------------------------------
     def getQ(self):
         self._chk(self.lib.hfem_getq(self.h), "getQ")
@@ -202,6 +215,10 @@ class HDGSolver:
         self._chk(self.lib.hfem_dirk_step(self.h, float(dt), stages, order, newton_tol, newton_maxiter, precond,
                                           restart, gmres_tol, gmres_maxit, C.byref(it)), "solveUnsteadyStep")
         return it.value
+
+    def set_precision(self, mode):
+        """0: FP64 throughout; 1: TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)."""
+        self._chk(self.lib.hfem_set_precision(self.h, int(mode)), "set_precision")
 
     def set_timing(self, on=True):
         self._chk(self.lib.hfem_set_timing(self.h, 1 if on else 0), "set_timing")

@@ -416,24 +416,36 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 double acc[C3<S>::NTK][2];
 #pragma unroll
                 for (int b = 0; b < C3<S>::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
-#pragma unroll 8
+                // the m-tile's A values for every k-step are loaded before the first
+                // DMMA, so their latencies overlap
+                double av[C3<S>::KV3 / 4];
+#pragma unroll
                 for (int ks = 0; ks < C3<S>::KV3 / 4; ks++) {
                     const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
-                    const double a = (rv && kk < NGV * ND1) ? yrow[(size_t)N * (g + NGV * NCU * dp)] : 0.0;
+                    av[ks] = (rv && kk < NGV * ND1) ? yrow[(size_t)N * (g + NGV * NCU * dp)] : 0.0;
+                }
+#pragma unroll
+                for (int ks = 0; ks < C3<S>::KV3 / 4; ks++) {
+                    const int kk = 4 * ks + gc;
 #pragma unroll
                     for (int b = 0; b < C3<S>::NTK; b++)
-                        dmma8x8x4(acc[b][0], acc[b][1], a, Phi[kk + C3<S>::LDBD * (8 * b + gr)]);
+                        dmma8x8x4(acc[b][0], acc[b][1], av[ks], Phi[kk + C3<S>::LDBD * (8 * b + gr)]);
                 }
                 double accf[C3<S>::NTH][2];
 #pragma unroll
                 for (int b = 0; b < C3<S>::NTH; b++) accf[b][0] = accf[b][1] = 0.0;
-#pragma unroll 8
+                double aq[C3<S>::KQ3 / 4];
+#pragma unroll
                 for (int ks = 0; ks < C3<S>::KQ3 / 4; ks++) {
                     const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
-                    const double a = (rv && kk < NGV * ND) ? yrow[(size_t)N * (g + NGV * NCU * (d + 1))] : 0.0;
+                    aq[ks] = (rv && kk < NGV * ND) ? yrow[(size_t)N * (g + NGV * NCU * (d + 1))] : 0.0;
+                }
+#pragma unroll
+                for (int ks = 0; ks < C3<S>::KQ3 / 4; ks++) {
+                    const int kk = 4 * ks + gc;
 #pragma unroll
                     for (int b = 0; b < C3<S>::NTH; b++)
-                        dmma8x8x4(accf[b][0], accf[b][1], a, Psi[kk + C3<S>::LDBD * (8 * b + gr)]);
+                        dmma8x8x4(accf[b][0], accf[b][1], aq[ks], Psi[kk + C3<S>::LDBD * (8 * b + gr)]);
                 }
                 if (rv) {
 #pragma unroll

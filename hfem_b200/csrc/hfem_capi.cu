@@ -21,6 +21,7 @@
 #include "krylov_seg.cuh"
 #include "schur_kernels.cuh"
 #include "elem_kernel_v2.cuh"
+#include "schur_tc.cuh"
 
 using namespace hfem;
 
@@ -93,6 +94,9 @@ struct Launch {
     int inv_threads;
     const void *elem_fn, *schur_fn, *q_fn, *inv_fn;
     GemmLaunch g1, g2;
+    void (*schur_tc)(dim3, size_t, cudaStream_t, const SchurTcArgs&);
+    size_t tc_smem;
+    const void* tc_fn;
 };
 
 template <int N>
@@ -108,6 +112,10 @@ template <class S>
 void launch_schur(dim3 g, size_t sm, cudaStream_t st, const SchurArgs& a) { schur_kernel<S::N, S::NB><<<g, NT, sm, st>>>(a); }
 template <class S>
 void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
+template <class S>
+void launch_schur_tc(dim3 g, size_t sm, cudaStream_t st, const SchurTcArgs& a) {
+    schur_tc_kernel<S::N, S::NB><<<g, TC_THREADS, sm, st>>>(a);
+}
 
 template <class S>
 Launch make_launch() {
@@ -132,6 +140,9 @@ Launch make_launch() {
     L.inv_fn = (const void*)inverse_kernel<S::N>;
     L.g1 = GemmParams<typename SchurCfg<S>::g1>::make();
     L.g2 = GemmParams<typename SchurCfg<S>::g2>::make();
+    L.schur_tc = launch_schur_tc<S>;
+    L.tc_smem = TcCfg<S::N, S::NB>::SMEM;
+    L.tc_fn = (const void*)schur_tc_kernel<S::N, S::NB>;
     return L;
 }
 
@@ -154,7 +165,9 @@ struct hfem_ctx {
     cudaStream_t own = nullptr, stream = nullptr;
     std::string err;
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
-    int grid_elem = 0, grid_schur = 0, grid_inv = 0;
+    int grid_elem = 0, grid_schur = 0, grid_inv = 0, grid_tc = 0;
+    int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
+    int* tc_err = nullptr;
     // master tables
     double *shapvt = nullptr, *shapvg = nullptr, *svsv = nullptr, *shapft = nullptr, *shapfg = nullptr, *sfsf = nullptr;
     int* perm = nullptr;
@@ -353,17 +366,28 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
             c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
-        {
-            Timed t(c, "gemm_DinvF");
-            c->L->g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb, 0.0,
-                         c->DinvF, n, (long long)n * nb);
-            if ((rc = check_launch(c, "gemm_DinvF"))) return rc;
-        }
-        {
-            Timed t(c, "gemm_schur");
-            c->L->g2.run(c->stream, ne, nb, nb, n, -1.0, c->K, nb, (long long)nb * n, c->DinvF, n, (long long)n * nb,
-                         1.0, c->H, nb, (long long)nb * nb);
-            if ((rc = check_launch(c, "gemm_schur"))) return rc;
+        if (c->precision == 0) {
+            {
+                Timed t(c, "gemm_DinvF");
+                c->L->g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb,
+                             0.0, c->DinvF, n, (long long)n * nb);
+                if ((rc = check_launch(c, "gemm_DinvF"))) return rc;
+            }
+            {
+                Timed t(c, "gemm_schur");
+                c->L->g2.run(c->stream, ne, nb, nb, n, -1.0, c->K, nb, (long long)nb * n, c->DinvF, n,
+                             (long long)n * nb, 1.0, c->H, nb, (long long)nb * nb);
+                if ((rc = check_launch(c, "gemm_schur"))) return rc;
+            }
+        } else {
+            if (!c->tc_err) {
+                if ((rc = dalloc(c, &c->tc_err, 1))) return rc;
+                CK(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
+            }
+            Timed t(c, "schur_tc");
+            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err};
+            c->L->schur_tc(dim3(c->grid_tc), c->L->tc_smem, c->stream, ta);
+            if ((rc = check_launch(c, "schur_tc"))) return rc;
         }
         {
             Timed t(c, "gemv_Rh");
@@ -392,6 +416,12 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
         CK(cudaStreamSynchronize(c->stream));
         for (int e = 0; e < c->dims.ne; e++)
             if (info[e]) return fail(c, HFEM_E_SINGULAR, "element %d: singular local matrix (pivot %d)", e, info[e]);
+        if (c->precision && c->tc_err) {
+            int terr = 0;
+            CK(cudaMemcpyAsync(&terr, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaStreamSynchronize(c->stream));
+            if (terr) return fail(c, HFEM_E_CUDA, "tensor-core Schur kernel: an MMA completion wait expired");
+        }
         c->assembled = true;
     }
     double rn = 0.0;
@@ -875,6 +905,11 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     c->grid_schur = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
+    cudaFuncSetAttribute(L.tc_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.tc_smem);
+    occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.tc_fn, TC_THREADS, L.tc_smem);
+    // each CTA holds 256 of the SM's 512 tensor-memory columns
+    c->grid_tc = std::max(1, std::min(d.ne, sms(device) * std::max(1, std::min(occ, 2))));
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.inv_fn, L.inv_threads, 0);
     c->grid_inv = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
@@ -902,7 +937,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
-                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k};
+                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& p : c->timer.pending) {
@@ -1289,28 +1324,48 @@ int hfem_update_problems(hfem_ctx* c, const double* alpha) {
     return 0;
 }
 
+int hfem_set_precision(hfem_ctx* c, int mode) {
+    if (!c) return HFEM_E_ARG;
+    if (mode != 0 && mode != 1) return fail(c, HFEM_E_ARG, "precision mode must be 0 (FP64) or 1 (TF32 Schur)");
+    c->precision = mode;
+    c->assembled = false;
+    return 0;
+}
+
 int hfem_gmres_problems(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters) {
     if (!c) return HFEM_E_ARG;
     return gmres_seg_impl(c, precond, restart, tol, maxit, conv, iters);
 }
 
+int device_buffer(hfem_ctx* c, int what, const double** src, size_t* need) {
+    const hfem_dims& d = c->dims;
+    switch (what) {
+        case 0: *src = c->Hg; *need = (size_t)d.nblocks * c->bsz * c->bsz; break;
+        case 1: *src = c->Rg; *need = (size_t)d.nf * c->bsz; break;
+        case 2: *src = c->Rr; *need = (size_t)d.nf * c->bsz; break;
+        case 3: *src = c->Ru; *need = (size_t)d.ne * c->n; break;
+        case 4: *src = c->DinvF; *need = (size_t)d.ne * c->n * c->nb; break;
+        case 5: *src = c->H; *need = (size_t)d.ne * c->nb * c->nb; break;
+        case 6: *src = c->Rh; *need = (size_t)d.ne * c->nb; break;
+        case 7: *src = c->x; *need = (size_t)d.nf * c->bsz; break;
+        default: return fail(c, HFEM_E_ARG, "unknown buffer %d", what);
+    }
+    if (!*src) return fail(c, HFEM_E_STATE, "nothing computed for buffer %d yet", what);
+    return 0;
+}
+
+int hfem_device_buffer(hfem_ctx* c, int what, const double** ptr, size_t* count) {
+    if (!c || !ptr || !count) return HFEM_E_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return device_buffer(c, what, ptr, count);
+}
+
 int hfem_download(hfem_ctx* c, int what, double* host, size_t count) {
     if (!c || !host) return HFEM_E_ARG;
-    const hfem_dims& d = c->dims;
     const double* src = nullptr;
     size_t need = 0;
-    switch (what) {
-        case 0: src = c->Hg; need = (size_t)d.nblocks * c->bsz * c->bsz; break;
-        case 1: src = c->Rg; need = (size_t)d.nf * c->bsz; break;
-        case 2: src = c->Rr; need = (size_t)d.nf * c->bsz; break;
-        case 3: src = c->Ru; need = (size_t)d.ne * c->n; break;
-        case 4: src = c->DinvF; need = (size_t)d.ne * c->n * c->nb; break;
-        case 5: src = c->H; need = (size_t)d.ne * c->nb * c->nb; break;
-        case 6: src = c->Rh; need = (size_t)d.ne * c->nb; break;
-        case 7: src = c->x; need = (size_t)d.nf * c->bsz; break;
-        default: return fail(c, HFEM_E_ARG, "unknown download target %d", what);
-    }
-    if (!src) return fail(c, HFEM_E_STATE, "nothing computed for target %d yet", what);
+    int rc = device_buffer(c, what, &src, &need);
+    if (rc) return rc;
     if (count < need) return fail(c, HFEM_E_ARG, "buffer of %zu < %zu entries", count, need);
     CK(cudaMemcpyAsync(host, src, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -124,6 +124,21 @@ int hfem_newton(hfem_ctx* ctx, double newton_tol, int newton_maxiter, int precon
 int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newton_tol, int newton_maxiter,
                    int precond, int restart, double gmres_tol, int gmres_maxit, int* newton_iters);
 
+/* Arithmetic of the assembly (no counterpart in the reference, which is FP64
+ * throughout).  mode 0: FP64 everywhere (default).  mode 1: the two Schur
+ * GEMMs (D^-1 F and H - K D^-1 F) on the tcgen05 tensor cores in TF32 with
+ * FP32 accumulation; the element LU, the residuals (rnorm), the Arnoldi
+ * process and the Newton update stay FP64, so Newton iterations refine the
+ * solution to the FP64 residual tolerance. */
+int hfem_set_precision(hfem_ctx* ctx, int mode);
+
+/* Device address and length (doubles) of one of the context's buffers, with
+ * the ids of hfem_download, for zero-copy use on the device after the
+ * context's stream has been synchronised (done here).  The buffer belongs to
+ * the context and moves when the context reallocates it.  No counterpart in
+ * the reference (its arrays live in host structs). */
+int hfem_device_buffer(hfem_ctx* ctx, int what, const double** ptr, size_t* count);
+
 /* Several independent problems in one context (a disjoint union of meshes, so
  * element work of many requests runs in one launch; no counterpart in the
  * reference, which runs one problem per process).  eprob (ne) and fprob (nf)
