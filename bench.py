@@ -495,6 +495,71 @@ def run_serve_task(args):
     return out
 
 
+def run_batched_task(args):
+    """Config 3: 64 periodic 2D NS meshes, 512-32,768 elements (log-uniform), p in
+    {1,2,3,4}, Mach U[0.2,0.8], vortex + noise.  One assembly pass over all of
+    them as (a) plain per-mesh FP64 calls, (b) one graph launch in FP64 with
+    autotuned tilings, (c) one graph launch with the TF32 tensor-core Schur GEMMs."""
+    import math
+    import torch
+    from hfem_b200.batched import MixedOrderAssembly
+    from hfem_b200.core import HDGSolver
+    from hfem_b200.gen.problem import ns2d_vortex
+    rng = np.random.default_rng(args.batched_seed)
+    probs = []
+    for i in range(args.batched_meshes):
+        ne = math.exp(rng.uniform(math.log(512), math.log(32768)))
+        n = max(4, int(round(math.sqrt(ne / 2))))
+        probs.append(ns2d_vortex(n=n, porder=int(rng.integers(1, 5)), seed=1000 + i,
+                                 mach=float(rng.uniform(0.2, 0.8))))
+    ne = sum(p.mesh.ne for p in probs)
+    # (a) plain FP64: one context and one assembleLinearSystem call per mesh
+    plain = [HDGSolver(p) for p in probs]
+    for s in plain:
+        s.getQ()
+        s.assembleLinearSystem()
+    torch.cuda.synchronize()
+    t_plain = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r_plain = [s.assembleLinearSystem() for s in plain]
+        e1.record()
+        torch.cuda.synchronize()
+        t_plain.append(e0.elapsed_time(e1))
+    for s in plain:
+        s.close()
+    out = {"metric": "batched mixed-order assembly+Schur elements/s (64 2D NS meshes, p 1-4)",
+           "unit": "elements/s", "impl": "hfem", "higher_is_better": True, "data": "synthetic",
+           "elements": ne, "meshes": len(probs), "steps": args.steps,
+           "orders": {str(p): int(sum(q.mesh.ne for q in probs if q.master.porder == p)) for p in (1, 2, 3, 4)},
+           "plain_fp64": {"value": ne / (np.median(t_plain) * 1e-3), "ms": float(np.median(t_plain))}}
+    for name, prec in (("graph_fp64", 0), ("graph_mixed", 1)):
+        m = MixedOrderAssembly(probs, precision=prec, tune=True)
+        for _ in range(max(3, args.warmup)):
+            m.launch()
+        m.finish()
+        ts = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(m.stream)
+            m.launch()
+            e1.record(m.stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        rn = m.finish()
+        out[name] = {"value": ne / (np.median(ts) * 1e-3), "ms": float(np.median(ts)),
+                     "max_rnorm_rel_diff_vs_plain": float(np.max(np.abs(rn - np.array(r_plain)) / np.array(r_plain))),
+                     "tiles": {f"{k[0]}d_p{k[1]}": v for k, v in m.tiles.items()}}
+        if prec == 1:
+            out[name]["dtype"] = "tf32 Schur GEMMs, f64 element LU / residual"
+        m.close()
+    out["value"] = out["graph_mixed"]["value"]
+    out["speedup_graph_mixed_vs_plain_fp64"] = out["graph_mixed"]["value"] / out["plain_fp64"]["value"]
+    out["speedup_graph_fp64_vs_plain_fp64"] = out["graph_fp64"]["value"] / out["plain_fp64"]["value"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -505,7 +570,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (TF32 Schur) leg")
-    ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve"])
+    ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve", "batched"])
+    ap.add_argument("--batched-meshes", type=int, default=64)
+    ap.add_argument("--batched-seed", type=int, default=0)
     ap.add_argument("--tgv-n", type=int, default=16)
     ap.add_argument("--dirk-steps", type=int, default=20)
     ap.add_argument("--dirk-tol", type=float, default=1e-9)
@@ -516,7 +583,8 @@ def main():
     ap.add_argument("--serve-gmres-tol", type=float, default=1e-10)
     args = ap.parse_args()
     if args.task != "assembly":
-        line = {"newton": run_newton_task, "dirk": run_dirk_task, "serve": run_serve_task}[args.task](args)
+        line = {"newton": run_newton_task, "dirk": run_dirk_task, "serve": run_serve_task,
+                "batched": run_batched_task}[args.task](args)
         print(json.dumps(line), flush=True)
         return
     args.warmup = max(args.warmup, 3) if args.impl == "hfem" else args.warmup

@@ -79,6 +79,20 @@ template <int MT, int WN, int NW> struct GemmParams<GemmCfg<MT, WN, NW>> {
     }
 };
 
+// Every batched-GEMM tiling compiled into the library; any of them is valid
+// for any shape (edges are masked), so the autotuner may pick any.
+const std::vector<GemmLaunch>& gemm_candidates() {
+    static std::vector<GemmLaunch> v = {
+        GemmParams<GemmCfg<2, 3, 1>>::make(), GemmParams<GemmCfg<3, 3, 1>>::make(),
+        GemmParams<GemmCfg<3, 5, 1>>::make(), GemmParams<GemmCfg<5, 5, 1>>::make(),
+        GemmParams<GemmCfg<5, 3, 2>>::make(), GemmParams<GemmCfg<6, 3, 2>>::make(),
+        GemmParams<GemmCfg<4, 4, 2>>::make(), GemmParams<GemmCfg<3, 4, 2>>::make(),
+        GemmParams<GemmCfg<7, 3, 5>>::make(), GemmParams<GemmCfg<5, 3, 5>>::make(),
+        GemmParams<GemmCfg<5, 5, 5>>::make(), GemmParams<GemmCfg<4, 2, 4>>::make(),
+    };
+    return v;
+}
+
 struct Launch {
     int nd, npv, npf, ngv, ngf;
     size_t ws;                  // workspace doubles per CTA slot (element_kernel)
@@ -167,6 +181,7 @@ struct hfem_ctx {
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
     int grid_elem = 0, grid_schur = 0, grid_inv = 0, grid_tc = 0;
     int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
+    int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
     int* tc_err = nullptr;
     // master tables
     double *shapvt = nullptr, *shapvg = nullptr, *svsv = nullptr, *shapft = nullptr, *shapfg = nullptr, *sfsf = nullptr;
@@ -306,6 +321,8 @@ int ensure_assembly_buffers(hfem_ctx* c) {
     if ((rc = dalloc(c, &c->ru2, ne))) return rc;
     if ((rc = dalloc(c, &c->info, ne))) return rc;
     if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws2))) return rc;
+    if ((rc = dalloc(c, &c->tc_err, 1))) return rc;
+    CK(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
     return 0;
 }
 
@@ -347,11 +364,11 @@ int ready(hfem_ctx* c) {
     return 0;
 }
 
-// Element pass: local blocks, condensation (matrix=true) and scatter.
-int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
-    int rc = ready(c);
-    if (rc) return rc;
-    if ((rc = ensure_assembly_buffers(c))) return rc;
+// Element pass: local blocks, condensation (matrix=true) and scatter, as
+// launches on the context's stream only (no host synchronisation, so the
+// sequence can be captured into a CUDA graph).  Buffers must exist.
+int enqueue_assembly(hfem_ctx* c, bool matrix) {
+    int rc;
     const dim3 ge(c->grid_elem);
     {
         Timed t(c, "element");
@@ -367,23 +384,21 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
         if (c->precision == 0) {
+            const GemmLaunch& g1 = c->g1_sel >= 0 ? gemm_candidates()[c->g1_sel] : c->L->g1;
+            const GemmLaunch& g2 = c->g2_sel >= 0 ? gemm_candidates()[c->g2_sel] : c->L->g2;
             {
                 Timed t(c, "gemm_DinvF");
-                c->L->g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb,
-                             0.0, c->DinvF, n, (long long)n * nb);
+                g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb, 0.0,
+                       c->DinvF, n, (long long)n * nb);
                 if ((rc = check_launch(c, "gemm_DinvF"))) return rc;
             }
             {
                 Timed t(c, "gemm_schur");
-                c->L->g2.run(c->stream, ne, nb, nb, n, -1.0, c->K, nb, (long long)nb * n, c->DinvF, n,
-                             (long long)n * nb, 1.0, c->H, nb, (long long)nb * nb);
+                g2.run(c->stream, ne, nb, nb, n, -1.0, c->K, nb, (long long)nb * n, c->DinvF, n, (long long)n * nb,
+                       1.0, c->H, nb, (long long)nb * nb);
                 if ((rc = check_launch(c, "gemm_schur"))) return rc;
             }
         } else {
-            if (!c->tc_err) {
-                if ((rc = dalloc(c, &c->tc_err, 1))) return rc;
-                CK(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
-            }
             Timed t(c, "schur_tc");
             SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err};
             c->L->schur_tc(dim3(c->grid_tc), c->L->tc_smem, c->stream, ta);
@@ -409,14 +424,19 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
         if ((rc = check_launch(c, "scatter_R"))) return rc;
     }
     rnorm_kernel<<<1, 1024, 0, c->stream>>>(c->dims.ne, c->ru2, c->dims.nf * c->bsz, c->Rr, c->rnorm);
-    if ((rc = check_launch(c, "rnorm"))) return rc;
+    return check_launch(c, "rnorm");
+}
+
+// Wait for an enqueued assembly, check the element LUs (and the tensor-core
+// kernel) and read the residual norm.
+int finish_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
     if (matrix) {
         std::vector<int> info(c->dims.ne);
         CK(cudaMemcpyAsync(info.data(), c->info, sizeof(int) * info.size(), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         for (int e = 0; e < c->dims.ne; e++)
             if (info[e]) return fail(c, HFEM_E_SINGULAR, "element %d: singular local matrix (pivot %d)", e, info[e]);
-        if (c->precision && c->tc_err) {
+        if (c->precision) {
             int terr = 0;
             CK(cudaMemcpyAsync(&terr, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
@@ -430,6 +450,14 @@ int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
     flush_timer(c);
     if (rnorm_out) *rnorm_out = rn;
     return 0;
+}
+
+int run_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
+    int rc = ready(c);
+    if (rc) return rc;
+    if ((rc = ensure_assembly_buffers(c))) return rc;
+    if ((rc = enqueue_assembly(c, matrix))) return rc;
+    return finish_assembly(c, matrix, rnorm_out);
 }
 
 int launch_getq(hfem_ctx* c, const double* duh, double alpha) {
@@ -906,6 +934,8 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
     cudaFuncSetAttribute(L.tc_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.tc_smem);
+    for (const GemmLaunch& g : gemm_candidates())
+        cudaFuncSetAttribute(g.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.tc_fn, TC_THREADS, L.tc_smem);
     // each CTA holds 256 of the SM's 512 tensor-memory columns
@@ -1321,6 +1351,160 @@ int hfem_update_problems(hfem_ctx* c, const double* alpha) {
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     flush_timer(c);
+    return 0;
+}
+
+int hfem_assemble_async(hfem_ctx* c) {
+    int rc = ready(c);
+    if (rc) return rc;
+    if ((rc = ensure_assembly_buffers(c))) return rc;
+    return enqueue_assembly(c, true);
+}
+
+int hfem_assemble_finish(hfem_ctx* c, double* rnorm) {
+    if (!c) return HFEM_E_ARG;
+    return finish_assembly(c, true, rnorm);
+}
+
+int hfem_gemm_candidates(void) { return (int)gemm_candidates().size(); }
+
+int hfem_set_gemm_tiles(hfem_ctx* c, int g1, int g2) {
+    if (!c) return HFEM_E_ARG;
+    const int nc = (int)gemm_candidates().size();
+    if (g1 < -1 || g1 >= nc || g2 < -1 || g2 >= nc) return fail(c, HFEM_E_ARG, "tiling index out of range");
+    c->g1_sel = g1;
+    c->g2_sel = g2;
+    return 0;
+}
+
+// Time every batched-GEMM tiling on this context's own operands (reps
+// launches each, CUDA events on the context's stream) and keep the fastest
+// for D^-1 F and for the Schur update.  The condensed blocks are overwritten
+// while timing, so the context must be assembled again before it is used.
+int hfem_autotune(hfem_ctx* c, int reps, int* best, double* ms) {
+    if (!c || reps < 1) return HFEM_E_ARG;
+    int rc = ready(c);
+    if (rc) return rc;
+    if ((rc = ensure_assembly_buffers(c))) return rc;
+    const bool timing = c->timer.on;
+    c->timer.on = false;
+    if ((rc = enqueue_assembly(c, true))) return rc;
+    if ((rc = finish_assembly(c, true, nullptr))) return rc;
+    const int ne = c->dims.ne, n = c->n, nb = c->nb;
+    const auto& cand = gemm_candidates();
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double bt[2] = {1e300, 1e300};
+    int bi[2] = {-1, -1};
+    for (int which = 0; which < 2; which++)
+        for (size_t k = 0; k < cand.size(); k++) {
+            const GemmLaunch& g = cand[k];
+            auto launch = [&]() {
+                if (which == 0)
+                    g.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb, 0.0,
+                          c->DinvF, n, (long long)n * nb);
+                else
+                    g.run(c->stream, ne, nb, nb, n, -1.0, c->K, nb, (long long)nb * n, c->DinvF, n,
+                          (long long)n * nb, 1.0, c->H, nb, (long long)nb * nb);
+            };
+            launch();                                      // warm-up
+            if ((rc = check_launch(c, "autotune"))) return rc;
+            CK(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < reps; r++) launch();
+            CK(cudaEventRecord(e1, c->stream));
+            CK(cudaEventSynchronize(e1));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, e0, e1));
+            const double per = (double)t / reps;
+            if (ms) ms[which * cand.size() + k] = per;
+            if (per < bt[which]) bt[which] = per, bi[which] = (int)k;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->g1_sel = bi[0];
+    c->g2_sel = bi[1];
+    c->assembled = false;
+    c->timer.on = timing;
+    if (best) best[0] = bi[0], best[1] = bi[1];
+    return 0;
+}
+
+struct hfem_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev;
+};
+
+// One CUDA graph holding the assembly of several contexts (e.g. one per
+// element shape), each on its own branch so they run concurrently.
+int hfem_graph_capture(hfem_ctx** ctxs, int n, void* stream, hfem_graph** out) {
+    if (!ctxs || n < 1 || !stream || !out) return HFEM_E_ARG;
+    hfem_ctx* c0 = ctxs[0];
+    hfem_ctx* c = c0;
+    for (int i = 0; i < n; i++) {
+        if (!ctxs[i] || ctxs[i]->device != c0->device) return fail(c0, HFEM_E_ARG, "contexts must share a device");
+        int rc = ready(ctxs[i]);
+        if (rc) return rc;
+        if ((rc = ensure_assembly_buffers(ctxs[i]))) return rc;
+        CK(cudaStreamSynchronize(ctxs[i]->stream));
+    }
+    CK(cudaSetDevice(c0->device));
+    auto* g = new hfem_graph();
+    g->side.resize(n);
+    g->ev.resize(n + 1);
+    for (int i = 0; i < n; i++) CK(cudaStreamCreateWithFlags(&g->side[i], cudaStreamNonBlocking));
+    for (int i = 0; i <= n; i++) CK(cudaEventCreateWithFlags(&g->ev[i], cudaEventDisableTiming));
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<cudaStream_t> saved(n);
+    std::vector<bool> timing(n);
+    int rc = 0;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(g->ev[n], s);
+    for (int i = 0; i < n && !rc; i++) {
+        saved[i] = ctxs[i]->stream;
+        timing[i] = ctxs[i]->timer.on;
+        ctxs[i]->timer.on = false;
+        ctxs[i]->stream = g->side[i];
+        cudaStreamWaitEvent(g->side[i], g->ev[n], 0);
+        rc = enqueue_assembly(ctxs[i], true);
+        cudaEventRecord(g->ev[i], g->side[i]);
+        cudaStreamWaitEvent(s, g->ev[i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &graph);
+    for (int i = 0; i < n; i++)
+        if (saved[i]) ctxs[i]->stream = saved[i], ctxs[i]->timer.on = timing[i];
+    if (rc || ee != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        hfem_graph_destroy(g);
+        return rc ? rc : fail(c, HFEM_E_CUDA, "graph capture: %s", cudaGetErrorString(ee));
+    }
+    g->graph = graph;
+    const cudaError_t ie = cudaGraphInstantiate(&g->exec, graph, 0);
+    if (ie != cudaSuccess) {
+        hfem_graph_destroy(g);
+        return fail(c, HFEM_E_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+    }
+    *out = g;
+    return 0;
+}
+
+int hfem_graph_launch(hfem_graph* g, void* stream) {
+    if (!g || !g->exec || !stream) return HFEM_E_ARG;
+    return cudaGraphLaunch(g->exec, (cudaStream_t)stream) == cudaSuccess ? 0 : HFEM_E_CUDA;
+}
+
+int hfem_graph_destroy(hfem_graph* g) {
+    if (!g) return HFEM_E_ARG;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    for (auto st : g->side)
+        if (st) cudaStreamDestroy(st);
+    for (auto e : g->ev)
+        if (e) cudaEventDestroy(e);
+    delete g;
     return 0;
 }
 

@@ -139,6 +139,32 @@ int hfem_set_precision(hfem_ctx* ctx, int mode);
  * the reference (its arrays live in host structs). */
 int hfem_device_buffer(hfem_ctx* ctx, int what, const double** ptr, size_t* count);
 
+/* Assembly split in two for graph capture: hfem_assemble_async only enqueues
+ * the kernels of hfem_assemble on the context's stream (buffers are
+ * allocated first if needed); hfem_assemble_finish waits, checks the element
+ * LUs and returns the residual norm.  Together they equal hfem_assemble. */
+int hfem_assemble_async(hfem_ctx* ctx);
+int hfem_assemble_finish(hfem_ctx* ctx, double* rnorm);
+
+/* Batched-GEMM tilings compiled into the library (any is valid for any
+ * shape); hfem_autotune times them all on the context's own operands and
+ * keeps the fastest for D^-1 F and for H - K D^-1 F (best[2], ms[2 * count]
+ * may be NULL); hfem_set_gemm_tiles applies a stored choice (-1: default).
+ * No counterpart in the reference (its BLAS picks its own kernels). */
+int hfem_gemm_candidates(void);
+int hfem_autotune(hfem_ctx* ctx, int reps, int* best, double* ms);
+int hfem_set_gemm_tiles(hfem_ctx* ctx, int gemm_dinvf, int gemm_schur);
+
+/* One CUDA graph replaying the assembly (hfem_assemble_async) of n contexts
+ * on the same device, each context on its own branch; launch it on any
+ * stream and call hfem_assemble_finish on each context afterwards.  The
+ * contexts must not be reallocated (new mesh, larger restart) while the
+ * graph is alive.  No counterpart in the reference. */
+typedef struct hfem_graph hfem_graph;
+int hfem_graph_capture(hfem_ctx** ctxs, int n, void* stream, hfem_graph** graph);
+int hfem_graph_launch(hfem_graph* graph, void* stream);
+int hfem_graph_destroy(hfem_graph* graph);
+
 /* Several independent problems in one context (a disjoint union of meshes, so
  * element work of many requests runs in one launch; no counterpart in the
  * reference, which runs one problem per process).  eprob (ne) and fprob (nf)
