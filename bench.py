@@ -400,21 +400,25 @@ def run_newton_task(args):
     u0, h0 = s.get_solution()
     for _ in range(args.warmup):
         s.set_solution(u0, h0, prob.sh)
-        s.solveNonlinearProblem(newton_tol=1e-10, maxiter=1)
+        s.solveNonlinearProblem(newton_tol=1e-10, maxiter=1, precond=args.precond)
     times, hist = [], None
     for _ in range(args.steps):
         s.set_solution(u0, h0, prob.sh)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=1)
+        conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=1, precond=args.precond)
         e1.record(st)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
-    _, gh = s.gmres(precond=2, restart=50, tol=1e-10)
+    s.set_timing(True)
+    _, gh = s.gmres(precond=args.precond, restart=50, tol=1e-10)
+    kt = s.kernel_times()
     s.close()
     ms = float(np.median(times))
-    line = {"metric": "Newton steps/s (2D NS p=2, 2048 elements, BJ-GMRES(50) tol 1e-10)", "value": 1e3 / ms,
+    pname = {2: "BJ", 0: "BILU0", -1: "unpreconditioned"}[args.precond]
+    line = {"metric": f"Newton steps/s (2D NS p=2, 2048 elements, {pname}-GMRES(50) tol 1e-10)", "value": 1e3 / ms,
+            "gmres_kernel_ms": {k: v[0] for k, v in kt.items()},
             "unit": "steps/s", "impl": "hfem", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
             "dtype": "f64", "rnorm_history": [float(v) for v in hist], "gmres_iterations": int(len(gh)),
             "higher_is_better": True}
@@ -425,7 +429,8 @@ def run_newton_task(args):
             write_inputs(prefix, prob, newton_maxiter=1, gmres_tol=1e-10)
             env = dict(os.environ, OPENBLAS_NUM_THREADS="1")
             t0 = time.time()
-            subprocess.run([REF_BIN, "newton", prefix, os.path.join(tmp, "out_"), "1", "2", "50", "1e-10"],
+            subprocess.run([REF_BIN, "newton", prefix, os.path.join(tmp, "out_"), "1", str(args.precond), "50",
+                            "1e-10", "1"],
                            check=True, capture_output=True, env=env)
             wall = time.time() - t0
             rh = np.fromfile(os.path.join(tmp, "out_rnorm_hist.bin"))
@@ -572,6 +577,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (TF32 Schur) leg")
     ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve", "batched"])
     ap.add_argument("--batched-meshes", type=int, default=64)
+    ap.add_argument("--precond", type=int, default=2, choices=[-1, 0, 2],
+                    help="GMRES preconditioner of the newton task: 2 block Jacobi, 0 BILU0 (MDF order), -1 none")
     ap.add_argument("--batched-seed", type=int, default=0)
     ap.add_argument("--tgv-n", type=int, default=16)
     ap.add_argument("--dirk-steps", type=int, default=20)

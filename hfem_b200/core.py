@@ -67,6 +67,8 @@ def load_library(path: str = LIB):
                                    C.c_double, C.c_int, _ip]
     lib.hfem_set_timing.argtypes = [C.c_void_p, C.c_int]
     lib.hfem_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.hfem_get_ordering.argtypes = [C.c_void_p, _ip]
+    lib.hfem_reset_ordering.argtypes = [C.c_void_p]
     lib.hfem_device_buffer.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]
     lib.hfem_kernel_times.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, _dp, _ip, C.c_int]
     _lib = lib
@@ -215,6 +217,12 @@ class HDGSolver:
         self._chk(self.lib.hfem_dirk_step(self.h, float(dt), stages, order, newton_tol, newton_maxiter, precond,
                                           restart, gmres_tol, gmres_maxit, C.byref(it)), "solveUnsteadyStep")
         return it.value
+
+    def ordering(self):
+        """ordered2unordered of the BILU0 ordering in use."""
+        o2u = np.zeros(self.prob.mesh.nf, dtype=np.int32)
+        self._chk(self.lib.hfem_get_ordering(self.h, _i(o2u)), "get_ordering")
+        return o2u
 
     def set_precision(self, mode):
         """0: FP64 throughout; 1: TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)."""

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <queue>
 #include <string>
 #include <vector>
 
@@ -22,6 +23,7 @@
 #include "schur_kernels.cuh"
 #include "elem_kernel_v2.cuh"
 #include "schur_tc.cuh"
+#include "bilu0.cuh"
 
 using namespace hfem;
 
@@ -220,6 +222,12 @@ struct hfem_ctx {
     unsigned char* seg_act = nullptr;
     int* seg_k = nullptr;
     int seg_restart = 0;
+    // BILU0: ordering (computed once, from the first system), level schedule, factors
+    bool have_order = false;
+    std::vector<int> h_o2u, h_u2o, lvl_lo, lvl_up;
+    int *d_u2o = nullptr, *d_rows_lo = nullptr, *d_rows_up = nullptr, *d_fptr = nullptr, *d_fpos = nullptr;
+    double *Mg = nullptr, *bl_t = nullptr, *bl_y = nullptr;
+    int prec_kind = 2;                  // preconditioner of the current GMRES: 2 BJ, 0 BILU0, -1 none
     KernelTimer timer;
 };
 
@@ -489,8 +497,225 @@ int dot(hfem_ctx* c, const double* a, const double* b, double* out, bool sq) {
     return check_launch(c, "dot");
 }
 
+// ---------------------------------------------------------------- BILU0
+// Same arithmetic as the LU of the oracle's restatement, so that the weights,
+// and with them the ordering, are reproduced bit for bit.
+int host_lu_factor(int n, double* a, int* piv) {
+    for (int j = 0; j < n; j++) {
+        int p = j;
+        double m = std::fabs(a[j + n * j]);
+        for (int i = j + 1; i < n; i++)
+            if (std::fabs(a[i + n * j]) > m) { m = std::fabs(a[i + n * j]); p = i; }
+        piv[j] = p;
+        if (a[p + n * j] == 0.0) return j + 1;
+        if (p != j) for (int k = 0; k < n; k++) std::swap(a[j + n * k], a[p + n * k]);
+        const double inv = 1.0 / a[j + n * j];
+        for (int i = j + 1; i < n; i++) a[i + n * j] *= inv;
+        for (int k = j + 1; k < n; k++) {
+            const double t = a[j + n * k];
+            if (t != 0.0) for (int i = j + 1; i < n; i++) a[i + n * k] -= a[i + n * j] * t;
+        }
+    }
+    return 0;
+}
+void host_lu_solve(int n, const double* lu, const int* piv, int nrhs, double* b) {
+    for (int r = 0; r < nrhs; r++) {
+        double* x = b + (size_t)n * r;
+        for (int i = 0; i < n; i++) if (piv[i] != i) std::swap(x[i], x[piv[i]]);
+        for (int i = 0; i < n; i++) { double t = x[i]; for (int k = 0; k < i; k++) t -= lu[i + n * k] * x[k]; x[i] = t; }
+        for (int i = n - 1; i >= 0; i--) {
+            double t = x[i];
+            for (int k = i + 1; k < n; k++) t -= lu[i + n * k] * x[k];
+            x[i] = t / lu[i + n * i];
+        }
+    }
+}
+
+int row_find(const std::vector<int>& rs, const std::vector<int>& ci, int r, int col) {
+    for (int k = rs[r]; k < rs[r + 1]; k++)
+        if (ci[k] == col) return k;
+    return -1;
+}
+
+// Minimum discarded fill ordering (kernel/computeMDFordering.m:1-150) of the
+// current Hg, with a lazy min-heap keyed (weight, row) in place of the
+// reference's linear search for the first minimum -- the same choice at every
+// step -- and the level schedule of the factorisation and of both solves.
+int compute_ordering(hfem_ctx* c) {
+    const int nf = c->dims.nf, b = c->bsz;
+    const size_t b2 = (size_t)b * b;
+    const std::vector<int>& rs = c->h_rowstart;
+    const std::vector<int>& ci = c->h_colidx;
+    const int nblk = rs[nf];
+    std::vector<double> Hg(b2 * nblk);
+    CK(cudaMemcpyAsync(Hg.data(), c->Hg, sizeof(double) * Hg.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<double> C(nblk), a(b2), t(b2);
+    std::vector<int> piv(b);
+    for (int i = 0; i < nf; i++) {
+        std::memcpy(a.data(), &Hg[b2 * rs[i]], sizeof(double) * b2);
+        if (host_lu_factor(b, a.data(), piv.data())) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d", i);
+        for (int n = rs[i]; n < rs[i + 1]; n++) {
+            std::memcpy(t.data(), &Hg[b2 * n], sizeof(double) * b2);
+            host_lu_solve(b, a.data(), piv.data(), b, t.data());
+            double s = 0.0;
+            for (size_t q = 0; q < b2; q++) s += t[q] * t[q];
+            C[n] = std::sqrt(s);
+        }
+    }
+    const double big = 1e100;
+    std::vector<double> w(nf);
+    std::vector<int> pos;
+    auto weight = [&](int k) {
+        double s = 0.0;
+        for (size_t ii = 0; ii < pos.size(); ii++) {
+            const int ri = ci[pos[ii]];
+            const double Cik = C[row_find(rs, ci, ri, k)];
+            for (size_t jj = 0; jj < pos.size(); jj++) {
+                if (jj == ii) continue;
+                if (row_find(rs, ci, ri, ci[pos[jj]]) < 0) {
+                    const double v = Cik * C[pos[jj]];
+                    s += v * v;
+                }
+            }
+        }
+        return std::sqrt(s);
+    };
+    using Item = std::pair<double, int>;
+    std::priority_queue<Item, std::vector<Item>, std::greater<Item>> heap;
+    for (int k = 0; k < nf; k++) {
+        pos.clear();
+        for (int q = rs[k] + 1; q < rs[k + 1]; q++) pos.push_back(q);
+        w[k] = weight(k);
+        heap.push({w[k], k});
+    }
+    c->h_o2u.assign(nf, 0);
+    c->h_u2o.assign(nf, 0);
+    for (int l = 0; l < nf; l++) {
+        int p = -1;
+        while (!heap.empty()) {
+            const Item it = heap.top();
+            heap.pop();
+            if (w[it.second] < big && it.first == w[it.second]) { p = it.second; break; }
+        }
+        if (p < 0) return fail(c, HFEM_E_STATE, "ordering heap exhausted");
+        c->h_o2u[l] = p;
+        w[p] = big;
+        for (int e = rs[p] + 1; e < rs[p + 1]; e++) {
+            const int k = ci[e];
+            if (!(w[k] < big)) continue;
+            pos.clear();
+            for (int q = rs[k] + 1; q < rs[k + 1]; q++)
+                if (w[ci[q]] < big) pos.push_back(q);
+            w[k] = weight(k);
+            heap.push({w[k], k});
+        }
+    }
+    for (int i = 0; i < nf; i++) c->h_u2o[c->h_o2u[i]] = i;
+    // level schedule: lower (and factorisation) over earlier neighbours, upper over later ones
+    const std::vector<int>& o2u = c->h_o2u;
+    const std::vector<int>& u2o = c->h_u2o;
+    std::vector<int> lev(nf, 0), levu(nf, 0);
+    int nl = 0, nu = 0;
+    for (int l = 0; l < nf; l++) {
+        const int i = o2u[l];
+        int m = 0;
+        for (int q = rs[i] + 1; q < rs[i + 1]; q++)
+            if (u2o[ci[q]] < l) m = std::max(m, lev[ci[q]] + 1);
+        lev[i] = m;
+        nl = std::max(nl, m + 1);
+    }
+    for (int l = nf - 1; l >= 0; l--) {
+        const int i = o2u[l];
+        int m = 0;
+        for (int q = rs[i] + 1; q < rs[i + 1]; q++)
+            if (u2o[ci[q]] > l) m = std::max(m, levu[ci[q]] + 1);
+        levu[i] = m;
+        nu = std::max(nu, m + 1);
+    }
+    auto group = [&](const std::vector<int>& L, int nlev, std::vector<int>& ptr) {
+        ptr.assign(nlev + 1, 0);
+        for (int i = 0; i < nf; i++) ptr[L[i] + 1]++;
+        for (int k = 0; k < nlev; k++) ptr[k + 1] += ptr[k];
+        std::vector<int> rows(nf), fill(ptr.begin(), ptr.end() - 1);
+        for (int l = 0; l < nf; l++) rows[fill[L[o2u[l]]]++] = o2u[l];
+        return rows;
+    };
+    const std::vector<int> rows_lo = group(lev, nl, c->lvl_lo);
+    const std::vector<int> rows_up = group(levu, nu, c->lvl_up);
+    // per row, the positions of its earlier neighbours in increasing order
+    std::vector<int> fptr(nf + 1, 0), fpos;
+    for (int i = 0; i < nf; i++) {
+        std::vector<std::pair<int, int>> e;
+        for (int q = rs[i] + 1; q < rs[i + 1]; q++)
+            if (u2o[ci[q]] < u2o[i]) e.push_back({u2o[ci[q]], q});
+        std::sort(e.begin(), e.end());
+        for (auto& x : e) fpos.push_back(x.second);
+        fptr[i + 1] = (int)fpos.size();
+    }
+    if (fpos.empty()) fpos.push_back(0);
+    int rc;
+    if ((rc = upload(c, &c->d_u2o, u2o.data(), (size_t)nf)) || (rc = upload(c, &c->d_rows_lo, rows_lo.data(), (size_t)nf)) ||
+        (rc = upload(c, &c->d_rows_up, rows_up.data(), (size_t)nf)) ||
+        (rc = upload(c, &c->d_fptr, fptr.data(), fptr.size())) || (rc = upload(c, &c->d_fpos, fpos.data(), fpos.size())))
+        return rc;
+    if (!c->Mg && (rc = dalloc(c, &c->Mg, b2 * nblk))) return rc;
+    if (!c->bl_t && (rc = dalloc(c, &c->bl_t, (size_t)nf * b))) return rc;
+    if (!c->bl_y && (rc = dalloc(c, &c->bl_y, (size_t)nf * b))) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_order = true;
+    return 0;
+}
+
+// Factor Hg into Mg level by level (computeBILU0.m).
+int bilu0_factor(hfem_ctx* c) {
+    Timed t(c, "bilu0_factor");
+    const int nf = c->dims.nf, b = c->bsz;
+    const size_t b2 = (size_t)b * b;
+    CK(cudaMemcpyAsync(c->Mg, c->Hg, sizeof(double) * b2 * c->dims.nblocks, cudaMemcpyDeviceToDevice, c->stream));
+    BiluArgs a{b, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, c->d_fptr, c->d_fpos, c->Mg, c->binfo};
+    const size_t smem = sizeof(double) * (2 * b2 + b) + sizeof(int) * b;
+    for (size_t l = 0; l + 1 < c->lvl_lo.size(); l++) {
+        a.rows = c->d_rows_lo + c->lvl_lo[l];
+        a.nrows = c->lvl_lo[l + 1] - c->lvl_lo[l];
+        bilu0_factor_kernel<<<std::min(a.nrows, sms(c->device) * 8), BILU_THREADS, smem, c->stream>>>(a);
+    }
+    int rc = check_launch(c, "bilu0_factor");
+    if (rc) return rc;
+    std::vector<int> bi(nf);
+    CK(cudaMemcpyAsync(bi.data(), c->binfo, sizeof(int) * nf, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < nf; i++)
+        if (bi[i]) return fail(c, HFEM_E_SINGULAR, "BILU0: singular pivot block at face %d", i);
+    return 0;
+}
+
+// v = (L U)^-1 x (applyBILU0.m); v may not alias x.
+int bilu0_apply(hfem_ctx* c, const double* x, double* v) {
+    Timed t(c, "bilu0_apply");
+    BiluSolveArgs a{c->bsz, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, c->Mg, x, c->bl_y, v};
+    for (size_t l = 0; l + 1 < c->lvl_lo.size(); l++) {
+        a.rows = c->d_rows_lo + c->lvl_lo[l];
+        a.nrows = c->lvl_lo[l + 1] - c->lvl_lo[l];
+        bilu0_lower_kernel<<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
+    }
+    for (size_t l = 0; l + 1 < c->lvl_up.size(); l++) {
+        a.rows = c->d_rows_up + c->lvl_up[l];
+        a.nrows = c->lvl_up[l + 1] - c->lvl_up[l];
+        bilu0_upper_kernel<<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
+    }
+    return check_launch(c, "bilu0_apply");
+}
+
 int matvec_prec(hfem_ctx* c, const double* x, double* z, bool prec) {
     Timed t(c, "matvec");
+    if (prec && c->prec_kind == 0) {
+        bsr_matvec_bj_kernel<<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
+            c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, nullptr, x, c->bl_t);
+        int rc = check_launch(c, "matvec");
+        if (rc) return rc;
+        return bilu0_apply(c, c->bl_t, z);
+    }
     bsr_matvec_bj_kernel<<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
         c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, prec ? c->Minv : nullptr, x, z);
     return check_launch(c, "matvec");
@@ -520,12 +745,18 @@ int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int
     int rc;
     if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before gmres");
     if (restart < 1 || maxit < 1 || !(tol > 0.0)) return fail(c, HFEM_E_ARG, "restart, maxit and tol must be positive");
-    if (precond != -1 && precond != 2) return fail(c, HFEM_E_ARG, "precond must be -1 (none) or 2 (block Jacobi)");
+    if (precond != -1 && precond != 0 && precond != 2)
+        return fail(c, HFEM_E_ARG, "precond must be -1 (none), 0 (BILU0) or 2 (block Jacobi)");
     if ((rc = ensure_krylov(c, restart))) return rc;
     const long long n = nvec(c);
     const int g = sms(c->device) * 4;
-    const bool prec = precond == 2;
-    if (prec) {
+    const bool prec = precond != -1;
+    c->prec_kind = precond;
+    if (precond == 0) {
+        if (!c->have_order && (rc = compute_ordering(c))) return rc;
+        if ((rc = bilu0_factor(c))) return rc;
+        if ((rc = bilu0_apply(c, c->Rg, c->pb))) return rc;
+    } else if (prec) {
         Timed t(c, "bj_inverse");
         const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
         bj_inverse_kernel<<<std::min(c->dims.nf, sms(c->device) * 8), 64, smem, c->stream>>>(
@@ -967,7 +1198,8 @@ int hfem_destroy(hfem_ctx* c) {
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
-                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err};
+                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err,
+                    c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& p : c->timer.pending) {
@@ -1067,6 +1299,7 @@ int hfem_set_mesh(hfem_ctx* c, const double* dgnodes, const int* elcon, const in
     CK(cudaStreamSynchronize(c->stream));
     c->h_rowstart.assign(rowstart, rowstart + nf + 1);
     c->h_colidx.assign(colidx, colidx + nblk);
+    c->have_order = false;
     c->have_mesh = true;
     return 0;
 }
@@ -1505,6 +1738,19 @@ int hfem_graph_destroy(hfem_graph* g) {
     for (auto e : g->ev)
         if (e) cudaEventDestroy(e);
     delete g;
+    return 0;
+}
+
+int hfem_get_ordering(hfem_ctx* c, int* ordered2unordered) {
+    if (!c || !ordered2unordered) return HFEM_E_ARG;
+    if (!c->have_order) return fail(c, HFEM_E_STATE, "no ordering yet (run hfem_gmres with precond 0)");
+    std::memcpy(ordered2unordered, c->h_o2u.data(), sizeof(int) * c->h_o2u.size());
+    return 0;
+}
+
+int hfem_reset_ordering(hfem_ctx* c) {
+    if (!c) return HFEM_E_ARG;
+    c->have_order = false;
     return 0;
 }
 

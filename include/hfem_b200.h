@@ -97,7 +97,11 @@ int hfem_assemble(hfem_ctx* ctx, double* rnorm);
 int hfem_residual(hfem_ctx* ctx, double* rnorm);
 
 /* Restarted GMRES on Hg x = Rg (x starts at 0), left preconditioning:
- * precond -1 none, 2 entity-wise block Jacobi (kernel/mkBlockJacobi.m).
+ * precond -1 none, 0 block ILU(0) in the minimum-discarded-fill order
+ * (kernel/computeMDFordering.m, computeBILU0.m, applyBILU0.m; the ordering is
+ * computed from the first system the context solves and kept, as the
+ * reference's reuseOrdering does), 2 entity-wise block Jacobi
+ * (kernel/mkBlockJacobi.m).
  * Replaces computeOrdering / computePreconditioner / gmres
  * (solvers/dgsolvers.cpp:16-20, closed in the reference; spec
  * kernel/gmres_bilu0.m).  conv: 1 converged, 0 max iterations, -1 breakdown.
@@ -131,6 +135,12 @@ int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newto
  * process and the Newton update stay FP64, so Newton iterations refine the
  * solution to the FP64 residual tolerance. */
 int hfem_set_precision(hfem_ctx* ctx, int mode);
+
+/* The BILU0 ordering in use: ordered2unordered[i] = face pivoted at step i
+ * (sys.ordered2unordered of the reference).  hfem_reset_ordering makes the
+ * next BILU0 solve recompute it from the current system. */
+int hfem_get_ordering(hfem_ctx* ctx, int* ordered2unordered);
+int hfem_reset_ordering(hfem_ctx* ctx);
 
 /* Device address and length (doubles) of one of the context's buffers, with
  * the ids of hfem_download, for zero-copy use on the device after the

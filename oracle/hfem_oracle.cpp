@@ -772,6 +772,10 @@ static void bj_apply(int nrows, int bsz, const double* Minv, const double* x, do
     }
 }
 
+// Preconditioner override used by oracle_gmres_bilu0 (single-threaded oracle).
+static void (*g_prec_fn)(const void*, const double*, double*) = nullptr;
+static const void* g_prec_ctx = nullptr;
+
 // Restarted GMRES, left block-Jacobi preconditioning, modified Gram-Schmidt,
 // Givens least squares; follows kernel/gmres_bilu0.m:17-105 with the BJ apply of
 // mkBlockJacobi.m (Minv == NULL: no preconditioner).  x holds the initial guess
@@ -783,7 +787,9 @@ int oracle_gmres(int nrows, int bsz, const int* rowstart, const int* colidx, con
     std::vector<double> V(N * (restart + 1)), w(N), t(N), pb(N);
     std::vector<double> h((size_t)(restart + 1) * restart), cs(restart), sn(restart), g(restart + 1), y(restart);
     auto prec = [&](const double* in, double* out) {
-        if (Minv) bj_apply(nrows, bsz, Minv, in, out); else std::memcpy(out, in, sizeof(double) * N);
+        if (g_prec_fn) g_prec_fn(g_prec_ctx, in, out);
+        else if (Minv) bj_apply(nrows, bsz, Minv, in, out);
+        else std::memcpy(out, in, sizeof(double) * N);
     };
     prec(b, pb.data());
     double nrmb = 0;
@@ -846,6 +852,195 @@ int oracle_gmres(int nrows, int bsz, const int* rowstart, const int* colidx, con
             for (size_t k = 0; k < N; k++) x[k] += V[N * i + k] * y[i];
     }
     if (iters) *iters = it;
+    return flag;
+}
+
+// ---------------------------------------------------------------- BILU0 + MDF
+// Position of column col in block row r (-1 if absent).
+static int find_in_row(const int* rowstart, const int* colidx, int r, int col) {
+    for (int k = rowstart[r]; k < rowstart[r + 1]; k++)
+        if (colidx[k] == col) return k;
+    return -1;
+}
+
+// Minimum discarded fill ordering (kernel/computeMDFordering.m:1-150):
+// C(n) = |Hg_ii^-1 Hg_n|_F for every block n of row i; the weight of row k is
+// the Frobenius norm of the fill C_ik C_kj that ILU(0) would discard for each
+// pair of distinct neighbours i, j of k that are not neighbours of each other
+// (after numbering starts, over unnumbered neighbours only); rows are numbered
+// greedily by minimum weight (first index on ties) and the weights of the
+// chosen row's unnumbered neighbours recomputed.
+int oracle_mdf_ordering(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                        int* o2u, int* u2o) {
+    const int nblk = rowstart[nrows];
+    std::vector<double> C(nblk), a((size_t)bsz * bsz), t((size_t)bsz * bsz);
+    std::vector<int> piv(bsz);
+    for (int i = 0; i < nrows; i++) {
+        std::memcpy(a.data(), Hg + (size_t)rowstart[i] * bsz * bsz, sizeof(double) * bsz * bsz);
+        if (lu_factor(bsz, a.data(), piv.data())) return 1 + i;
+        for (int n = rowstart[i]; n < rowstart[i + 1]; n++) {
+            std::memcpy(t.data(), Hg + (size_t)n * bsz * bsz, sizeof(double) * bsz * bsz);
+            lu_solve(bsz, a.data(), piv.data(), bsz, t.data());
+            double s = 0.0;
+            for (int q = 0; q < bsz * bsz; q++) s += t[q] * t[q];
+            C[n] = std::sqrt(s);
+        }
+    }
+    const double big = 1e100;
+    std::vector<double> w(nrows);
+    // weight of row k over the neighbour positions 'pos' (row-k positions, diagonal excluded)
+    auto weight = [&](int k, const std::vector<int>& pos) {
+        double s = 0.0;
+        for (size_t ii = 0; ii < pos.size(); ii++) {
+            const int ri = colidx[pos[ii]];
+            const int ik = find_in_row(rowstart, colidx, ri, k);
+            const double Cik = C[ik];
+            for (size_t jj = 0; jj < pos.size(); jj++) {
+                if (jj == ii) continue;
+                const int rj = colidx[pos[jj]];
+                if (find_in_row(rowstart, colidx, ri, rj) < 0) {
+                    const double v = Cik * C[pos[jj]];
+                    s += v * v;
+                }
+            }
+        }
+        return std::sqrt(s);
+    };
+    std::vector<int> pos;
+    for (int k = 0; k < nrows; k++) {
+        pos.clear();
+        for (int q = rowstart[k] + 1; q < rowstart[k + 1]; q++) pos.push_back(q);
+        w[k] = weight(k, pos);
+    }
+    for (int l = 0; l < nrows; l++) {
+        int p = 0;
+        for (int k = 1; k < nrows; k++) if (w[k] < w[p]) p = k;
+        o2u[l] = p;
+        w[p] = big;
+        for (int e = rowstart[p] + 1; e < rowstart[p + 1]; e++) {
+            const int k = colidx[e];
+            if (!(w[k] < big)) continue;
+            pos.clear();
+            for (int q = rowstart[k] + 1; q < rowstart[k + 1]; q++)
+                if (w[colidx[q]] < big) pos.push_back(q);
+            w[k] = weight(k, pos);
+        }
+    }
+    for (int i = 0; i < nrows; i++) u2o[o2u[i]] = i;
+    return 0;
+}
+
+static void blk_mul(int b, const double* A, const double* B, double* C) {   // C = A B
+    for (int c = 0; c < b; c++)
+        for (int r = 0; r < b; r++) {
+            double s = 0.0;
+            for (int k = 0; k < b; k++) s += A[r + b * k] * B[k + b * c];
+            C[r + b * c] = s;
+        }
+}
+static void blk_inv(int b, double* A) {
+    std::vector<double> a(A, A + (size_t)b * b), I((size_t)b * b, 0.0);
+    std::vector<int> piv(b);
+    lu_factor(b, a.data(), piv.data());
+    for (int i = 0; i < b; i++) I[i + b * i] = 1.0;
+    lu_solve(b, a.data(), piv.data(), b, I.data());
+    std::memcpy(A, I.data(), sizeof(double) * b * b);
+}
+
+// Block ILU(0) in the given order (kernel/computeBILU0.m:1-46): Mg holds L
+// (unit lower, off-diagonal blocks), U (upper blocks) and the inverted
+// diagonal blocks U_jj^-1 in Hg's block-CSR pattern.
+int oracle_bilu0_factor(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                        const int* o2u, const int* u2o, double* Mg) {
+    const size_t b2 = (size_t)bsz * bsz;
+    std::memcpy(Mg, Hg, sizeof(double) * b2 * rowstart[nrows]);
+    std::vector<double> tmp(b2);
+    for (int j = 0; j < nrows; j++) {
+        const int rj = o2u[j];
+        const int jj = rowstart[rj];
+        blk_inv(bsz, Mg + b2 * jj);
+        for (int i = rowstart[rj] + 1; i < rowstart[rj + 1]; i++) {
+            const int ri = colidx[i];
+            if (u2o[ri] <= j) continue;
+            const int ij = find_in_row(rowstart, colidx, ri, rj);
+            blk_mul(bsz, Mg + b2 * ij, Mg + b2 * jj, tmp.data());               // L_ij = U_ij U_jj^-1
+            std::memcpy(Mg + b2 * ij, tmp.data(), sizeof(double) * b2);
+            const int ii = rowstart[ri];
+            blk_mul(bsz, Mg + b2 * ij, Mg + b2 * i, tmp.data());                // U_ii -= L_ij U_ji
+            for (size_t q = 0; q < b2; q++) Mg[b2 * ii + q] -= tmp[q];
+            for (int l = rowstart[ri] + 1; l < rowstart[ri + 1]; l++) {
+                const int rl = colidx[l];
+                if (u2o[rl] <= j) continue;
+                const int jm = find_in_row(rowstart, colidx, rj, rl);
+                if (jm < 0 || jm == jj) continue;
+                blk_mul(bsz, Mg + b2 * ij, Mg + b2 * jm, tmp.data());           // U_il -= L_ij U_jm
+                for (size_t q = 0; q < b2; q++) Mg[b2 * l + q] -= tmp[q];
+            }
+        }
+    }
+    return 0;
+}
+
+// v = (L U)^-1 x (kernel/applyBILU0.m:1-48).
+void oracle_bilu0_apply(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Mg,
+                        const int* o2u, const int* u2o, const double* x, double* v) {
+    const size_t b2 = (size_t)bsz * bsz, N = (size_t)nrows * bsz;
+    std::vector<double> y(x, x + N), t(bsz);
+    for (int j = 0; j < nrows; j++) {
+        const int rj = o2u[j];
+        double* yj = &y[(size_t)rj * bsz];
+        for (int i = rowstart[rj] + 1; i < rowstart[rj + 1]; i++) {
+            const int ri = colidx[i];
+            if (u2o[ri] >= j) continue;
+            const double* L = Mg + b2 * i;
+            const double* yi = &y[(size_t)ri * bsz];
+            for (int r = 0; r < bsz; r++) {
+                double s = 0.0;
+                for (int c = 0; c < bsz; c++) s += L[r + bsz * c] * yi[c];
+                yj[r] -= s;
+            }
+        }
+    }
+    std::memcpy(v, y.data(), sizeof(double) * N);
+    for (int jj = nrows - 1; jj >= 0; jj--) {
+        const int rj = o2u[jj];
+        double* vj = v + (size_t)rj * bsz;
+        for (int i = rowstart[rj] + 1; i < rowstart[rj + 1]; i++) {
+            const int ri = colidx[i];
+            if (u2o[ri] <= u2o[rj]) continue;
+            const double* U = Mg + b2 * i;
+            const double* vi = v + (size_t)ri * bsz;
+            for (int r = 0; r < bsz; r++) {
+                double s = 0.0;
+                for (int c = 0; c < bsz; c++) s += U[r + bsz * c] * vi[c];
+                vj[r] -= s;
+            }
+        }
+        const double* Dinv = Mg + b2 * rowstart[rj];
+        for (int r = 0; r < bsz; r++) {
+            double s = 0.0;
+            for (int c = 0; c < bsz; c++) s += Dinv[r + bsz * c] * vj[c];
+            t[r] = s;
+        }
+        for (int r = 0; r < bsz; r++) vj[r] = t[r];
+    }
+}
+
+// GMRES of oracle_gmres with the BILU0 preconditioner.
+int oracle_gmres_bilu0(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                       const double* Mg, const int* o2u, const int* u2o, const double* b, double* x, int restart,
+                       double tol, int maxit, int* iters, double* hist, int hist_len) {
+    struct Ctx { int nrows, bsz; const int *rs, *ci; const double* Mg; const int *o2u, *u2o; } cx{
+        nrows, bsz, rowstart, colidx, Mg, o2u, u2o};
+    g_prec_ctx = &cx;
+    g_prec_fn = [](const void* p, const double* in, double* out) {
+        const Ctx* q = static_cast<const Ctx*>(p);
+        oracle_bilu0_apply(q->nrows, q->bsz, q->rs, q->ci, q->Mg, q->o2u, q->u2o, in, out);
+    };
+    const int flag = oracle_gmres(nrows, bsz, rowstart, colidx, Hg, nullptr, b, x, restart, tol, maxit, iters, hist,
+                                  hist_len);
+    g_prec_fn = nullptr;
+    g_prec_ctx = nullptr;
     return flag;
 }
 

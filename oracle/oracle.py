@@ -45,7 +45,8 @@ def lib():
             build()
         _lib = C.CDLL(LIB_PATH)
         for name in ("oracle_element", "oracle_getq", "oracle_assemble", "oracle_residual",
-                     "oracle_update", "oracle_bj_inverse", "oracle_gmres"):
+                     "oracle_update", "oracle_bj_inverse", "oracle_gmres", "oracle_mdf_ordering",
+                     "oracle_bilu0_factor", "oracle_gmres_bilu0"):
             getattr(_lib, name).restype = C.c_int
     return _lib
 
@@ -168,6 +169,38 @@ class Oracle:
         flag = lib().oracle_gmres(me.nf, self.bsz, _i(self._keep["rowstart"]), _i(self._keep["colidx"]), _d(Hg),
                                   _d(Minv) if Minv is not None else _dp(), _d(np.ascontiguousarray(b)), _d(x),
                                   restart, C.c_double(tol), maxit, C.byref(it), _d(hist), maxit + 1)
+        return x, flag, hist[:it.value]
+
+    # -- BILU0 with the MDF ordering (computeMDFordering.m, computeBILU0.m, applyBILU0.m)
+    def _rc(self):
+        return _i(self._keep["rowstart"]), _i(self._keep["colidx"])
+
+    def mdf_ordering(self, Hg):
+        nf = self.prob.mesh.nf
+        o2u = np.zeros(nf, dtype=np.int32)
+        u2o = np.zeros(nf, dtype=np.int32)
+        if lib().oracle_mdf_ordering(nf, self.bsz, *self._rc(), _d(Hg), _i(o2u), _i(u2o)):
+            raise RuntimeError("singular diagonal block")
+        return o2u, u2o
+
+    def bilu0_factor(self, Hg, o2u, u2o):
+        Mg = np.zeros_like(Hg)
+        lib().oracle_bilu0_factor(self.prob.mesh.nf, self.bsz, *self._rc(), _d(Hg), _i(o2u), _i(u2o), _d(Mg))
+        return Mg
+
+    def bilu0_apply(self, Mg, o2u, u2o, x):
+        v = np.zeros_like(x)
+        lib().oracle_bilu0_apply(self.prob.mesh.nf, self.bsz, *self._rc(), _d(Mg), _i(o2u), _i(u2o),
+                                 _d(np.ascontiguousarray(x)), _d(v))
+        return v
+
+    def gmres_bilu0(self, Hg, Mg, o2u, u2o, b, restart=50, tol=1e-10, maxit=1000):
+        x = np.zeros_like(b)
+        it = C.c_int(0)
+        hist = np.zeros(maxit + 1)
+        flag = lib().oracle_gmres_bilu0(self.prob.mesh.nf, self.bsz, *self._rc(), _d(Hg), _d(Mg), _i(o2u), _i(u2o),
+                                        _d(np.ascontiguousarray(b)), _d(x), restart, C.c_double(tol), maxit,
+                                        C.byref(it), _d(hist), maxit + 1)
         return x, flag, hist[:it.value]
 
 

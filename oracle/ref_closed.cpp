@@ -6,8 +6,10 @@
 // linked.  The algorithms follow the readable MATLAB specifications:
 //   dmdserial             face-to-face block CSR with the diagonal block first
 //                         (kernel/computeBILU0.m:15-17, kernel/mkBlockJacobi.m:10)
-//   computeOrdering       identity ordering (reorderMethod = 0)
-//   computePreconditioner block Jacobi: inverse of each row's diagonal block
+//   computeOrdering       identity (reorderMethod 0), else minimum discarded
+//                         fill (kernel/computeMDFordering.m:1-150) for BILU0
+//   computePreconditioner 0: block ILU(0) in that order (kernel/computeBILU0.m);
+//                         2: block Jacobi, inverse of each row's diagonal block
 //                         (kernel/mkBlockJacobi.m:1-16); -1 = none
 //   gmres                 restarted GMRES with left preconditioning and MGS
 //                         (kernel/gmres_bilu0.m:17-105), via oracle_gmres
@@ -23,6 +25,13 @@ int oracle_bj_inverse(int nrows, int bsz, const int* rowstart, const double* Hg,
 int oracle_gmres(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
                  const double* Minv, const double* b, double* x, int restart, double tol, int maxit,
                  int* iters, double* hist, int hist_len);
+int oracle_mdf_ordering(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                        int* o2u, int* u2o);
+int oracle_bilu0_factor(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                        const int* o2u, const int* u2o, double* Mg);
+int oracle_gmres_bilu0(int nrows, int bsz, const int* rowstart, const int* colidx, const double* Hg,
+                       const double* Mg, const int* o2u, const int* u2o, const double* b, double* x, int restart,
+                       double tol, int maxit, int* iters, double* hist, int hist_len);
 }
 
 // GMRES residual histories and the assembly residual seen by each linear solve.
@@ -61,6 +70,12 @@ void dmdserial(sysstruct& sys, meshstruct& mesh, appstruct& app)
 
 void computeOrdering(sysstruct& sys, Int preconditioner)
 {
+    if (preconditioner == 0 && sys.reorderMethod != 0) {
+        if (oracle_mdf_ordering(sys.numEntities, sys.blkSize, &sys.ent2entStart[0], &sys.ent2ent[0], &sys.Hg[0],
+                                &sys.ordered2unordered[0], &sys.unordered2ordered[0]) != 0)
+            error("singular diagonal block in the MDF ordering");
+        return;
+    }
     for (Int i = 0; i < sys.numEntities; i++) {
         sys.ordered2unordered[i] = i;
         sys.unordered2ordered[i] = i;
@@ -70,7 +85,12 @@ void computeOrdering(sysstruct& sys, Int preconditioner)
 void computePreconditioner(sysstruct& sys, Int preconditioner)
 {
     if (preconditioner == -1) return;
-    if (preconditioner != 2) error("only block Jacobi (2) and none (-1) are restated");
+    if (preconditioner == 0) {
+        oracle_bilu0_factor(sys.numEntities, sys.blkSize, &sys.ent2entStart[0], &sys.ent2ent[0], &sys.Hg[0],
+                            &sys.ordered2unordered[0], &sys.unordered2ordered[0], &sys.Mg[0]);
+        return;
+    }
+    if (preconditioner != 2) error("only BILU0 (0), block Jacobi (2) and none (-1) are restated");
     const Int bsz = sys.blkSize;
     if (oracle_bj_inverse(sys.numEntities, bsz, &sys.ent2entStart[0], &sys.Hg[0], &sys.Mg[0]) != 0)
         error("singular diagonal block in block Jacobi");
@@ -84,7 +104,14 @@ void gmres(sysstruct& sys, Int* convFlag)
     std::vector<double> hist(sys.maxiter + 1, 0.0);
     int iters = 0;
     const double* Minv = (sys.preconditioner == 2) ? &sys.Mg[0] : nullptr;
-    int flag = oracle_gmres(sys.numEntities, sys.blkSize, &sys.ent2entStart[0], &sys.ent2ent[0], &sys.Hg[0],
+    int flag;
+    if (sys.preconditioner == 0)
+        flag = oracle_gmres_bilu0(sys.numEntities, sys.blkSize, &sys.ent2entStart[0], &sys.ent2ent[0], &sys.Hg[0],
+                                  &sys.Mg[0], &sys.ordered2unordered[0], &sys.unordered2ordered[0], &sys.Rg[0],
+                                  &sys.x[0], sys.restart, sys.tol, sys.maxiter, &iters, hist.data(),
+                                  (int)hist.size());
+    else
+        flag = oracle_gmres(sys.numEntities, sys.blkSize, &sys.ent2entStart[0], &sys.ent2ent[0], &sys.Hg[0],
                             Minv, &sys.Rg[0], &sys.x[0], sys.restart, sys.tol, sys.maxiter, &iters,
                             hist.data(), (int)hist.size());
     g_gmres_iters.push_back(iters);

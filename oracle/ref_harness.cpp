@@ -145,6 +145,7 @@ int main(int argc, char** argv)
         c.sys.preconditioner = atoi(argv[5]);
         c.sys.restart = atoi(argv[6]);
         c.sys.tol = atof(argv[7]);
+        if (argc > 8) c.sys.reorderMethod = atoi(argv[8]);
         g_sol = &c.sol;
         Int conv[1] = {0};
         solveNonlinearProblem(c.sys, &c.elem, c.mesh, m, c.sol, c.app, &c.temp, &c.ndims[0], conv);
