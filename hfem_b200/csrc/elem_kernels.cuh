@@ -743,6 +743,60 @@ __global__ void scatter_H_kernel(ScatterArgs A) {
     }
 }
 
+// The same owner-gather with one warp per Hg block and the face shape known
+// at compile time: the warp first resolves, for each (at most two)
+// contributing element, the offsets of the block's rows and columns inside
+// that element's H (elcon gives the permutation of the face nodes), then
+// streams the block's entries in Hg order (rows fastest, coalesced stores).
+template <int NPF, int NCH, int NFE>
+__global__ void __launch_bounds__(256) scatter_H_block_kernel(ScatterArgs A) {
+    constexpr int BSZ = NPF * NCH, NDF = NPF * NFE, NB = NDF * NCH;
+    constexpr int WARPS = 8;
+    __shared__ long long s_col[WARPS][2][NPF];
+    __shared__ int s_row[WARPS][2][NPF];
+    __shared__ long long s_base[WARPS][2];
+    __shared__ int s_n[WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = blockIdx.x * WARPS + w; k < A.nblk; k += gridDim.x * WARPS) {
+        const int i = A.rowface[k], j = A.colface[k];
+        if (lane == 0) {
+            int n = 0;
+            for (int c = 0; c < 2; c++) {
+                const int e = A.blk_src[(k * 2 + c) * 3 + 0];
+                if (e < 0) break;
+                s_base[w][c] = (long long)e * NB * NB;
+                n++;
+            }
+            s_n[w] = n;
+        }
+        for (int t = lane; t < 2 * 2 * NPF; t += 32) {
+            const int c = t / (2 * NPF), r = t % (2 * NPF), m = r % NPF, isc = r / NPF;
+            const int e = A.blk_src[(k * 2 + c) * 3 + 0];
+            if (e < 0) continue;
+            const int a = A.blk_src[(k * 2 + c) * 3 + 1], b = A.blk_src[(k * 2 + c) * 3 + 2];
+            if (!isc) {
+                const int ind = A.elcon[(size_t)e * NDF + a * NPF + m] - i * NPF;
+                s_row[w][c][m] = a * BSZ + ind * NCH;
+            } else {
+                const int jnd = A.elcon[(size_t)e * NDF + b * NPF + m] - j * NPF;
+                s_col[w][c][m] = (long long)NB * (b * BSZ + jnd * NCH);
+            }
+        }
+        __syncwarp();
+        const int n = s_n[w];
+        double* out = A.Hg + (size_t)k * BSZ * BSZ;
+        for (int t = lane; t < BSZ * BSZ; t += 32) {
+            const int colpos = t / BSZ, rowpos = t - colpos * BSZ;
+            const int m1 = colpos / NCH, n1 = colpos - m1 * NCH, m2 = rowpos / NCH, n2 = rowpos - m2 * NCH;
+            double s = 0.0;
+            for (int c = 0; c < n; c++)
+                s += A.H[s_base[w][c] + s_row[w][c][m2] + n2 + s_col[w][c][m1] + (long long)NB * n1];
+            out[t] = s;
+        }
+        __syncwarp();
+    }
+}
+
 __global__ void scatter_R_kernel(ScatterArgs A) {
     const int bsz = A.npf * A.nch, ndf = A.npf * A.nfe;
     const int total = A.nf * bsz;
@@ -760,6 +814,33 @@ __global__ void scatter_R_kernel(ScatterArgs A) {
         }
         if (A.Rg) A.Rg[t] = s;
         if (A.Rr) A.Rr[t] = so;
+    }
+}
+
+// Partial sums of ru2 and Rr^2 per CTA (fixed grid-stride order).
+__global__ void rnorm_partial_kernel(int ne, const double* __restrict__ ru2, long long nr,
+                                     const double* __restrict__ rr, double* __restrict__ part) {
+    __shared__ double red[32];
+    double s = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ne; i += stride) s += ru2[i];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nr; i += stride) s += rr[i] * rr[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// out = sqrt(sum of the n partial sums), in order.
+__global__ void rnorm_final_kernel(int n, const double* __restrict__ part, double* out) {
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < n; i++) t += part[i];
+        *out = sqrt(t);
     }
 }
 

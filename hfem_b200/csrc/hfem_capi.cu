@@ -29,6 +29,8 @@ using namespace hfem;
 
 namespace {
 
+constexpr int RNORM_CTAS = 296;
+
 struct KernelTimer {
     bool on = false;
     std::map<std::string, std::pair<double, int>> acc;
@@ -113,6 +115,7 @@ struct Launch {
     void (*schur_tc)(dim3, size_t, cudaStream_t, const SchurTcArgs&);
     size_t tc_smem;
     const void* tc_fn;
+    void (*scatter_h)(dim3, cudaStream_t, const ScatterArgs&);
 };
 
 template <int N>
@@ -128,6 +131,10 @@ template <class S>
 void launch_schur(dim3 g, size_t sm, cudaStream_t st, const SchurArgs& a) { schur_kernel<S::N, S::NB><<<g, NT, sm, st>>>(a); }
 template <class S>
 void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
+template <class S>
+void launch_scatter_h(dim3 g, cudaStream_t st, const ScatterArgs& a) {
+    scatter_H_block_kernel<S::NPF, S::NCH, S::NFE><<<g, 256, 0, st>>>(a);
+}
 template <class S>
 void launch_schur_tc(dim3 g, size_t sm, cudaStream_t st, const SchurTcArgs& a) {
     schur_tc_kernel<S::N, S::NB><<<g, TC_THREADS, sm, st>>>(a);
@@ -159,6 +166,7 @@ Launch make_launch() {
     L.schur_tc = launch_schur_tc<S>;
     L.tc_smem = TcCfg<S::N, S::NB>::SMEM;
     L.tc_fn = (const void*)schur_tc_kernel<S::N, S::NB>;
+    L.scatter_h = launch_scatter_h<S>;
     return L;
 }
 
@@ -185,6 +193,7 @@ struct hfem_ctx {
     int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
     int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
     int* tc_err = nullptr;
+    double* rn_part = nullptr;
     // master tables
     double *shapvt = nullptr, *shapvg = nullptr, *svsv = nullptr, *shapft = nullptr, *shapfg = nullptr, *sfsf = nullptr;
     int* perm = nullptr;
@@ -330,6 +339,7 @@ int ensure_assembly_buffers(hfem_ctx* c) {
     if ((rc = dalloc(c, &c->info, ne))) return rc;
     if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws2))) return rc;
     if ((rc = dalloc(c, &c->tc_err, 1))) return rc;
+    if ((rc = dalloc(c, &c->rn_part, RNORM_CTAS))) return rc;
     CK(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
     return 0;
 }
@@ -420,7 +430,7 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
         }
         {
             Timed t(c, "scatter_H");
-            scatter_H_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(sa);
+            c->L->scatter_h(dim3(std::max(1, std::min((c->dims.nblocks + 7) / 8, sms(c->device) * 8))), c->stream, sa);
             if ((rc = check_launch(c, "scatter_H"))) return rc;
         }
     } else {
@@ -431,7 +441,9 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
         scatter_R_kernel<<<sms(c->device) * 4, 256, 0, c->stream>>>(sa);
         if ((rc = check_launch(c, "scatter_R"))) return rc;
     }
-    rnorm_kernel<<<1, 1024, 0, c->stream>>>(c->dims.ne, c->ru2, c->dims.nf * c->bsz, c->Rr, c->rnorm);
+    rnorm_partial_kernel<<<RNORM_CTAS, 256, 0, c->stream>>>(c->dims.ne, c->ru2, (long long)c->dims.nf * c->bsz,
+                                                            c->Rr, c->rn_part);
+    rnorm_final_kernel<<<1, 32, 0, c->stream>>>(RNORM_CTAS, c->rn_part, c->rnorm);
     return check_launch(c, "rnorm");
 }
 
@@ -1198,7 +1210,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
-                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err,
+                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y};
     for (void* p : ptrs)
         if (p) cudaFree(p);
