@@ -207,4 +207,64 @@ __global__ void __launch_bounds__(64) bilu0_upper_kernel(BiluSolveArgs A) {
     }
 }
 
+// Both triangular solves in one CTA of 1024 threads, level after level with a
+// CTA barrier in between: for orderings whose levels hold few rows (MDF gives
+// long dependency chains) this replaces two launches per level by one launch.
+// Each warp takes one row of the level at a time; lanes own the row's entries.
+__global__ void __launch_bounds__(1024) bilu0_apply_cta_kernel(BiluSolveArgs A, const int* __restrict__ lvl_lo,
+                                                               int nlo, const int* __restrict__ rows_lo,
+                                                               const int* __restrict__ lvl_up, int nup,
+                                                               const int* __restrict__ rows_up) {
+    __shared__ double t[32][64];
+    const int b = A.bsz;
+    const size_t b2 = (size_t)b * b;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int l = 0; l < nlo; l++) {
+        for (int q = lvl_lo[l] + w; q < lvl_lo[l + 1]; q += nw) {
+            const int i = rows_lo[q], oi = A.u2o[i];
+            for (int r = lane; r < b; r += 32) {
+                double s = A.x[(size_t)i * b + r];
+                for (int p = A.rowstart[i] + 1; p < A.rowstart[i + 1]; p++) {
+                    const int k = A.colidx[p];
+                    if (A.u2o[k] >= oi) continue;
+                    const double* L = A.Mg + (size_t)p * b2;
+                    const double* yk = A.y + (size_t)k * b;
+                    double d = 0.0;
+                    for (int c = 0; c < b; c++) d += L[r + b * c] * yk[c];
+                    s -= d;
+                }
+                A.y[(size_t)i * b + r] = s;
+            }
+        }
+        __syncthreads();
+    }
+    for (int l = 0; l < nup; l++) {
+        for (int q = lvl_up[l] + w; q < lvl_up[l + 1]; q += nw) {
+            const int i = rows_up[q], oi = A.u2o[i];
+            for (int r = lane; r < b; r += 32) {
+                double s = A.y[(size_t)i * b + r];
+                for (int p = A.rowstart[i] + 1; p < A.rowstart[i + 1]; p++) {
+                    const int k = A.colidx[p];
+                    if (A.u2o[k] <= oi) continue;
+                    const double* U = A.Mg + (size_t)p * b2;
+                    const double* vk = A.v + (size_t)k * b;
+                    double d = 0.0;
+                    for (int c = 0; c < b; c++) d += U[r + b * c] * vk[c];
+                    s -= d;
+                }
+                t[w][r] = s;
+            }
+            __syncwarp();
+            const double* Dinv = A.Mg + (size_t)A.rowstart[i] * b2;
+            for (int r = lane; r < b; r += 32) {
+                double s = 0.0;
+                for (int c = 0; c < b; c++) s += Dinv[r + b * c] * t[w][c];
+                A.v[(size_t)i * b + r] = s;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace hfem

@@ -235,6 +235,8 @@ struct hfem_ctx {
     bool have_order = false;
     std::vector<int> h_o2u, h_u2o, lvl_lo, lvl_up;
     int *d_u2o = nullptr, *d_rows_lo = nullptr, *d_rows_up = nullptr, *d_fptr = nullptr, *d_fpos = nullptr;
+    int *d_lvl_lo = nullptr, *d_lvl_up = nullptr;
+    cudaGraphExec_t bilu_exec = nullptr;    // the factorisation's per-level launches, replayed as one graph
     double *Mg = nullptr, *bl_t = nullptr, *bl_y = nullptr;
     int prec_kind = 2;                  // preconditioner of the current GMRES: 2 BJ, 0 BILU0, -1 none
     KernelTimer timer;
@@ -669,29 +671,57 @@ int compute_ordering(hfem_ctx* c) {
     int rc;
     if ((rc = upload(c, &c->d_u2o, u2o.data(), (size_t)nf)) || (rc = upload(c, &c->d_rows_lo, rows_lo.data(), (size_t)nf)) ||
         (rc = upload(c, &c->d_rows_up, rows_up.data(), (size_t)nf)) ||
-        (rc = upload(c, &c->d_fptr, fptr.data(), fptr.size())) || (rc = upload(c, &c->d_fpos, fpos.data(), fpos.size())))
+        (rc = upload(c, &c->d_fptr, fptr.data(), fptr.size())) || (rc = upload(c, &c->d_fpos, fpos.data(), fpos.size())) ||
+        (rc = upload(c, &c->d_lvl_lo, c->lvl_lo.data(), c->lvl_lo.size())) ||
+        (rc = upload(c, &c->d_lvl_up, c->lvl_up.data(), c->lvl_up.size())))
         return rc;
     if (!c->Mg && (rc = dalloc(c, &c->Mg, b2 * nblk))) return rc;
     if (!c->bl_t && (rc = dalloc(c, &c->bl_t, (size_t)nf * b))) return rc;
     if (!c->bl_y && (rc = dalloc(c, &c->bl_y, (size_t)nf * b))) return rc;
     CK(cudaStreamSynchronize(c->stream));
+    if (c->bilu_exec) {
+        cudaGraphExecDestroy(c->bilu_exec);
+        c->bilu_exec = nullptr;
+    }
     c->have_order = true;
     return 0;
 }
 
-// Factor Hg into Mg level by level (computeBILU0.m).
-int bilu0_factor(hfem_ctx* c) {
-    Timed t(c, "bilu0_factor");
-    const int nf = c->dims.nf, b = c->bsz;
+void enqueue_bilu0_levels(hfem_ctx* c, cudaStream_t st) {
+    const int b = c->bsz;
     const size_t b2 = (size_t)b * b;
-    CK(cudaMemcpyAsync(c->Mg, c->Hg, sizeof(double) * b2 * c->dims.nblocks, cudaMemcpyDeviceToDevice, c->stream));
     BiluArgs a{b, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, c->d_fptr, c->d_fpos, c->Mg, c->binfo};
     const size_t smem = sizeof(double) * (2 * b2 + b) + sizeof(int) * b;
     for (size_t l = 0; l + 1 < c->lvl_lo.size(); l++) {
         a.rows = c->d_rows_lo + c->lvl_lo[l];
         a.nrows = c->lvl_lo[l + 1] - c->lvl_lo[l];
-        bilu0_factor_kernel<<<std::min(a.nrows, sms(c->device) * 8), BILU_THREADS, smem, c->stream>>>(a);
+        bilu0_factor_kernel<<<std::min(a.nrows, sms(c->device) * 8), BILU_THREADS, smem, st>>>(a);
     }
+}
+
+// Factor Hg into Mg level by level (computeBILU0.m).  The level launches are
+// captured once per ordering (on a private stream) and replayed as a graph.
+int bilu0_factor(hfem_ctx* c) {
+    Timed t(c, "bilu0_factor");
+    const int nf = c->dims.nf, b = c->bsz;
+    const size_t b2 = (size_t)b * b;
+    CK(cudaMemcpyAsync(c->Mg, c->Hg, sizeof(double) * b2 * c->dims.nblocks, cudaMemcpyDeviceToDevice, c->stream));
+    if (!c->bilu_exec) {
+        cudaStream_t cap = nullptr;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            enqueue_bilu0_levels(c, cap);
+            if (cudaStreamEndCapture(cap, &g) == cudaSuccess && g) {
+                if (cudaGraphInstantiate(&c->bilu_exec, g, 0) != cudaSuccess) c->bilu_exec = nullptr;
+                cudaGraphDestroy(g);
+            }
+        }
+        if (cap) cudaStreamDestroy(cap);
+        cudaGetLastError();
+    }
+    if (c->bilu_exec) CK(cudaGraphLaunch(c->bilu_exec, c->stream));
+    else enqueue_bilu0_levels(c, c->stream);
     int rc = check_launch(c, "bilu0_factor");
     if (rc) return rc;
     std::vector<int> bi(nf);
@@ -706,6 +736,13 @@ int bilu0_factor(hfem_ctx* c) {
 int bilu0_apply(hfem_ctx* c, const double* x, double* v) {
     Timed t(c, "bilu0_apply");
     BiluSolveArgs a{c->bsz, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, c->Mg, x, c->bl_y, v};
+    const int nlo = (int)c->lvl_lo.size() - 1, nup = (int)c->lvl_up.size() - 1;
+    // few rows per level: one CTA walks all levels (no launch per level)
+    if ((long long)c->dims.nf < 64LL * std::max(nlo, nup)) {
+        bilu0_apply_cta_kernel<<<1, 1024, 0, c->stream>>>(a, c->d_lvl_lo, nlo, c->d_rows_lo, c->d_lvl_up, nup,
+                                                          c->d_rows_up);
+        return check_launch(c, "bilu0_apply");
+    }
     for (size_t l = 0; l + 1 < c->lvl_lo.size(); l++) {
         a.rows = c->d_rows_lo + c->lvl_lo[l];
         a.nrows = c->lvl_lo[l + 1] - c->lvl_lo[l];
@@ -1211,13 +1248,15 @@ int hfem_destroy(hfem_ctx* c) {
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
                     c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part,
-                    c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y};
+                    c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
+                    c->d_lvl_lo, c->d_lvl_up};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& p : c->timer.pending) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
     }
+    if (c->bilu_exec) cudaGraphExecDestroy(c->bilu_exec);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return 0;
