@@ -1,4 +1,4 @@
-"""Periodic simplex meshes with HDG trace numbering.
+"""Simplex meshes of a box with HDG trace numbering, periodic or bounded.
 
 Builds what the reference's front end builds for a periodic HDG mesh
 (``preprocessing/digasopre.m:39-88``): ``t2f`` (``mkt2fmatlab.m``), the HDG
@@ -14,6 +14,12 @@ Periodicity is handled topologically: vertex ids wrap modulo the grid size,
 so faces on opposite sides of the box are the same face; coordinates in
 ``dgnodes`` stay unwrapped.  Grids need ``n >= 3`` cells per direction so
 that distinct faces never share their wrapped vertex set.
+
+Bounded meshes (``periodic=False``) keep the boundary faces with one element;
+``bf`` of such an element face is ``-(ib + 1)`` with the side index
+``ib = 2 * axis + end`` (``end`` 0 at coordinate 0, 1 at ``length``), the
+reference's convention for ``mesh.bf`` (``elementassembly.cpp:1078-1103``:
+``ib = -bf - 1``, boundary condition ``app.bcm[ib]``).
 
 All arrays are 0-based and element-major (numpy C order), which is the
 reference's column-major layout: ``dgnodes[e, d, n]`` is
@@ -54,20 +60,22 @@ class Mesh:
         return self.nf * self.npf
 
 
-def _square_tris(n: int, length: float):
+def _square_tris(n: int, length: float, periodic: bool = True):
     h = length / n
+    m = n if periodic else n + 1
     verts, wrapped = [], []
     for j in range(n):
         for i in range(n):
             v00, v10, v11, v01 = (i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1)
             for tri in ((v00, v10, v11), (v00, v11, v01)):
                 verts.append([[h * a, h * b] for a, b in tri])
-                wrapped.append([(a % n) + n * (b % n) for a, b in tri])
-    return np.array(verts), np.array(wrapped, dtype=np.int64), n * n
+                wrapped.append([(a % m) + m * (b % m) for a, b in tri])
+    return np.array(verts), np.array(wrapped, dtype=np.int64), m * m
 
 
-def _cube_tets(n: int, length: float):
+def _cube_tets(n: int, length: float, periodic: bool = True):
     h = length / n
+    m = n if periodic else n + 1
     base = []
     for perm in itertools.permutations(range(3)):
         p = [np.zeros(3, dtype=np.int64)]
@@ -88,8 +96,8 @@ def _cube_tets(n: int, length: float):
                 for tet in base:
                     pts = [off + q for q in tet]
                     verts.append([[h * c for c in q] for q in pts])
-                    wrapped.append([(q[0] % n) + n * ((q[1] % n) + n * (q[2] % n)) for q in pts])
-    return np.array(verts), np.array(wrapped, dtype=np.int64), n ** 3
+                    wrapped.append([(q[0] % m) + m * ((q[1] % m) + m * (q[2] % m)) for q in pts])
+    return np.array(verts), np.array(wrapped, dtype=np.int64), m ** 3
 
 
 def _face_node_bary(master: Master):
@@ -99,14 +107,16 @@ def _face_node_bary(master: Master):
     return lam                                   # (npf, nvf)
 
 
-def build_mesh(master: Master, n: int, length: float) -> Mesh:
+def build_mesh(master: Master, n: int, length: float, periodic: bool = True) -> Mesh:
     nd = master.nd
-    if n < 3:
+    if n < 3 and periodic:
         raise ValueError("periodic grids need at least 3 cells per direction")
+    if n < 1:
+        raise ValueError("need at least one cell per direction")
     if nd == 2:
-        vcoord, t, nv = _square_tris(n, length)
+        vcoord, t, nv = _square_tris(n, length, periodic)
     else:
-        vcoord, t, nv = _cube_tets(n, length)
+        vcoord, t, nv = _cube_tets(n, length, periodic)
     ne = t.shape[0]
     nfe, npf, npv = master.nfe, master.npf, master.npv
     nvf = nd
@@ -126,7 +136,7 @@ def build_mesh(master: Master, n: int, length: float) -> Mesh:
     rank[order] = np.arange(order.size)
     fid = rank[inverse]                                  # face id per element face
     nf = order.size
-    if nf * 2 != ne * nfe:
+    if periodic and nf * 2 != ne * nfe:
         raise RuntimeError("periodic mesh is not closed (every face needs two elements)")
     face_first = first[order]                            # element-face index of the first owner
     canon = lv[face_first]                               # (nf, nvf)
@@ -161,6 +171,21 @@ def build_mesh(master: Master, n: int, length: float) -> Mesh:
     t2t = np.where(face_elems[t2f, 0] == np.arange(ne)[:, None], face_elems[t2f, 1], face_elems[t2f, 0])
     if np.any(face_elems[t2f, 0] == face_elems[t2f, 1]):
         raise RuntimeError("an element meets itself across a face")
+    bf = t2t.copy()
+    if not periodic:
+        # boundary element faces: side index from the face centroid
+        cen = vcoord[:, faces, :].mean(axis=2)           # (ne, nfe, nd)
+        for e, a in zip(*np.nonzero(t2t < 0)):
+            c = cen[e, a]
+            side = -1
+            for ax in range(nd):
+                if abs(c[ax]) < 1e-9 * length:
+                    side = 2 * ax
+                elif abs(c[ax] - length) < 1e-9 * length:
+                    side = 2 * ax + 1
+            if side < 0:
+                raise RuntimeError("boundary face off the box")
+            bf[e, a] = -(side + 1)
 
     # ent2ent: faces sharing an element with face i; diagonal first, rest ascending
     rows = [[] for _ in range(nf)]
@@ -178,5 +203,5 @@ def build_mesh(master: Master, n: int, length: float) -> Mesh:
     colidx = np.array(cols, dtype=np.int64)
 
     return Mesh(nd=nd, ne=ne, nf=nf, nv=nv, npv=npv, npf=npf, nfe=nfe, dgnodes=np.ascontiguousarray(dg),
-                t=t, t2f=t2f, t2t=t2t, bf=t2t.copy(), elcon=elcon.reshape(ne, nfe * npf),
+                t=t, t2f=t2f, t2t=t2t, bf=bf, elcon=elcon.reshape(ne, nfe * npf),
                 face_verts=canon, face_elems=face_elems, rowstart=rowstart, colidx=colidx)

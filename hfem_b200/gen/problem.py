@@ -45,6 +45,8 @@ class Problem:
     sh: np.ndarray               # (ne, nc, npv)
     dt: float = 0.0
     meta: dict = field(default_factory=dict)
+    bcm: np.ndarray = None       # boundary condition type per boundary index (app.bcm); None: periodic
+    bcs: np.ndarray = None       # (nbnd, nch) boundary states (app.bcs)
 
     @property
     def nd(self):
@@ -118,5 +120,52 @@ def ns3d_tgv(n=16, porder=3, mach=0.1, re=1600.0, dt=0.01):
     return _finish("ns3d_tgv", master, mesh, udg, gamma, re, 0.72, mach, 2.0, dt, meta)
 
 
+def _freestream(nd, gamma, mach):
+    """Conserved free-stream state: rho 1, velocity 1 along x, p = 1/(gamma M^2)."""
+    p = 1.0 / (gamma * mach * mach)
+    u = np.zeros(nd + 2)
+    u[0], u[1] = 1.0, 1.0
+    u[nd + 1] = p / (gamma - 1.0) + 0.5
+    return u
+
+
+# boundary condition types of the reference's NS boundary flux (application/FM/fbou.cpp)
+BC_NOSLIP_ADIABATIC, BC_DIRICHLET, BC_EXTRAPOLATION, BC_SLIP = 2, 5, 6, 7
+
+
+def ns2d_channel(n=16, porder=2, seed=0, mach=0.5, re=100.0, dt=0.1, noise=1e-3, length=10.0,
+                 bcm=(BC_DIRICHLET, BC_EXTRAPOLATION, BC_SLIP, BC_NOSLIP_ADIABATIC)):
+    """[0,L]^2 box (not periodic), isentropic vortex + noise.  Sides ib = 2 axis + end:
+    0 x=0 (Dirichlet free stream), 1 x=L (extrapolation), 2 y=0 (slip wall),
+    3 y=L (no-slip adiabatic wall)."""
+    master = make_master(2, porder)
+    mesh = build_mesh(master, n, length, periodic=False)
+    gamma = 1.4
+    udg = make_udg(master, mesh, "vortex", gamma, mach, seed=seed, noise=noise,
+                   centre=(0.5 * length, 0.5 * length))
+    meta = dict(kind="ns2d_channel", n=n, porder=porder, seed=seed, mach=mach, re=re, dt=dt, noise=noise,
+                length=length, bcm=list(bcm))
+    p = _finish("ns2d_channel", master, mesh, udg, gamma, re, 0.72, mach, 2.0, dt, meta)
+    p.bcm = np.array(bcm, dtype=np.int64)
+    p.bcs = np.tile(_freestream(2, gamma, mach), (len(bcm), 1))
+    return p
+
+
+def ns3d_box(n=4, porder=2, seed=0, mach=0.3, re=400.0, dt=0.01,
+             bcm=(BC_DIRICHLET, BC_EXTRAPOLATION, BC_SLIP, BC_NOSLIP_ADIABATIC, BC_SLIP, BC_EXTRAPOLATION)):
+    """Unit cube (not periodic), uniform flow + Fourier modes; one condition per side
+    (ib = 2 axis + end)."""
+    master = make_master(3, porder)
+    mesh = build_mesh(master, n, 1.0, periodic=False)
+    gamma = 1.4
+    udg = make_udg(master, mesh, "fourier", gamma, mach, seed=seed)
+    meta = dict(kind="ns3d_box", n=n, porder=porder, seed=seed, mach=mach, re=re, dt=dt, bcm=list(bcm))
+    p = _finish("ns3d_box", master, mesh, udg, gamma, re, 0.72, mach, 2.0, dt, meta)
+    p.bcm = np.array(bcm, dtype=np.int64)
+    p.bcs = np.tile(_freestream(3, gamma, mach), (len(bcm), 1))
+    return p
+
+
 def make_problem(kind: str, **kw) -> Problem:
-    return {"ns2d_vortex": ns2d_vortex, "ns3d_fourier": ns3d_fourier, "ns3d_tgv": ns3d_tgv}[kind](**kw)
+    return {"ns2d_vortex": ns2d_vortex, "ns3d_fourier": ns3d_fourier, "ns3d_tgv": ns3d_tgv,
+            "ns2d_channel": ns2d_channel, "ns3d_box": ns3d_box}[kind](**kw)

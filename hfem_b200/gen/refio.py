@@ -68,7 +68,9 @@ def write_app(path, prob: Problem, **kw):
         np.array([m.pgauss]),                 # pgauss
         np.array([m.pgauss]),                 # pgaussR
         np.array([0.0]),                      # quadtype
-        np.zeros(0), np.zeros(0), np.zeros(0), np.zeros(0),   # bcm bcs bcd bcv
+        np.zeros(0) if prob.bcm is None else np.asarray(prob.bcm, dtype=np.float64),          # bcm
+        np.zeros(0) if prob.bcs is None else np.ascontiguousarray(prob.bcs, dtype=np.float64).ravel(),  # bcs[ib*nch + c]
+        np.zeros(0), np.zeros(0),             # bcd bcv
         dt, flag, factor, problem, prob.param, solversparam,
     ]
     ndims = np.zeros(40)

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <vector>
 #include <algorithm>
 
@@ -39,6 +40,9 @@ struct oracle_problem {
     double param[6];                                   // gamma eps Re Pr Mach tau
     int tdep;
     double fc_u, fc_q, time;
+    const int *bf;                                     // nfe x ne; < 0: boundary -(ib+1); NULL: none
+    const int *bcm;                                    // boundary condition type per ib (app.bcm)
+    const double *bcs;                                 // nch per ib (app.bcs)
 };
 
 }  // extern "C"
@@ -48,7 +52,7 @@ namespace {
 // ------------------------------------------------------------ dual numbers
 // Forward-mode derivatives for the pointwise flux Jacobian (the reference uses
 // symbolically generated derivatives, application/FM/nsNew/flux_ns2dNEW.c).
-constexpr int NDMAX = 20;
+constexpr int NDMAX = 32;
 struct Dual {
     double v;
     double d[NDMAX];
@@ -110,6 +114,55 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
         Dual heat = q[nd + 1] / rho - E * q[0] / (rho * rho) - vdv;
         f[d * ncu + nd + 1] = fe + kappa * heat;
     }
+}
+
+// Boundary flux fb(u, q, uh) of the NS boundary conditions (application/FM/fbou.cpp)
+// at one point, with its Jacobians fb_u[j + nch*k] (k over u and q) and
+// fb_uh[j + nch*k], by forward differentiation over (u, q, uh):
+//   2 no-slip adiabatic wall (fbou.cpp:219-277, fixed mesh): rho - rho_hat,
+//     -m_hat (wall velocity 0), energy row = the interior trace flux
+//     F(uh, q).n + tau (u - uh) of fhatDriver;
+//   5 Dirichlet (fbou.cpp:569-583): tau (ui - uh);
+//   6 extrapolation (fbou.cpp:584-600): u - uh;
+//   7 slip wall (fbou.cpp:601-652, fixed mesh): rho - rho_hat,
+//     m - (m.n) n - m_hat, E - E_hat.
+// Returns nonzero for a type that is not restated.
+static int fbou_point(int bn, int nd, const double* param, const double* ui, const double* nl, const double* w,
+                      const double* uh, double* fb, double* fb_u, double* fb_uh) {
+    const int ncu = nd + 2, nc = ncu * (nd + 1), nch = ncu, nv = nc + nch;
+    const double tau = param[5];
+    std::vector<Dual> W(nc), U(nch), F(nch), fl(ncu * nd);
+    for (int k = 0; k < nc; k++) W[k] = dvar(w[k], nv, k);
+    for (int k = 0; k < nch; k++) U[k] = dvar(uh[k], nv, nc + k);
+    if (bn == 2) {
+        F[0] = W[0] - U[0];
+        for (int j = 0; j < nd; j++) F[1 + j] = dconst(0.0, nv) - U[1 + j];
+        std::vector<Dual> wf(nc);
+        for (int k = 0; k < ncu; k++) wf[k] = U[k];
+        for (int k = ncu; k < nc; k++) wf[k] = W[k];
+        ns_flux(nd, param, wf.data(), fl.data());
+        Dual t = tau * (W[nd + 1] - U[nd + 1]);
+        for (int d = 0; d < nd; d++) t = t + nl[d] * fl[d * ncu + nd + 1];
+        F[nd + 1] = t;
+    } else if (bn == 5) {
+        for (int j = 0; j < nch; j++) F[j] = tau * (dconst(ui[j], nv) - U[j]);
+    } else if (bn == 6) {
+        for (int j = 0; j < nch; j++) F[j] = W[j] - U[j];
+    } else if (bn == 7) {
+        F[0] = W[0] - U[0];
+        Dual un = dconst(0.0, nv);
+        for (int i = 0; i < nd; i++) un = un + nl[i] * W[1 + i];
+        for (int j = 0; j < nd; j++) F[1 + j] = W[1 + j] - nl[j] * un - U[1 + j];
+        F[nd + 1] = W[nd + 1] - U[nd + 1];
+    } else {
+        return 1;
+    }
+    for (int j = 0; j < nch; j++) {
+        fb[j] = F[j].v;
+        for (int k = 0; k < nc; k++) fb_u[j + nch * k] = F[j].d[k];
+        for (int k = 0; k < nch; k++) fb_uh[j + nch * k] = F[j].d[nc + k];
+    }
+    return 0;
 }
 
 // Pointwise flux and Jacobian: f[g + ng*(c + ncu*d)], f_udg[g + ng*(c + ncu*(d + nd*k))].
@@ -460,15 +513,44 @@ static void element(const oracle_problem& P, const Dims& D, const double* udg_al
             }
         }
     }
+    // On boundary faces the trace equations take the boundary flux instead
+    // (faceint 1075-1246): tn_* = fn_* except there; the element equations keep fn_*.
+    std::vector<double> tn_(fn_), tn_u(fn_u), tn_uh(fn_uh);
+    if (P.bf) {
+        std::vector<double> wq(nc), uq(nch), fb(nch), fbu(nch * nc), fbuh(nch * nch), nlq(nd);
+        for (int fc = 0; fc < nfe; fc++) {
+            const int bfv = P.bf[(size_t)ie * nfe + fc];
+            if (bfv >= 0) continue;
+            const int ib = -bfv - 1, bn = P.bcm[ib];
+            for (int g = 0; g < ngf; g++) {
+                const int gg = g + ngf * fc;
+                for (int c = 0; c < nc; c++) wq[c] = ugf[gg + na * c];
+                for (int c = 0; c < nch; c++) uq[c] = uhg[gg + na * c];
+                for (int d = 0; d < nd; d++) nlq[d] = G.nl[gg + na * d];
+                if (fbou_point(bn, nd, P.param, P.bcs + (size_t)ib * nch, nlq.data(), wq.data(), uq.data(), fb.data(),
+                               fbu.data(), fbuh.data()))
+                    { std::fprintf(stderr, "boundary condition type %d not restated\n", bn); std::abort(); }
+                const double jf = G.jacf[gg];
+                for (int j = 0; j < nch; j++) {
+                    tn_[gg + na * j] = fb[j] * jf;
+                    for (int k = 0; k < nc; k++) tn_u[gg + na * (j + nch * k)] = fbu[j + nch * k] * jf;
+                    for (int k = 0; k < nch; k++) tn_uh[gg + na * (j + nch * k)] = fbuh[j + nch * k] * jf;
+                }
+            }
+        }
+    }
     // face residual Rutmp(m, fc, j) = sum_g psi_m w fhn
     O.Rh.assign(nb, 0.0);
     for (int fc = 0; fc < nfe; fc++)
         for (int j = 0; j < nch; j++)
             for (int m = 0; m < npf; m++) {
-                double t = 0;
-                for (int g = 0; g < ngf; g++) t += P.shapfg[m + npf * g] * fn_[g + ngf * fc + na * j];
+                double t = 0, th = 0;
+                for (int g = 0; g < ngf; g++) {
+                    t += P.shapfg[m + npf * g] * fn_[g + ngf * fc + na * j];
+                    th += P.shapfg[m + npf * g] * tn_[g + ngf * fc + na * j];
+                }
                 O.Ru[P.perm[fc * npf + m] + npv * j] -= t;                       // faceint 853-855
-                O.Rh[j + nch * (fc * npf + m)] = -t;                              // faceint 1248-1251
+                O.Rh[j + nch * (fc * npf + m)] = -th;                             // faceint 1248-1251
             }
     // face mass-weighted Jacobians: BDtmp (wrt u), Ftmp (wrt uh)
     O.K.assign((size_t)nb * n, 0.0);
@@ -480,18 +562,22 @@ static void element(const oracle_problem& P, const Dims& D, const double* udg_al
                 const int row_e = P.perm[fc * npf + ks], col_e = P.perm[fc * npf + kk];
                 for (int j = 0; j < nch; j++) {
                     for (int m = 0; m < ncu; m++) {
-                        double t = 0;
-                        for (int g = 0; g < ngf; g++)
+                        double t = 0, th = 0;
+                        for (int g = 0; g < ngf; g++) {
                             t += P.shapfgdotshapfc[(ks + npf * kk) + npf2 * g] * fn_u[g + ngf * fc + na * (j + nch * m)];
+                            th += P.shapfgdotshapfc[(ks + npf * kk) + npf2 * g] * tn_u[g + ngf * fc + na * (j + nch * m)];
+                        }
                         O.Dm[row_e + npv * (j + ncu * (col_e + npv * m))] += t;                     // faceint 909-917
-                        O.K[j + nch * (fc * npf + ks) + nb * (col_e + npv * m)] = t;                 // faceint 1254-1277
+                        O.K[j + nch * (fc * npf + ks) + nb * (col_e + npv * m)] = th;                // faceint 1254-1277
                     }
                     for (int m = 0; m < nch; m++) {
-                        double t = 0;
-                        for (int g = 0; g < ngf; g++)
+                        double t = 0, th = 0;
+                        for (int g = 0; g < ngf; g++) {
                             t += P.shapfgdotshapfc[(ks + npf * kk) + npf2 * g] * fn_uh[g + ngf * fc + na * (j + nch * m)];
+                            th += P.shapfgdotshapfc[(ks + npf * kk) + npf2 * g] * tn_uh[g + ngf * fc + na * (j + nch * m)];
+                        }
                         O.F[row_e + npv * (j + ncu * (m + nch * (fc * npf + kk)))] += t;          // faceint 897-905
-                        O.H[j + nch * (fc * npf + ks) + nb * (m + nch * (fc * npf + kk))] = t;       // faceint 1281-1296
+                        O.H[j + nch * (fc * npf + ks) + nb * (m + nch * (fc * npf + kk))] = th;      // faceint 1281-1296
                     }
                 }
             }
@@ -519,26 +605,32 @@ static void element(const oracle_problem& P, const Dims& D, const double* udg_al
             for (int k = 0; k < ncu; k++)
                 for (int j = 0; j < ncu; j++) {
                     for (int a = 0; a < npv; a++) {
-                        double t = 0;
+                        double t = 0, th = 0;
                         for (int g = 0; g < ngf; g++) {
-                            double v = 0;
-                            for (int d = 0; d < nd; d++)
+                            double v = 0, vh = 0;
+                            for (int d = 0; d < nd; d++) {
                                 v += fn_u[g + ngf * fc + na * (j + nch * (ncu * (1 + d) + k))] * sMiCf[g + ngf * fc + na * (a + npv * d)];
+                                vh += tn_u[g + ngf * fc + na * (j + nch * (ncu * (1 + d) + k))] * sMiCf[g + ngf * fc + na * (a + npv * d)];
+                            }
                             t += P.shapfg[ip + npf * g] * v;
+                            th += P.shapfg[ip + npf * g] * vh;
                         }
                         O.Dm[row_e + npv * (j + ncu * (a + npv * k))] += t;
-                        O.K[j + nch * fdof + nb * (a + npv * k)] += t;
+                        O.K[j + nch * fdof + nb * (a + npv * k)] += th;
                     }
                     for (int fn2 = 0; fn2 < ndf; fn2++) {
-                        double t = 0;
+                        double t = 0, th = 0;
                         for (int g = 0; g < ngf; g++) {
-                            double v = 0;
-                            for (int d = 0; d < nd; d++)
+                            double v = 0, vh = 0;
+                            for (int d = 0; d < nd; d++) {
                                 v += fn_u[g + ngf * fc + na * (j + nch * (ncu * (1 + d) + k))] * sMiEf[g + ngf * fc + na * (fn2 + ndf * d)];
+                                vh += tn_u[g + ngf * fc + na * (j + nch * (ncu * (1 + d) + k))] * sMiEf[g + ngf * fc + na * (fn2 + ndf * d)];
+                            }
                             t += P.shapfg[ip + npf * g] * v;
+                            th += P.shapfg[ip + npf * g] * vh;
                         }
                         O.F[row_e + npv * (j + ncu * (k + nch * fn2))] -= t;
-                        O.H[j + nch * fdof + nb * (k + nch * fn2)] -= t;
+                        O.H[j + nch * fdof + nb * (k + nch * fn2)] -= th;
                     }
                 }
         }

@@ -32,7 +32,11 @@ class OracleProblem(C.Structure):
         ("rowstart", _ip), ("colidx", _ip),
         ("param", C.c_double * 6), ("tdep", C.c_int),
         ("fc_u", C.c_double), ("fc_q", C.c_double), ("time", C.c_double),
+        ("bf", _ip), ("bcm", _ip), ("bcs", _dp),
     ]
+
+# boundary condition types restated in hfem_oracle.cpp (fbou_point)
+BC_TYPES = (2, 5, 6, 7)
 
 
 _lib = None
@@ -93,6 +97,13 @@ class Oracle:
         for i in range(6):
             p.param[i] = float(prob.param[i])
         p.tdep, p.fc_u, p.fc_q, p.time = prob.tdep, prob.fc_u, prob.fc_q, prob.time
+        if getattr(prob, "bcm", None) is not None:
+            if any(int(b) not in BC_TYPES for b in prob.bcm):
+                raise ValueError(f"boundary condition types {list(prob.bcm)} not all in {BC_TYPES}")
+            k["bf"] = np.ascontiguousarray(me.bf, dtype=np.int32)
+            k["bcm"] = np.ascontiguousarray(prob.bcm, dtype=np.int32)
+            k["bcs"] = np.ascontiguousarray(prob.bcs, dtype=np.float64)
+            p.bf, p.bcm, p.bcs = _i(k["bf"]), _i(k["bcm"]), _d(k["bcs"])
         self.p = p
         self.n = prob.n_local
         self.nb = prob.n_trace

@@ -4,7 +4,7 @@ Runs oracle/_ref/hfem_ref (the reference's serial hot path compiled from its
 sources by oracle/Makefile; needs the reference tree) on small seeded problems
 and stores its outputs next to the generated inputs:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 
 Each fixture holds the inputs (so the CPU tests also pin the generator) and
 the reference outputs: q from getQ, Hg / Rg / Rr, D^-1 Ru, D^-1 F, rNorm and the
@@ -22,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from hfem_b200.gen.problem import ns2d_vortex, ns3d_fourier  # noqa: E402
+from hfem_b200.gen.problem import ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier  # noqa: E402
 from oracle import run_reference  # noqa: E402
 
 CASES = {
@@ -31,6 +31,9 @@ CASES = {
     "ns2d_p3_n3": lambda: ns2d_vortex(n=3, porder=3),
     "ns3d_p1_n3": lambda: ns3d_fourier(n=3, porder=1),
     "ns3d_p3_n3": lambda: ns3d_fourier(n=3, porder=3),
+    # bounded meshes: Dirichlet, extrapolation, slip and no-slip adiabatic walls
+    "ns2d_channel_p2_n3": lambda: ns2d_channel(n=3, porder=2),
+    "ns3d_box_p1_n2": lambda: ns3d_box(n=2, porder=1),
 }
 FULL_LIMIT = 400_000          # store arrays up to this many entries in full
 
@@ -44,8 +47,10 @@ def squeeze(name, a):
     return {name + "_proj": p @ a.ravel(), name + "_absmax": np.array([np.max(np.abs(a))])}
 
 
-def main():
+def main(only=None):
     for key, make in CASES.items():
+        if only and key not in only:
+            continue
         prob = make()
         ref = run_reference(prob, ndump=2)
         out = dict(udg_in=prob.udg, uh_in=prob.uh, dgnodes=prob.mesh.dgnodes, elcon=prob.mesh.elcon,
@@ -54,6 +59,8 @@ def main():
             out.update(squeeze(k, ref[k]))
         np.savez_compressed(os.path.join(HERE, key + ".npz"), **out)
         print(key, {k: v.shape for k, v in out.items()})
+    if only:
+        return
     prob = ns2d_vortex(n=4, porder=2)
     ref = run_reference(prob, mode="newton", newton=dict(maxiter=2, precond=2, restart=50, tol=1e-10))
     np.savez_compressed(os.path.join(HERE, "ns2d_p2_n4_newton.npz"), rnorm_hist=ref["rnorm_hist"],
@@ -62,4 +69,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)      # optional: names of the fixtures to (re)make

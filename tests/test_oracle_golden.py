@@ -12,7 +12,7 @@ import os
 import numpy as np
 import pytest
 
-from hfem_b200.gen.problem import ns2d_vortex, ns3d_fourier
+from hfem_b200.gen.problem import ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier
 from oracle import Oracle
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -22,6 +22,8 @@ CASES = {
     "ns2d_p3_n3": lambda: ns2d_vortex(n=3, porder=3),
     "ns3d_p1_n3": lambda: ns3d_fourier(n=3, porder=1),
     "ns3d_p3_n3": lambda: ns3d_fourier(n=3, porder=3),
+    "ns2d_channel_p2_n3": lambda: ns2d_channel(n=3, porder=2),
+    "ns3d_box_p1_n2": lambda: ns3d_box(n=2, porder=1),
 }
 
 
