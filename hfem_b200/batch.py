@@ -46,14 +46,27 @@ def union_problem(probs: list) -> tuple:
     fe = np.concatenate([p.mesh.face_elems + eoff[i] for i, p in enumerate(probs)])
     fv = np.concatenate([p.mesh.face_verts for p in probs])
     tt = np.concatenate([p.mesh.t for p in probs])
+    # boundary flags: each problem's boundary indices shifted past the earlier problems'
+    bfl, bcm, bcs, nbnd = [], [], [], 0
+    for i, p in enumerate(probs):
+        pb = getattr(p, "bcm", None)
+        bfi = np.where(p.mesh.bf < 0, p.mesh.bf - nbnd, p.mesh.bf + eoff[i])
+        bfl.append(bfi)
+        if pb is not None:
+            bcm.extend(int(x) for x in pb)
+            bcs.append(np.asarray(p.bcs, dtype=np.float64))
+            nbnd += len(pb)
+    bf = np.concatenate(bfl)
     mesh = Mesh(nd=m.nd, ne=int(eoff[-1]), nf=int(foff[-1]), nv=0, npv=m.npv, npf=npf, nfe=m.nfe, dgnodes=dg,
-                t=tt, t2f=t2f, t2t=t2t, bf=t2t.copy(), elcon=elcon, face_verts=fv, face_elems=fe, rowstart=rs,
+                t=tt, t2f=t2f, t2t=t2t, bf=bf, elcon=elcon, face_verts=fv, face_elems=fe, rowstart=rs,
                 colidx=ci)
     eprob = np.repeat(np.arange(len(probs)), [p.mesh.ne for p in probs]).astype(np.int32)
     fprob = np.repeat(np.arange(len(probs)), [p.mesh.nf for p in probs]).astype(np.int32)
     params = np.array([[*p.param, float(p.tdep), p.fc_u] for p in probs], dtype=np.float64)
     u = replace(probs[0], name="union", mesh=mesh, udg=np.concatenate([p.udg for p in probs]),
-                uh=np.concatenate([p.uh for p in probs]), sh=np.concatenate([p.sh for p in probs]))
+                uh=np.concatenate([p.uh for p in probs]), sh=np.concatenate([p.sh for p in probs]),
+                bcm=np.array(bcm, dtype=np.int64) if bcm else None,
+                bcs=np.concatenate(bcs) if bcs else None)
     return u, eprob, fprob, params, eoff, foff * npf
 
 

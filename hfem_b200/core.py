@@ -51,6 +51,7 @@ def load_library(path: str = LIB):
     lib.hfem_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     lib.hfem_set_master.argtypes = [C.c_void_p] + [_dp] * 6 + [_ip]
     lib.hfem_set_mesh.argtypes = [C.c_void_p, _dp, _ip, _ip, _ip, _ip]
+    lib.hfem_set_boundary.argtypes = [C.c_void_p, _ip, C.c_int, _ip, _dp]
     lib.hfem_set_physics.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_double]
     lib.hfem_set_solution.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.hfem_set_solution_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -103,6 +104,8 @@ class HDGSolver:
         perm = np.ascontiguousarray(m.perm, dtype=np.int32)
         self._chk(self.lib.hfem_set_master(self.h, *[_d(k) for k in keep], _i(perm)), "set_master")
         self.set_mesh(me)
+        if getattr(prob, "bcm", None) is not None:
+            self.set_boundary(me.bf, prob.bcm, prob.bcs)
         self.set_physics(prob.param, prob.tdep, prob.fc_u, prob.fc_q, prob.time)
         self.set_solution(prob.udg, prob.uh, prob.sh)
 
@@ -136,6 +139,12 @@ class HDGSolver:
         k = self._mesh
         self._chk(self.lib.hfem_set_mesh(self.h, _d(k["dg"]), _i(k["elcon"]), _i(k["t2f"]), _i(k["rs"]), _i(k["ci"])),
                   "set_mesh")
+
+    def set_boundary(self, bf, bcm, bcs):
+        self._bnd = (np.ascontiguousarray(bf, dtype=np.int32), np.ascontiguousarray(bcm, dtype=np.int32),
+                     np.ascontiguousarray(bcs, dtype=np.float64))
+        b = self._bnd
+        self._chk(self.lib.hfem_set_boundary(self.h, _i(b[0]), int(b[1].size), _i(b[1]), _d(b[2])), "set_boundary")
 
     def set_physics(self, param, tdep, fc_u, fc_q, time=0.0):
         p = np.ascontiguousarray(param, dtype=np.float64)

@@ -94,6 +94,9 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
     double* sMiEf = sMiCf + S::W_SMICF;
     double* fnu = sMiEf + S::W_SMIEF;
     double* fnuh = fnu + S::W_FNU;
+    double* fnub = fnuh + S::W_FNUH;
+    double* fnuhb = fnub + S::W_FNUB;
+    double* fnb = fnuhb + S::W_FNUHB;
 
     // q-phase views into the union
     double* M = sm.un;
@@ -265,13 +268,48 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 }
             }
         }
+        // boundary faces: fb and its Jacobians at their points (one item per point and variable)
+        const int* bfe = A.bf ? A.bf + (size_t)e * NFE : nullptr;
+        if (bfe) {
+            for (int t = tid; t < NFE * NGF * (NC + NCH); t += NT) {
+                const int fc = t / (NGF * (NC + NCH)), r = t % (NGF * (NC + NCH));
+                if (bfe[fc] >= 0) continue;
+                using DD = Dual<1>;
+                const int q = r % NGF, k = r / NGF, gg = q + NGF * fc;
+                DD w[NC], uhd[NCH], fb[NCH];
+#pragma unroll
+                for (int c = 0; c < NC; c++) {
+                    w[c].v = ugf[gg + NA * c];
+                    w[c].d[0] = (c == k) ? 1.0 : 0.0;
+                }
+#pragma unroll
+                for (int c = 0; c < NCH; c++) {
+                    uhd[c].v = uhg[gg + NA * c];
+                    uhd[c].d[0] = (NC + c == k) ? 1.0 : 0.0;
+                }
+                double nlq[ND];
+#pragma unroll
+                for (int d = 0; d < ND; d++) nlq[d] = sm.nl[gg + NA * d];
+                const int ib = -bfe[fc] - 1;
+                if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb)) {
+                    for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
+                }
+                const double jf = sm.jacf[gg];
+#pragma unroll
+                for (int j = 0; j < NCH; j++) {
+                    if (k == 0) fnb[gg + NA * j] = fb[j].v * jf;
+                    if (k < NC) fnub[gg + NA * (j + NCH * k)] = fb[j].d[0] * jf;
+                    else fnuhb[gg + NA * (j + NCH * (k - NC))] = fb[j].d[0] * jf;
+                }
+            }
+        }
         __syncthreads();
 
         double* Ke = A.K + (size_t)e * NB * N;
         double* He = A.H + (size_t)e * NB * NB;
         double* Rhe = A.Rh + (size_t)e * NB;
         double* Roe = A.Ro + (size_t)e * NB;
-        double* Ys = fnuh + S::W_FNUH;      // Y(i,g,j,c) = sum_r shapvg(i,(g,r)) wrl((g,r), j, c)
+        double* Ys = fnb + S::W_FNB;        // Y(i,g,j,c) = sum_r shapvg(i,(g,r)) wrl((g,r), j, c)
         for (int t = tid; t < NB; t += NT) {
             const int j = t % NCH, fdof = t / NCH, fc = fdof / NPF, ip = fdof % NPF;
             double s = 0.0;
@@ -295,7 +333,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             }
         }
         // ---- K and H face by face: rows (ip, j, m), k = (q, d'), generated A = shapfg(ip,q) x fhn
-        for (int fc = 0; fc < NFE; fc++) {
+        // (fnu_s/fnuh_s: the face flux Jacobians, fhat or, on boundary faces later, fb)
+        auto face_rows = [&](int fc, const double* fnu_s, const double* fnuh_s) {
             __syncthreads();
             double* BK = Bs;                              // KFD x NPV  (ld C3::LDBK)
             double* BH = Bs + C3<S>::LDBK * C3<S>::NKP;   // KFD x NDF  (ld C3::LDBK)
@@ -342,10 +381,10 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                     if (rv && k < NGF * ND1) {
                         const double sf = sm.Af[ip + C2::LDAF * q];
                         if (dp == 0) {
-                            vK = sf * fnu[gg + NA * (j + NCH * m)];
-                            vH = sf * fnuh[gg + NA * (j + NCH * m)];
+                            vK = sf * fnu_s[gg + NA * (j + NCH * m)];
+                            vH = sf * fnuh_s[gg + NA * (j + NCH * m)];
                         } else {
-                            vK = sf * fnu[gg + NA * (j + NCH * (NCU * dp + m))];
+                            vK = sf * fnu_s[gg + NA * (j + NCH * (NCU * dp + m))];
                             vH = vK;
                         }
                     }
@@ -383,7 +422,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                         if (rv && f2 < NDF) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[b][h];
                     }
             }
-        }
+                };
+        for (int fc = 0; fc < NFE; fc++) face_rows(fc, fnu, fnuh);
         __syncthreads();
         // ---- D_vol = Y' Phi and F_vol = Y'_q Psi, B operands in shared memory
         {
@@ -489,6 +529,22 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         }
         const double tot = block_sum(ru2, sm.red);
         if (tid == 0) A.ru2[e] = tot;
+        // ---- boundary faces: their trace equations take the boundary flux
+        // (faceint 1075-1246); the element equations above keep fhat
+        if (bfe) {
+            for (int fc = 0; fc < NFE; fc++) {
+                if (bfe[fc] >= 0) continue;
+                __syncthreads();
+                for (int t = tid; t < NPF * NCH; t += NT) {
+                    const int j = t % NCH, ip = t / NCH;
+                    double s = 0.0;
+                    for (int q = 0; q < NGF; q++) s += sm.Af[ip + C2::LDAF * q] * fnb[q + NGF * fc + NA * j];
+                    Rhe[j + NCH * (fc * NPF + ip)] = -s;
+                    Roe[j + NCH * (fc * NPF + ip)] = -s;
+                }
+                face_rows(fc, fnub, fnuhb);
+            }
+        }
     }
 }
 

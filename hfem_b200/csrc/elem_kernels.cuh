@@ -35,7 +35,11 @@ struct Shape {
     static constexpr int W_SMIEF = NA * NDF * ND;
     static constexpr int W_FNU = NA * NCH * NC;
     static constexpr int W_FNUH = NA * NCH * NCH;
-    static constexpr int WS = W_WRL + W_SMIC + W_SMIE + W_SMICF + W_SMIEF + W_FNU + W_FNUH;
+    // boundary faces: the boundary flux and its Jacobians at the face points
+    static constexpr int W_FNUB = NA * NCH * NC;
+    static constexpr int W_FNUHB = NA * NCH * NCH;
+    static constexpr int W_FNB = NA * NCH;
+    static constexpr int WS = W_WRL + W_SMIC + W_SMIE + W_SMICF + W_SMIEF + W_FNU + W_FNUH + W_FNUB + W_FNUHB + W_FNB;
 };
 
 struct Tables {                 // master element tables, reference layouts
@@ -58,6 +62,11 @@ struct ElemArgs {
     // problem, and per problem [gamma, eps, Re, Pr, Mach, tau, tdep, fc_u]
     const int* eprob;
     const double* pparam;
+    // boundary faces (NULL bf = none): bf[e * nfe + face] < 0 is boundary -(ib + 1),
+    // condition bcm[ib] (fbou.cpp types 2, 5, 6, 7) with state bcs[ib * nch + c]
+    const int* bf;
+    const int* bcm;
+    const double* bcs;
 };
 
 constexpr int NT = 256;         // threads per CTA for element kernels

@@ -192,6 +192,10 @@ struct hfem_ctx {
     int grid_elem = 0, grid_schur = 0, grid_inv = 0, grid_tc = 0;
     int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
     int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
+    // boundary faces (mesh.bf, app.bcm, app.bcs); bf == NULL: no boundary faces
+    int *bf = nullptr, *bcm = nullptr;
+    double* bcs = nullptr;
+    int nbnd = 0;
     int* tc_err = nullptr;
     double* rn_part = nullptr;
     // master tables
@@ -348,6 +352,9 @@ int ensure_assembly_buffers(hfem_ctx* c) {
 
 ElemArgs elem_args(hfem_ctx* c) {
     ElemArgs a;
+    a.bf = c->bf;
+    a.bcm = c->bcm;
+    a.bcs = c->bcs;
     a.T = Tables{c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm};
     a.dgnodes = c->dgnodes;
     a.elcon = c->elcon;
@@ -1247,7 +1254,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
-                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part,
+                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
                     c->d_lvl_lo, c->d_lvl_up};
     for (void* p : ptrs)
@@ -1351,7 +1358,49 @@ int hfem_set_mesh(hfem_ctx* c, const double* dgnodes, const int* elcon, const in
     c->h_rowstart.assign(rowstart, rowstart + nf + 1);
     c->h_colidx.assign(colidx, colidx + nblk);
     c->have_order = false;
+    if (c->bf) { cudaFree(c->bf); c->bf = nullptr; }       // boundary flags belong to the old mesh
     c->have_mesh = true;
+    return 0;
+}
+
+int hfem_set_boundary(hfem_ctx* c, const int* bf, int nbnd, const int* bcm, const double* bcs) {
+    if (!c || !bf || nbnd < 0 || (nbnd > 0 && (!bcm || !bcs))) return HFEM_E_ARG;
+    if (!c->have_mesh) return fail(c, HFEM_E_STATE, "set the mesh before its boundary");
+    const hfem_dims& d = c->dims;
+    for (int b = 0; b < nbnd; b++)
+        if (bcm[b] != 2 && bcm[b] != 5 && bcm[b] != 6 && bcm[b] != 7)
+            return fail(c, HFEM_E_UNSUPPORTED, "boundary condition type %d (supported: 2, 5, 6, 7)", bcm[b]);
+    // a boundary face belongs to one element, an interior one to two
+    std::vector<int> fsrc((size_t)d.nf * 4);
+    CK(cudaMemcpy(fsrc.data(), c->face_src, sizeof(int) * fsrc.size(), cudaMemcpyDeviceToHost));
+    int any = 0;
+    for (int e = 0; e < d.ne; e++)
+        for (int a = 0; a < d.nfe; a++) {
+            const int v = bf[(size_t)e * d.nfe + a];
+            if (v < 0) {
+                if (-v - 1 >= nbnd) return fail(c, HFEM_E_ARG, "bf of element %d face %d names boundary %d", e, a, -v - 1);
+                any = 1;
+            }
+        }
+    for (int f = 0; f < d.nf; f++) {
+        const bool two = fsrc[(f * 2 + 1) * 2] >= 0;
+        const int e = fsrc[(f * 2) * 2], a = fsrc[(f * 2) * 2 + 1];
+        const bool bnd = bf[(size_t)e * d.nfe + a] < 0;
+        if (bnd == two) return fail(c, HFEM_E_MESH, "face %d: boundary flag and element count disagree", f);
+    }
+    int rc;
+    CK(cudaSetDevice(c->device));
+    if (!any) {
+        if (c->bf) { cudaFree(c->bf); c->bf = nullptr; }
+        c->nbnd = 0;
+        return 0;
+    }
+    if ((rc = upload(c, &c->bf, bf, (size_t)d.ne * d.nfe)) || (rc = upload(c, &c->bcm, bcm, (size_t)nbnd)) ||
+        (rc = upload(c, &c->bcs, bcs, (size_t)nbnd * c->nch)))
+        return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    c->nbnd = nbnd;
+    c->assembled = false;
     return 0;
 }
 
@@ -2010,6 +2059,9 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.ws = scratch;
     a.eprob = nullptr;
     a.pparam = nullptr;
+    a.bf = nullptr;
+    a.bcm = nullptr;
+    a.bcs = nullptr;
     L->element(dim3(ge), L->elem_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     SchurArgs s{d.ne, D, DinvF, K, H, DinvRu, Rh, info};

@@ -122,4 +122,57 @@ __device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, c
     }
 }
 
+// Boundary flux fb(u, q, uh) of the NS boundary conditions at one point
+// (application/FM/fbou.cpp on a fixed mesh), in dual numbers so that one pass
+// per differentiated variable gives fb and its derivative:
+//   2 no-slip adiabatic wall: rho - rho_hat, -m_hat, and for energy the
+//     interior trace flux F(uh, q).n + tau (E - E_hat);
+//   5 Dirichlet: tau (ui - uh);   6 extrapolation: u - uh;
+//   7 slip wall: rho - rho_hat, m - (m.n) n - m_hat, E - E_hat.
+// w holds (u, q) (NC entries), uh the trace state (NCH); returns false for a
+// type without a restatement.
+template <int ND, int M>
+__device__ __forceinline__ bool ns_fbou_dual(int bn, const double* __restrict__ param, const double* ui,
+                                             const double* nl, const Dual<M>* w, const Dual<M>* uh, Dual<M>* fb) {
+    constexpr int NCU = ND + 2, NC = NCU * (ND + 1);
+    const double tau = param[5];
+    if (bn == 2) {
+        fb[0] = w[0] - uh[0];
+#pragma unroll
+        for (int j = 0; j < ND; j++) fb[1 + j] = dc<M>(0.0) - uh[1 + j];
+        Dual<M> wf[NC], f[ND * NCU];
+#pragma unroll
+        for (int k = 0; k < NCU; k++) wf[k] = uh[k];
+#pragma unroll
+        for (int k = NCU; k < NC; k++) wf[k] = w[k];
+        ns_flux_dual<ND, M>(param, wf, f);
+        Dual<M> t = tau * (w[ND + 1] - uh[ND + 1]);
+#pragma unroll
+        for (int d = 0; d < ND; d++) t = t + nl[d] * f[d * NCU + ND + 1];
+        fb[ND + 1] = t;
+        return true;
+    }
+    if (bn == 5) {
+#pragma unroll
+        for (int j = 0; j < NCU; j++) fb[j] = tau * (dc<M>(ui[j]) - uh[j]);
+        return true;
+    }
+    if (bn == 6) {
+#pragma unroll
+        for (int j = 0; j < NCU; j++) fb[j] = w[j] - uh[j];
+        return true;
+    }
+    if (bn == 7) {
+        fb[0] = w[0] - uh[0];
+        Dual<M> un = dc<M>(0.0);
+#pragma unroll
+        for (int i = 0; i < ND; i++) un = un + nl[i] * w[1 + i];
+#pragma unroll
+        for (int j = 0; j < ND; j++) fb[1 + j] = w[1 + j] - nl[j] * un - uh[1 + j];
+        fb[ND + 1] = w[ND + 1] - uh[ND + 1];
+        return true;
+    }
+    return false;
+}
+
 }  // namespace hfem

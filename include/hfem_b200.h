@@ -67,6 +67,15 @@ int hfem_set_master(hfem_ctx* ctx, const double* shapvt, const double* shapvg, c
 int hfem_set_mesh(hfem_ctx* ctx, const double* dgnodes, const int* elcon, const int* t2f,
                   const int* ent2entStart, const int* ent2ent);
 
+/* Boundary faces of a bounded mesh (mesh.bf, app.bcm, app.bcs of the
+ * reference; faceint elementassembly.cpp:1075-1246 with fbouDriver): bf[ne x
+ * nfe] element-major, >= 0 interior, -(ib + 1) on boundary ib; bcm[nbnd] the
+ * boundary condition types (2 no-slip adiabatic wall, 5 Dirichlet, 6
+ * extrapolation, 7 slip wall, as application/FM/fbou.cpp on a fixed mesh);
+ * bcs[nbnd x nch] their states.  The trace equations of boundary faces take
+ * the boundary flux.  Call after hfem_set_mesh (which clears it). */
+int hfem_set_boundary(hfem_ctx* ctx, const int* bf, int nbnd, const int* bcm, const double* bcs);
+
 /* Physics: physicsparam = [gamma, eps, Re, Pr, Mach, tau] (compressible
  * Navier-Stokes, constant tau, constant viscosity), tdep/fc_u/fc_q/time as
  * appstruct (digasopre.h:7-91).  appname 1 (NS) is the one supported. */
