@@ -219,6 +219,7 @@ struct hfem_ctx {
     int* info = nullptr;
     // Krylov
     double *Minv = nullptr, *V = nullptr, *w = nullptr, *x = nullptr, *pb = nullptr, *scal = nullptr, *part = nullptr;
+    float* Minv32 = nullptr;    // FP32 block-Jacobi inverses (mixed mode)
     int* binfo = nullptr;
     int krylov_restart = 0;
     double* udgi = nullptr;     // state at the start of the current time step
@@ -766,14 +767,18 @@ int bilu0_apply(hfem_ctx* c, const double* x, double* v) {
 int matvec_prec(hfem_ctx* c, const double* x, double* z, bool prec) {
     Timed t(c, "matvec");
     if (prec && c->prec_kind == 0) {
-        bsr_matvec_bj_kernel<<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
-            c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, nullptr, x, c->bl_t);
+        bsr_matvec_bj_kernel<double><<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
+            c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, (const double*)nullptr, x, c->bl_t);
         int rc = check_launch(c, "matvec");
         if (rc) return rc;
         return bilu0_apply(c, c->bl_t, z);
     }
-    bsr_matvec_bj_kernel<<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
-        c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, prec ? c->Minv : nullptr, x, z);
+    if (prec && c->precision == 1)
+        bsr_matvec_bj_kernel<float><<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
+            c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, c->Minv32, x, z);
+    else
+        bsr_matvec_bj_kernel<double><<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
+            c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, prec ? c->Minv : nullptr, x, z);
     return check_launch(c, "matvec");
 }
 
@@ -823,7 +828,14 @@ int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int
         CK(cudaStreamSynchronize(c->stream));
         for (int i = 0; i < c->dims.nf; i++)
             if (bi[i]) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d is singular", i);
-        bj_apply_kernel<<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv, c->Rg, c->pb);
+        if (c->precision == 1) {
+            const long long nm = (long long)c->dims.nf * c->bsz * c->bsz;
+            if (!c->Minv32 && (rc = dalloc(c, &c->Minv32, (size_t)nm))) return rc;
+            to_float_kernel<<<g, 256, 0, c->stream>>>(nm, c->Minv, c->Minv32);
+            bj_apply_kernel<float><<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv32, c->Rg, c->pb);
+        } else {
+            bj_apply_kernel<double><<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv, c->Rg, c->pb);
+        }
     } else {
         CK(cudaMemcpyAsync(c->pb, c->Rg, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
     }
@@ -915,10 +927,14 @@ int matvec_warp(hfem_ctx* c, const double* x, double* z, bool prec, const unsign
     const double* M = prec ? c->Minv : nullptr;
     const int* rseg = act ? c->fprob : nullptr;
     switch (c->bsz) {
-#define HFEM_MV(B)                                                                                               \
-    case B:                                                                                                      \
-        bsr_matvec_warp_kernel<B><<<grid, 256, 0, c->stream>>>(c->dims.nf, c->rowstart, c->colidx, c->Hg, M, x, z, \
-                                                                 rseg, act);                                     \
+#define HFEM_MV(B)                                                                                                \
+    case B:                                                                                                       \
+        if (prec && c->precision == 1)                                                                            \
+            bsr_matvec_warp_kernel<B, float><<<grid, 256, 0, c->stream>>>(c->dims.nf, c->rowstart, c->colidx,      \
+                                                                            c->Hg, c->Minv32, x, z, rseg, act);   \
+        else                                                                                                      \
+            bsr_matvec_warp_kernel<B, double><<<grid, 256, 0, c->stream>>>(c->dims.nf, c->rowstart, c->colidx,     \
+                                                                             c->Hg, M, x, z, rseg, act);          \
         break;
         HFEM_MV(8) HFEM_MV(12) HFEM_MV(15) HFEM_MV(16) HFEM_MV(20) HFEM_MV(30) HFEM_MV(50)
 #undef HFEM_MV
@@ -961,7 +977,14 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
         CK(cudaStreamSynchronize(c->stream));
         for (int i = 0; i < c->dims.nf; i++)
             if (bi[i]) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d is singular", i);
-        bj_apply_kernel<<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv, c->Rg, c->pb);
+        if (c->precision == 1) {
+            const long long nm = (long long)c->dims.nf * c->bsz * c->bsz;
+            if (!c->Minv32 && (rc = dalloc(c, &c->Minv32, (size_t)nm))) return rc;
+            to_float_kernel<<<g, 256, 0, c->stream>>>(nm, c->Minv, c->Minv32);
+            bj_apply_kernel<float><<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv32, c->Rg, c->pb);
+        } else {
+            bj_apply_kernel<double><<<g, 256, 0, c->stream>>>(c->dims.nf, c->bsz, c->Minv, c->Rg, c->pb);
+        }
     } else {
         CK(cudaMemcpyAsync(c->pb, c->Rg, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
     }
@@ -1254,7 +1277,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
-                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs,
+                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
                     c->d_lvl_lo, c->d_lvl_up};
     for (void* p : ptrs)

@@ -84,8 +84,9 @@ __global__ void bj_inverse_kernel(int nrows, int bsz, const int* __restrict__ ro
 
 // z = M^-1 (Hg x) for every block row (M^-1 == NULL: z = Hg x).
 // One CTA of 64 threads per block row, rows r = threadIdx.x < bsz.
+template <typename MT>
 __global__ void bsr_matvec_bj_kernel(int nrows, int bsz, const int* __restrict__ rowstart, const int* __restrict__ colidx,
-                                     const double* __restrict__ Hg, const double* __restrict__ Minv,
+                                     const double* __restrict__ Hg, const MT* __restrict__ Minv,
                                      const double* __restrict__ x, double* __restrict__ z) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* y = reinterpret_cast<double*>(smem_raw);
@@ -107,26 +108,33 @@ __global__ void bsr_matvec_bj_kernel(int nrows, int bsz, const int* __restrict__
         if (r < bsz) y[r] = s;
         __syncthreads();
         if (r < bsz) {
-            const double* m = Minv + (size_t)i * bsz * bsz;
+            const MT* m = Minv + (size_t)i * bsz * bsz;
             double t = 0.0;
-            for (int c = 0; c < bsz; c++) t += m[r + bsz * c] * y[c];
+            for (int c = 0; c < bsz; c++) t += (double)m[r + bsz * c] * y[c];
             z[(size_t)i * bsz + r] = t;
         }
     }
 }
 
-// z = M^-1 b (block-diagonal apply).
-__global__ void bj_apply_kernel(int nrows, int bsz, const double* __restrict__ Minv, const double* __restrict__ b,
+// z = M^-1 b (block-diagonal apply; MT = float: the FP32 preconditioner of the mixed mode).
+template <typename MT>
+__global__ void bj_apply_kernel(int nrows, int bsz, const MT* __restrict__ Minv, const double* __restrict__ b,
                                 double* __restrict__ z) {
     const long long total = (long long)nrows * bsz;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / bsz), r = (int)(t % bsz);
-        const double* m = Minv + (size_t)i * bsz * bsz;
+        const MT* m = Minv + (size_t)i * bsz * bsz;
         const double* bi = b + (size_t)i * bsz;
         double s = 0.0;
-        for (int c = 0; c < bsz; c++) s += m[r + bsz * c] * bi[c];
+        for (int c = 0; c < bsz; c++) s += (double)m[r + bsz * c] * bi[c];
         z[t] = s;
     }
+}
+
+// FP32 copy of the block-Jacobi inverses (the mixed mode's preconditioner).
+__global__ void to_float_kernel(long long n, const double* __restrict__ a, float* __restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
 }
 
 // Deterministic dot product: fixed grid of DOT_CTAS partial sums, then one CTA.

@@ -132,11 +132,11 @@ __global__ void __launch_bounds__(SEG_THREADS) seg_sub_from_kernel(SegPieces P, 
 // lanes form G = 32 / BSZ column groups of BSZ rows (R = 2 rows per lane when
 // BSZ > 32), and the groups' partial sums are added in group order.  Rows of
 // inactive segments (act[rseg[i]] == 0) are skipped.
-template <int BSZ>
+template <int BSZ, typename MT>
 __global__ void __launch_bounds__(256) bsr_matvec_warp_kernel(int nrows, const int* __restrict__ rowstart,
                                                               const int* __restrict__ colidx,
                                                               const double* __restrict__ Hg,
-                                                              const double* __restrict__ Minv,
+                                                              const MT* __restrict__ Minv,
                                                               const double* __restrict__ x, double* __restrict__ z,
                                                               const int* __restrict__ rseg,
                                                               const unsigned char* __restrict__ act) {
@@ -200,14 +200,14 @@ __global__ void __launch_bounds__(256) bsr_matvec_warp_kernel(int nrows, const i
             if (r < BSZ) ys[wib][0][r] = y[t];
         }
         __syncwarp();
-        const double* m = Minv + (size_t)i * BSZ * BSZ;
+        const MT* m = Minv + (size_t)i * BSZ * BSZ;
 #pragma unroll
         for (int t = 0; t < R; t++) {
             const int r = lane + 32 * t;
             if (r < BSZ) {
                 double s = 0.0;
 #pragma unroll 4
-                for (int c = 0; c < BSZ; c++) s += __ldg(&m[(size_t)c * BSZ + r]) * ys[wib][0][c];
+                for (int c = 0; c < BSZ; c++) s += (double)__ldg(&m[(size_t)c * BSZ + r]) * ys[wib][0][c];
                 z[(size_t)i * BSZ + r] = s;
             }
         }

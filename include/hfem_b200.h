@@ -137,12 +137,13 @@ int hfem_newton(hfem_ctx* ctx, double newton_tol, int newton_maxiter, int precon
 int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newton_tol, int newton_maxiter,
                    int precond, int restart, double gmres_tol, int gmres_maxit, int* newton_iters);
 
-/* Arithmetic of the assembly (no counterpart in the reference, which is FP64
- * throughout).  mode 0: FP64 everywhere (default).  mode 1: the two Schur
- * GEMMs (D^-1 F and H - K D^-1 F) on the tcgen05 tensor cores in TF32 with
- * FP32 accumulation; the element LU, the residuals (rnorm), the Arnoldi
- * process and the Newton update stay FP64, so Newton iterations refine the
- * solution to the FP64 residual tolerance. */
+/* Arithmetic of the assembly and solve (no counterpart in the reference, which
+ * is FP64 throughout).  mode 0: FP64 everywhere (default).  mode 1: the two
+ * Schur GEMMs (D^-1 F and H - K D^-1 F) on the tcgen05 tensor cores in TF32
+ * with FP32 accumulation, and the block-Jacobi preconditioner applied with FP32
+ * inverses; the element LU, the residuals (rnorm), the Arnoldi process and the
+ * Newton update stay FP64, so Newton iterations refine the solution to the
+ * FP64 residual tolerance. */
 int hfem_set_precision(hfem_ctx* ctx, int mode);
 
 /* The BILU0 ordering in use: ordered2unordered[i] = face pivoted at step i

@@ -56,3 +56,20 @@ def test_mixed_newton_reaches_fp64_tolerance(name, make):
     conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=12, gmres_tol=1e-10)
     s.close()
     assert conv == 1 and hist[-1] < 1e-10, hist
+
+
+def test_mixed_gmres_reaches_tolerance_with_fp32_preconditioner():
+    prob = ns3d_fourier(n=3, porder=2)
+    s = HDGSolver(prob)
+    s.getQ()
+    s.assembleLinearSystem()
+    c64, h64 = s.gmres(precond=2, restart=50, tol=1e-10)
+    x64 = s.download("x")
+    s.set_precision(1)
+    s.assembleLinearSystem()
+    c32, h32 = s.gmres(precond=2, restart=50, tol=1e-10)
+    x32 = s.download("x")
+    s.close()
+    assert c64 == 1 and c32 == 1
+    # the mixed system differs from the FP64 one by TF32 rounding, not by the preconditioner
+    assert rel(x32, x64) < 1e-2
