@@ -63,7 +63,7 @@ struct ElemArgs {
     const int* eprob;
     const double* pparam;
     // boundary faces (NULL bf = none): bf[e * nfe + face] < 0 is boundary -(ib + 1),
-    // condition bcm[ib] (fbou.cpp types 2, 5, 6, 7) with state bcs[ib * nch + c]
+    // condition bcm[ib] (fbou.cpp types 1, 2, 5, 6, 7) with state bcs[ib * nch + c]
     const int* bf;
     const int* bcm;
     const double* bcs;

@@ -1391,8 +1391,8 @@ int hfem_set_boundary(hfem_ctx* c, const int* bf, int nbnd, const int* bcm, cons
     if (!c->have_mesh) return fail(c, HFEM_E_STATE, "set the mesh before its boundary");
     const hfem_dims& d = c->dims;
     for (int b = 0; b < nbnd; b++)
-        if (bcm[b] != 2 && bcm[b] != 5 && bcm[b] != 6 && bcm[b] != 7)
-            return fail(c, HFEM_E_UNSUPPORTED, "boundary condition type %d (supported: 2, 5, 6, 7)", bcm[b]);
+        if (bcm[b] != 1 && bcm[b] != 2 && bcm[b] != 5 && bcm[b] != 6 && bcm[b] != 7)
+            return fail(c, HFEM_E_UNSUPPORTED, "boundary condition type %d (supported: 1, 2, 5, 6, 7)", bcm[b]);
     // a boundary face belongs to one element, an interior one to two
     std::vector<int> fsrc((size_t)d.nf * 4);
     CK(cudaMemcpy(fsrc.data(), c->face_src, sizeof(int) * fsrc.size(), cudaMemcpyDeviceToHost));

@@ -122,9 +122,81 @@ __device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, c
     }
 }
 
+template <int N>
+__device__ __forceinline__ Dual<N> dsqrt(const Dual<N>& a) {
+    Dual<N> r;
+    r.v = sqrt(a.v);
+    const double h = 0.5 / r.v;
+#pragma unroll
+    for (int i = 0; i < N; i++) r.d[i] = a.d[i] * h;
+    return r;
+}
+template <int N>
+__device__ __forceinline__ Dual<N> dabs(const Dual<N>& a) {
+    return a.v < 0.0 ? (-1.0) * a : a;
+}
+
+// Free-stream far field (application/FM/fbou.cpp:126-218):
+//   fb = (A_n + |A_n|)(u - uh) - (A_n - |A_n|)(ui - uh)
+// with the Euler normal-flux Jacobian A_n at uh and |A_n| = R |Lambda| R^-1 in the
+// closed form of application/FM/getan.c (eigenvalues un + c, un - c, un; with
+// eps > 0 the eigenvalues below eps c are smoothed as there).  Column k of
+// either matrix is lam3 e_k + cc1_k [1, v, h] + cc2_k [0, n, un]; the matrices
+// are applied column by column without being stored.
+template <int ND, int M>
+__device__ __forceinline__ void ns_farfield_dual(const double* __restrict__ param, const double* ui, const double* nl,
+                                                 const Dual<M>* w, const Dual<M>* uh, Dual<M>* fb) {
+    constexpr int NCU = ND + 2;
+    using D = Dual<M>;
+    const double gam = param[0], eps = param[1], g1 = gam - 1.0;
+    const D r = uh[0];
+    D uv[ND], af = dc<M>(0.0), un = dc<M>(0.0);
+#pragma unroll
+    for (int i = 0; i < ND; i++) {
+        uv[i] = uh[1 + i] / r;
+        af = af + 0.5 * (uv[i] * uv[i]);
+        un = un + nl[i] * uv[i];
+    }
+    const D E = uh[ND + 1] / r;
+    const D p = g1 * (uh[ND + 1] - r * af);
+    const D h = E + p / r;
+    const D c2 = gam * (p / r);
+    const D c = dsqrt(c2);
+    D la[3] = {un + c, un - c, un}, lb[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        lb[m] = dabs(la[m]);
+        if (eps > 0.0 && lb[m].v < eps * c.v) lb[m] = 0.5 * (lb[m] * lb[m] / (eps * c) + eps * c);
+    }
+    const D s1a = 0.5 * (la[0] + la[1]), s2a = 0.5 * (la[0] - la[1]);
+    const D s1b = 0.5 * (lb[0] + lb[1]), s2b = 0.5 * (lb[0] - lb[1]);
+#pragma unroll
+    for (int j = 0; j < NCU; j++) fb[j] = dc<M>(0.0);
+#pragma unroll
+    for (int k = 0; k < NCU; k++) {
+        const D a = (k == 0) ? af : (k == ND + 1 ? dc<M>(1.0) : dc<M>(0.0) - uv[k > 0 ? k - 1 : 0]);
+        const D b = (k == 0) ? dc<M>(0.0) - un : (k == ND + 1 ? dc<M>(0.0) : dc<M>(nl[k > 0 ? k - 1 : 0]));
+        const D c1a = g1 * ((s1a - la[2]) * a / c2) + s2a * b / c, c2a = g1 * (s2a * a / c) + (s1a - la[2]) * b;
+        const D c1b = g1 * ((s1b - lb[2]) * a / c2) + s2b * b / c, c2b = g1 * (s2b * a / c) + (s1b - lb[2]) * b;
+        const D du = w[k] - uh[k], di = dc<M>(ui[k]) - uh[k];
+#pragma unroll
+        for (int j = 0; j < NCU; j++) {
+            const D v1 = (j == 0) ? dc<M>(1.0) : (j == ND + 1 ? h : uv[j > 0 ? j - 1 : 0]);
+            const D v2 = (j == 0) ? dc<M>(0.0) : (j == ND + 1 ? un : dc<M>(nl[j > 0 ? j - 1 : 0]));
+            D Aa = c1a * v1 + c2a * v2, Ab = c1b * v1 + c2b * v2;
+            if (j == k) {
+                Aa = Aa + la[2];
+                Ab = Ab + lb[2];
+            }
+            fb[j] = fb[j] + (Aa + Ab) * du - (Aa - Ab) * di;
+        }
+    }
+}
+
 // Boundary flux fb(u, q, uh) of the NS boundary conditions at one point
 // (application/FM/fbou.cpp on a fixed mesh), in dual numbers so that one pass
 // per differentiated variable gives fb and its derivative:
+//   1 free-stream far field (ns_farfield_dual);
 //   2 no-slip adiabatic wall: rho - rho_hat, -m_hat, and for energy the
 //     interior trace flux F(uh, q).n + tau (E - E_hat);
 //   5 Dirichlet: tau (ui - uh);   6 extrapolation: u - uh;
@@ -136,6 +208,10 @@ __device__ __forceinline__ bool ns_fbou_dual(int bn, const double* __restrict__ 
                                              const double* nl, const Dual<M>* w, const Dual<M>* uh, Dual<M>* fb) {
     constexpr int NCU = ND + 2, NC = NCU * (ND + 1);
     const double tau = param[5];
+    if (bn == 1) {
+        ns_farfield_dual<ND, M>(param, ui, nl, w, uh, fb);
+        return true;
+    }
     if (bn == 2) {
         fb[0] = w[0] - uh[0];
 #pragma unroll

@@ -70,8 +70,9 @@ int hfem_set_mesh(hfem_ctx* ctx, const double* dgnodes, const int* elcon, const 
 /* Boundary faces of a bounded mesh (mesh.bf, app.bcm, app.bcs of the
  * reference; faceint elementassembly.cpp:1075-1246 with fbouDriver): bf[ne x
  * nfe] element-major, >= 0 interior, -(ib + 1) on boundary ib; bcm[nbnd] the
- * boundary condition types (2 no-slip adiabatic wall, 5 Dirichlet, 6
- * extrapolation, 7 slip wall, as application/FM/fbou.cpp on a fixed mesh);
+ * boundary condition types (1 free-stream far field, 2 no-slip adiabatic
+ * wall, 5 Dirichlet, 6 extrapolation, 7 slip wall, as
+ * application/FM/fbou.cpp on a fixed mesh);
  * bcs[nbnd x nch] their states.  The trace equations of boundary faces take
  * the boundary flux.  Call after hfem_set_mesh (which clears it). */
 int hfem_set_boundary(hfem_ctx* ctx, const int* bf, int nbnd, const int* bcm, const double* bcs);

@@ -116,6 +116,54 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
     }
 }
 
+static Dual dsqrt(const Dual& a) {
+    Dual r; r.n = a.n; r.v = std::sqrt(a.v);
+    for (int i = 0; i < a.n; i++) r.d[i] = 0.5 * a.d[i] / r.v;
+    return r;
+}
+static Dual dabs(const Dual& a) { return a.v < 0 ? (-1.0) * a : a; }
+
+// Normal flux Jacobian A_n of the Euler part at the trace state uh (absflag 0)
+// or |A_n| = R |Lambda| R^-1 (absflag 1), closed form of application/FM/getan.c
+// (eigenvalues un + c, un - c, un; with eps > 0 the small eigenvalues are
+// smoothed as there).  M[j + ncu*k]: row j, column k.
+static void normal_jacobian(int absflag, int nd, const double* param, const Dual* uh, const double* nl, Dual* M) {
+    const int ncu = nd + 2, n = uh[0].n;
+    const double gam = param[0], eps = param[1], g1 = gam - 1.0;
+    const Dual r = uh[0];
+    Dual uv[3], af = dconst(0.0, n), un = dconst(0.0, n);
+    for (int i = 0; i < nd; i++) {
+        uv[i] = uh[1 + i] / r;
+        af = af + 0.5 * (uv[i] * uv[i]);
+        un = un + nl[i] * uv[i];
+    }
+    const Dual E = uh[nd + 1] / r;
+    const Dual p = g1 * (uh[nd + 1] - r * af);
+    const Dual h = E + p / r;
+    const Dual c2 = gam * (p / r);
+    const Dual c = dsqrt(c2);
+    Dual lam[3] = {un + c, un - c, un};
+    if (absflag)
+        for (int m = 0; m < 3; m++) {
+            lam[m] = dabs(lam[m]);
+            if (eps > 0 && lam[m].v < eps * c.v) lam[m] = 0.5 * (lam[m] * lam[m] / (eps * c) + eps * c);
+        }
+    const Dual s1 = 0.5 * (lam[0] + lam[1]), s2 = 0.5 * (lam[0] - lam[1]), l3 = lam[2];
+    for (int k = 0; k < ncu; k++) {
+        const Dual a = (k == 0) ? af : (k == nd + 1 ? dconst(1.0, n) : dconst(0.0, n) - uv[k - 1]);
+        const Dual b = (k == 0) ? dconst(0.0, n) - un : (k == nd + 1 ? dconst(0.0, n) : dconst(nl[k - 1], n));
+        const Dual cc1 = g1 * ((s1 - l3) * a / c2) + s2 * b / c;
+        const Dual cc2 = g1 * (s2 * a / c) + (s1 - l3) * b;
+        for (int j = 0; j < ncu; j++) {
+            Dual v1 = (j == 0) ? dconst(1.0, n) : (j == nd + 1 ? h : uv[j - 1]);
+            Dual v2 = (j == 0) ? dconst(0.0, n) : (j == nd + 1 ? un : dconst(nl[j - 1], n));
+            Dual m = cc1 * v1 + cc2 * v2;
+            if (j == k) m = m + l3;
+            M[j + ncu * k] = m;
+        }
+    }
+}
+
 // Boundary flux fb(u, q, uh) of the NS boundary conditions (application/FM/fbou.cpp)
 // at one point, with its Jacobians fb_u[j + nch*k] (k over u and q) and
 // fb_uh[j + nch*k], by forward differentiation over (u, q, uh):
@@ -126,6 +174,8 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
 //   6 extrapolation (fbou.cpp:584-600): u - uh;
 //   7 slip wall (fbou.cpp:601-652, fixed mesh): rho - rho_hat,
 //     m - (m.n) n - m_hat, E - E_hat.
+//   1 free-stream far field (fbou.cpp:126-218): characteristic upwinding
+//     (A_n + |A_n|)(u - uh) - (A_n - |A_n|)(ui - uh), A_n at uh (getan.c);
 // Returns nonzero for a type that is not restated.
 static int fbou_point(int bn, int nd, const double* param, const double* ui, const double* nl, const double* w,
                       const double* uh, double* fb, double* fb_u, double* fb_uh) {
@@ -134,7 +184,18 @@ static int fbou_point(int bn, int nd, const double* param, const double* ui, con
     std::vector<Dual> W(nc), U(nch), F(nch), fl(ncu * nd);
     for (int k = 0; k < nc; k++) W[k] = dvar(w[k], nv, k);
     for (int k = 0; k < nch; k++) U[k] = dvar(uh[k], nv, nc + k);
-    if (bn == 2) {
+    if (bn == 1) {      // free-stream far field (fbou.cpp:126-218): (A_n + |A_n|)(u - uh) - (A_n - |A_n|)(ui - uh)
+        std::vector<Dual> An(ncu * ncu), Aa(ncu * ncu);
+        normal_jacobian(0, nd, param, U.data(), nl, An.data());
+        normal_jacobian(1, nd, param, U.data(), nl, Aa.data());
+        for (int j = 0; j < ncu; j++) {
+            Dual t = dconst(0.0, nv);
+            for (int k = 0; k < ncu; k++)
+                t = t + (An[j + ncu * k] + Aa[j + ncu * k]) * (W[k] - U[k]) -
+                    (An[j + ncu * k] - Aa[j + ncu * k]) * (dconst(ui[k], nv) - U[k]);
+            F[j] = t;
+        }
+    } else if (bn == 2) {
         F[0] = W[0] - U[0];
         for (int j = 0; j < nd; j++) F[1 + j] = dconst(0.0, nv) - U[1 + j];
         std::vector<Dual> wf(nc);

@@ -36,7 +36,7 @@ class OracleProblem(C.Structure):
     ]
 
 # boundary condition types restated in hfem_oracle.cpp (fbou_point)
-BC_TYPES = (2, 5, 6, 7)
+BC_TYPES = (1, 2, 5, 6, 7)
 
 
 _lib = None

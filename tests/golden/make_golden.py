@@ -34,6 +34,7 @@ CASES = {
     # bounded meshes: Dirichlet, extrapolation, slip and no-slip adiabatic walls
     "ns2d_channel_p2_n3": lambda: ns2d_channel(n=3, porder=2),
     "ns3d_box_p1_n2": lambda: ns3d_box(n=2, porder=1),
+    "ns2d_farfield_p2_n3": lambda: ns2d_channel(n=3, porder=2, bcm=(1, 1, 1, 1)),
 }
 FULL_LIMIT = 400_000          # store arrays up to this many entries in full
 

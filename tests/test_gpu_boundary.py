@@ -2,8 +2,8 @@
 to the reference's fbou.cpp by the golden fixtures).
 
 * Element blocks, Hg, Rg, Rr, DinvF within 1e-12 relative, rnorm 1e-12, for
-  2D p1-p3 and 3D p1-p2 with Dirichlet, extrapolation, slip and no-slip
-  adiabatic walls.
+  2D p1-p3 and 3D p1-p2 with free-stream far field, Dirichlet, extrapolation,
+  slip and no-slip adiabatic walls.
 * Newton on a bounded channel converges to 1e-10; packed with a periodic
   problem, a bounded problem assembles as it does alone.
 """
@@ -23,6 +23,8 @@ CASES = [
     ("2d_p3", lambda: ns2d_channel(n=3, porder=3)),
     ("3d_p1", lambda: ns3d_box(n=2, porder=1)),
     ("3d_p2", lambda: ns3d_box(n=2, porder=2)),
+    ("2d_p2_farfield", lambda: ns2d_channel(n=4, porder=2, bcm=(1, 1, 1, 1))),
+    ("3d_p1_farfield", lambda: ns3d_box(n=2, porder=1, bcm=(1, 1, 2, 7, 1, 5))),
 ]
 
 

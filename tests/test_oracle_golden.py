@@ -24,6 +24,7 @@ CASES = {
     "ns3d_p3_n3": lambda: ns3d_fourier(n=3, porder=3),
     "ns2d_channel_p2_n3": lambda: ns2d_channel(n=3, porder=2),
     "ns3d_box_p1_n2": lambda: ns3d_box(n=2, porder=1),
+    "ns2d_farfield_p2_n3": lambda: ns2d_channel(n=3, porder=2, bcm=(1, 1, 1, 1)),
 }
 
 
