@@ -730,29 +730,8 @@ struct ScatterArgs {
     double *Hg, *Rg, *Rr;
 };
 
-__global__ void scatter_H_kernel(ScatterArgs A) {
-    const int bsz = A.npf * A.nch, ndf = A.npf * A.nfe;
-    const long long total = (long long)A.nblk * bsz * bsz;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t / (bsz * bsz));
-        const int w = (int)(t % (bsz * bsz));
-        const int colpos = w / bsz, rowpos = w % bsz;     // Hg block column-major: rowpos fastest
-        const int m1 = colpos / A.nch, n1 = colpos % A.nch, m2 = rowpos / A.nch, n2 = rowpos % A.nch;
-        const int i = A.rowface[k], j = A.colface[k];
-        double s = 0.0;
-        for (int c = 0; c < 2; c++) {
-            const int e = A.blk_src[(k * 2 + c) * 3 + 0];
-            if (e < 0) break;
-            const int a = A.blk_src[(k * 2 + c) * 3 + 1], b = A.blk_src[(k * 2 + c) * 3 + 2];
-            const int ind = A.elcon[(size_t)e * ndf + a * A.npf + m2] - i * A.npf;
-            const int jnd = A.elcon[(size_t)e * ndf + b * A.npf + m1] - j * A.npf;
-            s += A.H[(size_t)e * A.nb * A.nb + (a * bsz + ind * A.nch + n2) + (size_t)A.nb * (b * bsz + jnd * A.nch + n1)];
-        }
-        A.Hg[t] = s;
-    }
-}
-
-// The same owner-gather with one warp per Hg block and the face shape known
+// Scatter of the condensed blocks into Hg (mapElement2LinearSystem,
+// globalassembly.cpp:40-89) as an owner-gather, one warp per Hg block, face shape known
 // at compile time: the warp first resolves, for each (at most two)
 // contributing element, the offsets of the block's rows and columns inside
 // that element's H (elcon gives the permutation of the face nodes), then
@@ -849,24 +828,6 @@ __global__ void rnorm_final_kernel(int n, const double* __restrict__ part, doubl
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int i = 0; i < n; i++) t += part[i];
-        *out = sqrt(t);
-    }
-}
-
-// sqrt(sum ru2 + sum Rr^2), one CTA, fixed summation order.
-__global__ void rnorm_kernel(int ne, const double* ru2, int nr, const double* rr, double* out) {
-    __shared__ double red[32];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < ne; i += blockDim.x) s += ru2[i];
-    double s2 = 0.0;
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) s2 += rr[i] * rr[i];
-    s += s2;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
         *out = sqrt(t);
     }
 }

@@ -236,6 +236,7 @@ struct hfem_ctx {
     unsigned char* seg_act = nullptr;
     int* seg_k = nullptr;
     int seg_restart = 0;
+    bool seg_single = false;    // segment tables describe one segment over the whole vector
     // BILU0: ordering (computed once, from the first system), level schedule, factors
     bool have_order = false;
     std::vector<int> h_o2u, h_u2o, lvl_lo, lvl_up;
@@ -801,8 +802,14 @@ int ensure_krylov(hfem_ctx* c, int restart) {
     return 0;
 }
 
+int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters,
+                   double* hist, int hist_len);
+
 int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters, double* hist,
                int hist_len) {
+    // one problem, block Jacobi or none: the fused single-segment kernels
+    if (c->nprob == 0 && precond != 0 && c->assembled)
+        return gmres_seg_impl(c, precond, restart, tol, maxit, conv, iters, hist, hist_len);
     int rc;
     if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before gmres");
     if (restart < 1 || maxit < 1 || !(tol > 0.0)) return fail(c, HFEM_E_ARG, "restart, maxit and tol must be positive");
@@ -949,15 +956,47 @@ int matvec_warp(hfem_ctx* c, const double* x, double* z, bool prec, const unsign
 // vectors), Hessenberg matrix, Givens rotations and stopping test, so it takes
 // exactly the iterations it takes alone; the launches are shared, and a
 // problem that has stopped is skipped by every kernel.
-int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters) {
+// Segment tables for one segment over the whole trace vector (GMRES of a
+// context without a problem map runs on the same fused kernels).
+int ensure_single_segment(hfem_ctx* c) {
+    if (c->seg_single) return 0;
+    const long long ntot = (long long)c->dims.nf * c->bsz;
+    long long piece = 1024;
+    while (piece < SEG_PIECE && piece * 4 * sms(c->device) < ntot) piece *= 2;
+    std::vector<long long> pstart;
+    std::vector<int> pseg;
+    for (long long s = 0; s < ntot; s += piece) {
+        pstart.push_back(s);
+        pseg.push_back(0);
+    }
+    pstart.push_back(ntot);
+    const int p0[2] = {0, (int)pseg.size()};
+    int rc;
+    if ((rc = upload(c, &c->seg_pstart, pstart.data(), pstart.size())) ||
+        (rc = upload(c, &c->seg_pseg, pseg.data(), pseg.size())) || (rc = upload(c, &c->seg_p0, p0, 2)) ||
+        (rc = dalloc(c, &c->seg_ticket, 1)) || (rc = dalloc(c, &c->seg_part, pseg.size())) ||
+        (rc = dalloc(c, &c->seg_nrm, 2)) || (rc = dalloc(c, &c->seg_act, 1)) || (rc = dalloc(c, &c->seg_k, 1)))
+        return rc;
+    CK(cudaMemsetAsync(c->seg_ticket, 0, sizeof(int), c->stream));
+    c->npieces = (int)pseg.size();
+    c->seg_restart = 0;
+    c->seg_single = true;
+    return 0;
+}
+
+int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters,
+                   double* hist = nullptr, int hist_len = 0) {
     int rc;
     if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before gmres");
-    if (!c->nprob || !c->npieces)
+    const bool single = c->nprob == 0;
+    if (single && (rc = ensure_single_segment(c))) return rc;
+    if (!single && (!c->npieces || c->seg_single))
         return fail(c, HFEM_E_STATE, "per-problem GMRES needs a problem map with each problem's faces contiguous");
     if (restart < 1 || maxit < 1 || !(tol > 0.0)) return fail(c, HFEM_E_ARG, "restart, maxit and tol must be positive");
     if (precond != -1 && precond != 2) return fail(c, HFEM_E_ARG, "precond must be -1 (none) or 2 (block Jacobi)");
     if ((rc = ensure_krylov(c, restart))) return rc;
-    const int P = c->nprob;
+    const int P = single ? 1 : c->nprob;
+    const unsigned char* mv_act = single ? nullptr : c->seg_act;   // row -> problem map only with a problem map
     if (c->seg_restart < restart) {
         if ((rc = dalloc(c, &c->seg_h, (size_t)(restart + 2) * P))) return rc;
         if ((rc = dalloc(c, &c->seg_y, (size_t)restart * P))) return rc;
@@ -1018,7 +1057,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
         if (!running) break;
         if ((rc = set_act())) return rc;
         // r = M^-1 b - M^-1 A x, beta = |r| per problem
-        if ((rc = matvec_warp(c, c->x, c->w, prec, c->seg_act))) return rc;
+        if ((rc = matvec_warp(c, c->x, c->w, prec, mv_act))) return rc;
         seg_sub_from_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, c->pb, c->w);
         axpy_dot(nullptr, nullptr, c->w, c->w, c->seg_nrm, 1);
         CK(cudaMemcpyAsync(beta.data(), c->seg_nrm, sizeof(double) * P, cudaMemcpyDeviceToHost, c->stream));
@@ -1041,7 +1080,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
         for (int j = 0; j < restart && live; j++) {
             double* vj = c->V + (size_t)j * n;
             double* vn = c->V + (size_t)(j + 1) * n;
-            if ((rc = matvec_warp(c, vj, vn, prec, c->seg_act))) return rc;
+            if ((rc = matvec_warp(c, vj, vn, prec, mv_act))) return rc;
             {
                 Timed t(c, "orthogonalise_seg");
                 for (int i = 0; i <= j; i++)
@@ -1079,6 +1118,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
                 its[p]++;
                 jc[p] = j + 1;
                 const double res = std::fabs(gp[j + 1]);
+                if (p == 0 && hist && its[0] - 1 < hist_len) hist[its[0] - 1] = res / nrmb[0];
                 int stop = 2;
                 if (res / nrmb[p] <= tol) stop = 1;
                 else if (its[p] >= maxit) stop = 0;
@@ -1630,6 +1670,7 @@ int hfem_set_problem_map(hfem_ctx* c, int nprob, const int* eprob, const int* fp
     // every problem owns a face, problem p's slice of the trace vector is one
     // contiguous segment, cut into pieces of <= SEG_PIECE entries.
     c->npieces = 0;
+    c->seg_single = false;
     bool sorted = true;
     std::vector<int> fcount(nprob, 0);
     for (int f = 0; f < d.nf; f++) {
