@@ -75,8 +75,11 @@ class BatchSolver:
 
     def __init__(self, probs: list, device: int = 0, stream: int | None = None):
         self.probs = probs
+        t0 = time.perf_counter()
         self.union, self.eprob, self.fprob, self.params, self.eoff, self.hoff = union_problem(probs)
+        t1 = time.perf_counter()
         self.s = HDGSolver(self.union, device=device)
+        self.build_times = {"repack_union": t1 - t0, "repack_context": time.perf_counter() - t1}
         if stream is not None:
             self.s.set_stream(stream)
         lib = load_library()

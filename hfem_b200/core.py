@@ -22,7 +22,7 @@ _ip = C.POINTER(C.c_int)
 ERRORS = {-1: "invalid argument", -2: "unsupported element", -3: "CUDA error", -4: "bad call order",
           -5: "inconsistent mesh", -6: "singular matrix", -7: "out of device memory"}
 
-DOWNLOAD = {"Hg": 0, "Rg": 1, "Rr": 2, "DinvRu": 3, "DinvF": 4, "H": 5, "Rh": 6, "x": 7}
+DOWNLOAD = {"Hg": 0, "Rg": 1, "Rr": 2, "DinvRu": 3, "DinvF": 4, "H": 5, "Rh": 6, "x": 7, "udg": 8, "uh": 9}
 
 
 class HfemError(RuntimeError):

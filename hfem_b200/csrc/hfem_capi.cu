@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <queue>
 #include <string>
 #include <vector>
@@ -266,14 +267,111 @@ int fail(hfem_ctx* c, int code, const char* fmt, ...) {
         if (e_ != cudaSuccess) return fail(c, HFEM_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// Device memory of contexts comes from a per-process pool of size-class
+// blocks: the buffers of a destroyed context are kept and handed to the next
+// context that asks for the same class, so building and dropping contexts
+// (the serving loop repacks them at iteration boundaries) does not pay
+// cudaMalloc / cudaFree, each of which synchronises the device.  A block is
+// returned to the pool only after its context's stream is idle.
+// hfem_pool_trim gives the cached blocks back to the driver; a failed
+// cudaMalloc trims and retries once.
+struct DevicePool {
+    std::mutex m;
+    std::map<std::pair<int, size_t>, std::vector<void*>> free;   // (device, class) -> idle blocks
+    std::map<void*, std::pair<int, size_t>> live;                // block -> (device, class)
+    size_t cached = 0;
+};
+
+DevicePool& pool() {
+    static DevicePool* p = new DevicePool();        // outlives every context (never destroyed)
+    return *p;
+}
+
+size_t size_class(size_t bytes) {
+    if (bytes <= 256) return 256;
+    if (bytes <= (1u << 20)) {
+        size_t s = 256;
+        while (s < bytes) s <<= 1;
+        return s;
+    }
+    const size_t step = 2u << 20;
+    return (bytes + step - 1) / step * step;
+}
+
+size_t pool_trim_device(int device) {
+    DevicePool& P = pool();
+    std::vector<void*> drop;
+    {
+        std::lock_guard<std::mutex> g(P.m);
+        for (auto it = P.free.begin(); it != P.free.end();) {
+            if (device < 0 || it->first.first == device) {
+                for (void* q : it->second) drop.push_back(q);
+                P.cached -= it->first.second * it->second.size();
+                it = P.free.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    for (void* q : drop) cudaFree(q);
+    return drop.size();
+}
+
+cudaError_t pool_alloc(int device, void** p, size_t bytes) {
+    DevicePool& P = pool();
+    const size_t cls = size_class(bytes);
+    {
+        std::lock_guard<std::mutex> g(P.m);
+        auto it = P.free.find({device, cls});
+        if (it != P.free.end() && !it->second.empty()) {
+            *p = it->second.back();
+            it->second.pop_back();
+            P.cached -= cls;
+            P.live[*p] = {device, cls};
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, cls);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        pool_trim_device(device);
+        e = cudaMalloc(p, cls);
+    }
+    if (e == cudaSuccess) {
+        std::lock_guard<std::mutex> g(P.m);
+        P.live[*p] = {device, cls};
+    }
+    return e;
+}
+
+void pool_free(void* p) {
+    if (!p) return;
+    DevicePool& P = pool();
+    {
+        std::lock_guard<std::mutex> g(P.m);
+        auto it = P.live.find(p);
+        if (it != P.live.end()) {
+            P.free[it->second].push_back(p);
+            P.cached += it->second.second;
+            P.live.erase(it);
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
 template <class T>
 int dalloc(hfem_ctx* c, T** p, size_t count) {
-    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (*p) {
+        cudaStreamSynchronize(c->stream);          // the old block may still be read by queued work
+        pool_free(*p);
+        *p = nullptr;
+    }
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    cudaError_t e = pool_alloc(c->device, (void**)p, sizeof(T) * count);
     if (e != cudaSuccess) {
         *p = nullptr;
-        return fail(c, HFEM_E_NOMEM, "cudaMalloc of %zu bytes: %s", sizeof(T) * count, cudaGetErrorString(e));
+        return fail(c, HFEM_E_NOMEM, "device allocation of %zu bytes: %s", sizeof(T) * count, cudaGetErrorString(e));
     }
     return 0;
 }
@@ -1293,7 +1391,7 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.inv_fn, L.inv_threads, 0);
     c->grid_inv = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
-    if (cudaMalloc(&c->rnorm, sizeof(double)) != cudaSuccess) {
+    if (pool_alloc(device, (void**)&c->rnorm, sizeof(double)) != cudaSuccess) {
         cudaStreamDestroy(c->own);
         delete c;
         return HFEM_E_NOMEM;
@@ -1321,7 +1419,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
                     c->d_lvl_lo, c->d_lvl_up};
     for (void* p : ptrs)
-        if (p) cudaFree(p);
+        if (p) pool_free(p);
     for (auto& p : c->timer.pending) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -1421,7 +1519,7 @@ int hfem_set_mesh(hfem_ctx* c, const double* dgnodes, const int* elcon, const in
     c->h_rowstart.assign(rowstart, rowstart + nf + 1);
     c->h_colidx.assign(colidx, colidx + nblk);
     c->have_order = false;
-    if (c->bf) { cudaFree(c->bf); c->bf = nullptr; }       // boundary flags belong to the old mesh
+    if (c->bf) { pool_free(c->bf); c->bf = nullptr; }      // boundary flags belong to the old mesh
     c->have_mesh = true;
     return 0;
 }
@@ -1454,7 +1552,7 @@ int hfem_set_boundary(hfem_ctx* c, const int* bf, int nbnd, const int* bcm, cons
     int rc;
     CK(cudaSetDevice(c->device));
     if (!any) {
-        if (c->bf) { cudaFree(c->bf); c->bf = nullptr; }
+        if (c->bf) { pool_free(c->bf); c->bf = nullptr; }
         c->nbnd = 0;
         return 0;
     }
@@ -1918,6 +2016,13 @@ int hfem_reset_ordering(hfem_ctx* c) {
     return 0;
 }
 
+int hfem_pool_trim(void) { return (int)pool_trim_device(-1); }
+
+long long hfem_pool_cached_bytes(void) {
+    std::lock_guard<std::mutex> g(pool().m);
+    return (long long)pool().cached;
+}
+
 int hfem_set_precision(hfem_ctx* c, int mode) {
     if (!c) return HFEM_E_ARG;
     if (mode != 0 && mode != 1) return fail(c, HFEM_E_ARG, "precision mode must be 0 (FP64) or 1 (TF32 Schur)");
@@ -1942,6 +2047,8 @@ int device_buffer(hfem_ctx* c, int what, const double** src, size_t* need) {
         case 5: *src = c->H; *need = (size_t)d.ne * c->nb * c->nb; break;
         case 6: *src = c->Rh; *need = (size_t)d.ne * c->nb; break;
         case 7: *src = c->x; *need = (size_t)d.nf * c->bsz; break;
+        case 8: *src = c->udg; *need = (size_t)d.ne * d.npv * c->nc; break;
+        case 9: *src = c->uh; *need = (size_t)d.nf * d.npf * c->nch; break;
         default: return fail(c, HFEM_E_ARG, "unknown buffer %d", what);
     }
     if (!*src) return fail(c, HFEM_E_STATE, "nothing computed for buffer %d yet", what);

@@ -140,33 +140,57 @@ class _Group:
         dead = sum(r.prob.mesh.ne for r in self.members if not r.live)
         return dead / tot if tot else 0.0
 
-    def repack(self, device, stream):
+    def repack(self, device, stream, phases=None, on_device=True):
         """Rebuild the context from the live members plus the joining
         requests; returns the device bytes of the retired members it drops."""
         keep = self.live()
         freed = sum(footprint_bytes(r.prob) for r in self.members if not r.live)
-        if self.solver is not None:
-            if keep:
-                udg, uh = self.solver.s.get_solution()
-                for i, r in enumerate(self.members):
-                    if r.live:
-                        e0, e1 = self.solver.eoff[i], self.solver.eoff[i + 1]
-                        h0, h1 = self.solver.hoff[i], self.solver.hoff[i + 1]
-                        r.cur = replace(r.cur, udg=udg[e0:e1].copy(), uh=uh[h0:h1].copy())
-            self.solver.close()
-            self.solver = None
+        t0 = time.perf_counter()
+        old = self.solver
+        old_pos = {id(r): i for i, r in enumerate(self.members)}
+        if old is not None and keep and not on_device:
+            udg, uh = old.s.get_solution()
+            for r in keep:
+                i = old_pos[id(r)]
+                r.cur = replace(r.cur, udg=udg[old.eoff[i]:old.eoff[i + 1]].copy(),
+                                uh=uh[old.hoff[i]:old.hoff[i + 1]].copy())
+        t1 = time.perf_counter()
         self.members = keep + self.joining
         self.joining = []
+        self.solver = None
         if self.members:
+            # in-flight requests start from their packed state on the host side
+            # and get their current state by device-to-device copies below
             self.solver = BatchSolver([r.cur for r in self.members], device=device, stream=stream)
+            if old is not None and keep and on_device:
+                import torch
+                src_u, src_h = old.s.device_tensor("udg"), old.s.device_tensor("uh")
+                dst_u, dst_h = self.solver.s.device_tensor("udg"), self.solver.s.device_tensor("uh")
+                su = src_u.numel() // old.eoff[-1]
+                sh = src_h.numel() // old.hoff[-1]
+                for j, r in enumerate(keep):
+                    i = old_pos[id(r)]
+                    e0, e1, n0 = old.eoff[i], old.eoff[i + 1], self.solver.eoff[j]
+                    h0, h1, m0 = old.hoff[i], old.hoff[i + 1], self.solver.hoff[j]
+                    dst_u[n0 * su:(n0 + e1 - e0) * su].copy_(src_u[e0 * su:e1 * su])
+                    dst_h[m0 * sh:(m0 + h1 - h0) * sh].copy_(src_h[h0 * sh:h1 * sh])
+                torch.cuda.synchronize(device)
             # q of joining requests from their (u, uhat); in-flight ones already
             # satisfy q = getQ(u, uhat), so recomputing them is a no-op up to rounding
             self.solver.s.getQ()
+        if old is not None:
+            old.close()
+        if phases is not None:
+            phases["repack_readback"] = phases.get("repack_readback", 0.0) + (t1 - t0)
+            phases["repack_build"] = phases.get("repack_build", 0.0) + (time.perf_counter() - t1)
+            if self.solver is not None:
+                for k, v in self.solver.build_times.items():
+                    phases[k] = phases.get(k, 0.0) + v
         return freed
 
 
 def serve(requests, tol=1e-10, hbm_budget=None, max_newton=20, device=0, clock=time.perf_counter,
-          keep_states=False, stream=None, repack_fraction=0.5, gmres_tol=1e-10, restart=50):
+          keep_states=False, stream=None, repack_fraction=0.5, gmres_tol=1e-10, restart=50, repack_on_device=True):
     """Continuous batching over `requests` (sorted by arrival); returns ServeStats."""
     if hbm_budget is None:
         import torch
@@ -203,7 +227,7 @@ def serve(requests, tol=1e-10, hbm_budget=None, max_newton=20, device=0, clock=t
                 tr = time.perf_counter()
                 if g.solver is not None:
                     _merge(phases, g.solver.phases)
-                used -= g.repack(device, stream)
+                used -= g.repack(device, stream, phases, repack_on_device)
                 phases["repack"] += time.perf_counter() - tr
             b = g.solver
             active = np.array([r.live for r in g.members])
@@ -220,15 +244,20 @@ def serve(requests, tol=1e-10, hbm_budget=None, max_newton=20, device=0, clock=t
                     finished.append(i)
             if finished:
                 tr = time.perf_counter()
-                udg, uh = b.s.get_solution()             # results go back to the host
+                # each finished request's result goes back to the host (its slice only)
+                du, dh = b.s.device_tensor("udg"), b.s.device_tensor("uh")
+                su, sh = du.numel() // b.eoff[-1], dh.numel() // b.hoff[-1]
+                for i in finished:
+                    r = g.members[i]
+                    u = du[b.eoff[i] * su:b.eoff[i + 1] * su].cpu().numpy()
+                    h = dh[b.hoff[i] * sh:b.hoff[i + 1] * sh].cpu().numpy()
+                    r.udg = u.reshape(r.prob.udg.shape) if keep_states else None
+                    r.uh = h.reshape(r.prob.uh.shape) if keep_states else None
                 tnow = clock() - t0
                 for i in finished:
                     r = g.members[i]
                     r.live = False
                     r.finish = tnow
-                    if keep_states:
-                        r.udg = udg[b.eoff[i]:b.eoff[i + 1]].copy()
-                        r.uh = uh[b.hoff[i]:b.hoff[i + 1]].copy()
                     done.append(r)
                 if not g.live():
                     used -= sum(footprint_bytes(r.prob) for r in g.members)

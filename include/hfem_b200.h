@@ -153,8 +153,18 @@ int hfem_set_precision(hfem_ctx* ctx, int mode);
 int hfem_get_ordering(hfem_ctx* ctx, int* ordered2unordered);
 int hfem_reset_ordering(hfem_ctx* ctx);
 
+/* Device memory of contexts is drawn from a per-process pool of size-class
+ * blocks; a destroyed context's blocks stay cached for the next context (no
+ * cudaMalloc/cudaFree, which synchronise the device, when contexts are built
+ * and dropped repeatedly).  hfem_pool_trim frees the cached blocks and returns
+ * how many; hfem_pool_cached_bytes reports their total.  No counterpart in
+ * the reference. */
+int hfem_pool_trim(void);
+long long hfem_pool_cached_bytes(void);
+
 /* Device address and length (doubles) of one of the context's buffers, with
- * the ids of hfem_download, for zero-copy use on the device after the
+ * the ids of hfem_download plus 8 = UDG and 9 = UH (the resident state, which
+ * a caller may also write), for zero-copy use on the device after the
  * context's stream has been synchronised (done here).  The buffer belongs to
  * the context and moves when the context reallocates it.  No counterpart in
  * the reference (its arrays live in host structs). */
