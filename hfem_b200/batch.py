@@ -33,6 +33,8 @@ def union_problem(probs: list) -> tuple:
     for p in probs:
         if (p.master.nd, p.master.porder, p.master.ngv) != (m.nd, m.porder, m.ngv):
             raise ValueError("all problems in a union must share the master element")
+        if getattr(p, "appname", 1) != getattr(probs[0], "appname", 1):
+            raise ValueError("all problems in a union must solve the same equations")
     npf = m.npf
     eoff = np.cumsum([0] + [p.mesh.ne for p in probs])
     foff = np.cumsum([0] + [p.mesh.nf for p in probs])

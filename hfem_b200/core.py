@@ -52,6 +52,7 @@ def load_library(path: str = LIB):
     lib.hfem_set_master.argtypes = [C.c_void_p] + [_dp] * 6 + [_ip]
     lib.hfem_set_mesh.argtypes = [C.c_void_p, _dp, _ip, _ip, _ip, _ip]
     lib.hfem_set_boundary.argtypes = [C.c_void_p, _ip, C.c_int, _ip, _dp]
+    lib.hfem_set_app.argtypes = [C.c_void_p, C.c_int]
     lib.hfem_set_physics.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_double]
     lib.hfem_set_solution.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.hfem_set_solution_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -104,6 +105,7 @@ class HDGSolver:
         perm = np.ascontiguousarray(m.perm, dtype=np.int32)
         self._chk(self.lib.hfem_set_master(self.h, *[_d(k) for k in keep], _i(perm)), "set_master")
         self.set_mesh(me)
+        self._chk(self.lib.hfem_set_app(self.h, int(getattr(prob, "appname", 1))), "set_app")
         if getattr(prob, "bcm", None) is not None:
             self.set_boundary(me.bf, prob.bcm, prob.bcs)
         self.set_physics(prob.param, prob.tdep, prob.fc_u, prob.fc_q, prob.time)

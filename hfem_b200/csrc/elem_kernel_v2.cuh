@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 w[c].v = val;
                 w[c].d[0] = (c == k) ? 1.0 : 0.0;
             }
-            ns_flux_dual<ND>(P, w, f);
+            ns_flux_dual<ND>(P, w, f, !A.inviscid);
             if (vol) {
                 const double jg = sm.jac[g];
 #pragma unroll
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
 #pragma unroll
                 for (int d = 0; d < ND; d++) nlq[d] = sm.nl[gg + NA * d];
                 const int ib = -bfe[fc] - 1;
-                if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb)) {
+                if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb, !A.inviscid)) {
                     for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
                 }
                 const double jf = sm.jacf[gg];

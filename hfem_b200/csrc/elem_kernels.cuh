@@ -67,6 +67,7 @@ struct ElemArgs {
     const int* bf;
     const int* bcm;
     const double* bcs;
+    int inviscid;               // 1: Euler flux (app.appname 0)
 };
 
 constexpr int NT = 256;         // threads per CTA for element kernels

@@ -197,6 +197,7 @@ struct hfem_ctx {
     int *bf = nullptr, *bcm = nullptr;
     double* bcs = nullptr;
     int nbnd = 0;
+    int appname = 1;            // app.appname: 1 Navier-Stokes, 0 Euler
     int* tc_err = nullptr;
     double* rn_part = nullptr;
     // master tables
@@ -452,6 +453,7 @@ int ensure_assembly_buffers(hfem_ctx* c) {
 
 ElemArgs elem_args(hfem_ctx* c) {
     ElemArgs a;
+    a.inviscid = c->appname == 0;
     a.bf = c->bf;
     a.bcm = c->bcm;
     a.bcs = c->bcs;
@@ -1565,6 +1567,15 @@ int hfem_set_boundary(hfem_ctx* c, const int* bf, int nbnd, const int* bcm, cons
     return 0;
 }
 
+int hfem_set_app(hfem_ctx* c, int appname) {
+    if (!c) return HFEM_E_ARG;
+    if (appname != 0 && appname != 1)
+        return fail(c, HFEM_E_UNSUPPORTED, "appname %d (supported: 0 Euler, 1 Navier-Stokes)", appname);
+    c->appname = appname;
+    c->assembled = false;
+    return 0;
+}
+
 int hfem_set_physics(hfem_ctx* c, const double* param, int tdep, double fc_u, double fc_q, double time) {
     if (!c || !param) return HFEM_E_ARG;
     if (!(param[0] > 1.0) || !(param[2] > 0.0) || !(param[3] > 0.0))
@@ -2233,6 +2244,7 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.bf = nullptr;
     a.bcm = nullptr;
     a.bcs = nullptr;
+    a.inviscid = 0;
     L->element(dim3(ge), L->elem_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     SchurArgs s{d.ne, D, DinvF, K, H, DinvRu, Rh, info};

@@ -75,8 +75,11 @@ __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, const Dual<N>& b)
 
 // f[d*ncu + c] for one point; w has ND+2 + (ND+2)*ND entries, each carrying M
 // partial derivatives (M = nc for the full Jacobian, 1 for one column of it).
+// viscous == false: the Euler flux (flux_euler2dNEW.c / flux_euler3dNEW.c), the
+// same expression without the stress and heat terms.
 template <int ND, int M>
-__device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, const Dual<M>* w, Dual<M>* f) {
+__device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, const Dual<M>* w, Dual<M>* f,
+                                             bool viscous = true) {
     constexpr int NCU = ND + 2;
     constexpr int NC = M;
     using D = Dual<M>;
@@ -110,7 +113,7 @@ __device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, c
         for (int i = 0; i < ND; i++) {
             D t = dv[i][d] + dv[d][i];
             if (i == d) t = t - (2.0 / 3.0) * div;
-            t = iRe * t;                                   // tau_id
+            t = viscous ? iRe * t : dc<NC>(0.0);           // tau_id
             D fm = w[1 + i] * v[d] + t;
             if (i == d) fm = fm + p;
             f[d * NCU + 1 + i] = fm;
@@ -118,7 +121,7 @@ __device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, c
             vdv = vdv + v[i] * dv[i][d];
         }
         const D heat = w[NCU * (1 + d) + ND + 1] / rho - E * w[NCU * (1 + d)] / (rho * rho) - vdv;
-        f[d * NCU + ND + 1] = fe + kappa * heat;
+        f[d * NCU + ND + 1] = viscous ? fe + kappa * heat : fe;
     }
 }
 
@@ -205,7 +208,8 @@ __device__ __forceinline__ void ns_farfield_dual(const double* __restrict__ para
 // type without a restatement.
 template <int ND, int M>
 __device__ __forceinline__ bool ns_fbou_dual(int bn, const double* __restrict__ param, const double* ui,
-                                             const double* nl, const Dual<M>* w, const Dual<M>* uh, Dual<M>* fb) {
+                                             const double* nl, const Dual<M>* w, const Dual<M>* uh, Dual<M>* fb,
+                                             bool viscous = true) {
     constexpr int NCU = ND + 2, NC = NCU * (ND + 1);
     const double tau = param[5];
     if (bn == 1) {
@@ -221,7 +225,7 @@ __device__ __forceinline__ bool ns_fbou_dual(int bn, const double* __restrict__ 
         for (int k = 0; k < NCU; k++) wf[k] = uh[k];
 #pragma unroll
         for (int k = NCU; k < NC; k++) wf[k] = w[k];
-        ns_flux_dual<ND, M>(param, wf, f);
+        ns_flux_dual<ND, M>(param, wf, f, viscous);
         Dual<M> t = tau * (w[ND + 1] - uh[ND + 1]);
 #pragma unroll
         for (int d = 0; d < ND; d++) t = t + nl[d] * f[d * NCU + ND + 1];

@@ -47,6 +47,7 @@ class Problem:
     meta: dict = field(default_factory=dict)
     bcm: np.ndarray = None       # boundary condition type per boundary index (app.bcm); None: periodic
     bcs: np.ndarray = None       # (nbnd, nch) boundary states (app.bcs)
+    appname: int = 1             # app.appname: 1 compressible Navier-Stokes, 0 Euler (inviscid, no q equation)
 
     @property
     def nd(self):
@@ -164,6 +165,20 @@ def ns3d_box(n=4, porder=2, seed=0, mach=0.3, re=400.0, dt=0.01,
     p.bcm = np.array(bcm, dtype=np.int64)
     p.bcs = np.tile(_freestream(3, gamma, mach), (len(bcm), 1))
     return p
+
+
+def as_euler(prob: Problem) -> Problem:
+    """The same mesh, state and boundary conditions with the Euler equations
+    (app.appname 0, flag_q 0).  The state keeps the NS layout with q slots: the
+    inviscid flux does not depend on q, so every q coupling of the element
+    matrices vanishes and they equal those of the q-free formulation."""
+    from dataclasses import replace
+    udg = prob.udg.copy()
+    udg[:, prob.ncu:, :] = 0.0
+    sh = prob.sh.copy()
+    sh[:, prob.ncu:, :] = 0.0
+    meta = dict(prob.meta, physics="euler")
+    return replace(prob, name=prob.name + "_euler", udg=udg, sh=sh, appname=0, meta=meta)
 
 
 def make_problem(kind: str, **kw) -> Problem:

@@ -23,7 +23,7 @@ def app_arrays(prob: Problem, preconditioner=0, newton_tol=1e-10, gmres_tol=1e-1
                dirk_stage=1, dirk_order=1, dt_list=None):
     flag = np.zeros(FLAG_LEN)
     flag[0] = prob.tdep
-    flag[5] = 1                      # flag_q: q eliminated by the local solve
+    flag[5] = 1 if prob.appname == 1 else 0   # flag_q: q eliminated by the local solve (NS only)
     flag[9] = 1                      # overlapping level
     flag[16] = preconditioner        # serial reference accepts -1 or 0
     flag[17] = 0                     # left preconditioning
@@ -35,7 +35,7 @@ def app_arrays(prob: Problem, preconditioner=0, newton_tol=1e-10, gmres_tol=1e-1
     factor = np.array([prob.fc_u, prob.fc_q, 0.0, prob.time, 0.0, 0.0])
     problem = np.zeros(PROBLEM_LEN)
     problem[0] = 0                   # HDG
-    problem[1] = 1                   # compressible Navier-Stokes
+    problem[1] = prob.appname        # app.appname: 1 compressible Navier-Stokes, 0 Euler
     problem[3] = dirk_order
     problem[4] = dirk_stage
     problem[5] = 0                   # constant tau
@@ -80,10 +80,11 @@ def write_app(path, prob: Problem, **kw):
     ndims[19] = 1                             # nfile
     ndims[20] = prob.nd
     ndims[21] = prob.nd                       # ncd
-    ndims[22] = prob.nc
+    euler = prob.appname == 0
+    ndims[22] = prob.ncu if euler else prob.nc  # nc (Euler: no gradient unknowns)
     ndims[23] = prob.ncu
     ndims[24] = prob.nch
-    ndims[25] = prob.ncu * prob.nd            # ncq
+    ndims[25] = 0 if euler else prob.ncu * prob.nd   # ncq
     ndims[26] = 0                             # ncp
     ndims[27] = 0                             # nco
     with open(path, "wb") as f:
@@ -174,6 +175,8 @@ def write_mesh(path, prob: Problem):
 def write_sol(path, prob: Problem, udg=None, uh=None):
     udg = prob.udg if udg is None else udg
     uh = prob.uh if uh is None else uh
+    if prob.appname == 0:
+        udg = udg[:, :prob.ncu, :]          # the Euler state has no q
     ndims = np.zeros(10)
     ndims[0] = udg.size
     ndims[1] = uh.size

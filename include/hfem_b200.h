@@ -77,6 +77,13 @@ int hfem_set_mesh(hfem_ctx* ctx, const double* dgnodes, const int* elcon, const 
  * the boundary flux.  Call after hfem_set_mesh (which clears it). */
 int hfem_set_boundary(hfem_ctx* ctx, const int* bf, int nbnd, const int* bcm, const double* bcs);
 
+/* The equations (app.appname of the reference, initializestructs.cpp:126):
+ * 1 compressible Navier-Stokes (default), 0 Euler.  Euler keeps the
+ * Navier-Stokes state layout (the q slots are carried but unused): the
+ * inviscid flux does not depend on q, so the element matrices equal those of
+ * the reference's q-free Euler discretisation (flag_q 0, nc = ncu). */
+int hfem_set_app(hfem_ctx* ctx, int appname);
+
 /* Physics: physicsparam = [gamma, eps, Re, Pr, Mach, tau] (compressible
  * Navier-Stokes, constant tau, constant viscosity), tdep/fc_u/fc_q/time as
  * appstruct (digasopre.h:7-91).  appname 1 (NS) is the one supported. */

@@ -43,6 +43,7 @@ struct oracle_problem {
     const int *bf;                                     // nfe x ne; < 0: boundary -(ib+1); NULL: none
     const int *bcm;                                    // boundary condition type per ib (app.bcm)
     const double *bcs;                                 // nch per ib (app.bcs)
+    int appname;                                       // 1 Navier-Stokes, 0 Euler (inviscid flux)
 };
 
 }  // extern "C"
@@ -76,6 +77,9 @@ static Dual operator/(const Dual& a, const Dual& b) {
 //   f_mi^d  = m_i v_d + p delta_id + tau_id
 //   f_E^d   = (E + p) v_d + sum_i tau_id v_i + mu gamma/(Re Pr) (q_E^d/rho - E q_rho^d/rho^2 - sum_i v_i dv_i/dx_d)
 // with dv_i/dx_d := (q_mi^d - v_i q_rho^d)/rho, tau_ij = mu/Re (dv_i/dx_j + dv_j/dx_i - 2/3 delta_ij div v).
+// Euler (flux_euler2dNEW.c / flux_euler3dNEW.c) is the same flux without the
+// viscous stress and heat terms (g_inviscid).
+static int g_inviscid = 0;
 static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*ncu + c] */) {
     const int ncu = nd + 2;
     const int n = w[0].n;
@@ -100,6 +104,9 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
             tau[i][j] = (1.0 / Re) * t;
         }
     const double kappa = gam / (Re * Pr);
+    if (g_inviscid)
+        for (int i = 0; i < nd; i++)
+            for (int j = 0; j < nd; j++) tau[i][j] = dconst(0.0, n);
     for (int d = 0; d < nd; d++) {
         const Dual* q = &w[ncu * (1 + d)];
         f[d * ncu + 0] = w[1 + d];
@@ -112,7 +119,7 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
         Dual vdv = dconst(0.0, n);
         for (int i = 0; i < nd; i++) { fe = fe + tau[i][d] * v[i]; vdv = vdv + v[i] * dv[i][d]; }
         Dual heat = q[nd + 1] / rho - E * q[0] / (rho * rho) - vdv;
-        f[d * ncu + nd + 1] = fe + kappa * heat;
+        f[d * ncu + nd + 1] = g_inviscid ? fe : fe + kappa * heat;
     }
 }
 
@@ -411,6 +418,7 @@ struct ElemOut {
 //   elementint (elementassembly.cpp:307-572) + faceint (717-1321), flag_q = 1.
 static void element(const oracle_problem& P, const Dims& D, const double* udg_all, const double* uh_all,
                     const double* sh_all, int ie, ElemOut& O) {
+    g_inviscid = (P.appname == 0);
     const int nd = D.nd, npv = D.npv, ngv = D.ngv, ngf = D.ngf, nfe = D.nfe, npf = D.npf;
     const int ncu = D.ncu, nc = D.nc, nch = D.nch, ndf = D.ndf, nd1 = D.nd1, n = D.n, nb = D.nb;
     const double* udg = udg_all + (size_t)ie * npv * nc;

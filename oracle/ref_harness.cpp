@@ -89,7 +89,8 @@ static void setup(Ctx& c, const string& in)
                     c.sol.SH[idx] = (j < ncu) ? c.app.fc_u * c.sol.UDG[idx] : 0.0;
                 }
     }
-    for (Int ie = 0; ie < ne; ie++)
+    if (c.app.flag_q == 1)
+      for (Int ie = 0; ie < ne; ie++)
         getQ(c.elem, c.mesh, m, c.app, c.sol, c.temp, &c.sol.UDG[ie * npv * nc],
              &c.sol.UDG[ie * npv * nc + npv * ncu], &c.sol.UH[0], &c.sol.SH[ie * npv * nc + npv * ncu], ie);
 }

@@ -22,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from hfem_b200.gen.problem import ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier  # noqa: E402
+from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier  # noqa: E402
 from oracle import run_reference  # noqa: E402
 
 CASES = {
@@ -35,6 +35,7 @@ CASES = {
     "ns2d_channel_p2_n3": lambda: ns2d_channel(n=3, porder=2),
     "ns3d_box_p1_n2": lambda: ns3d_box(n=2, porder=1),
     "ns2d_farfield_p2_n3": lambda: ns2d_channel(n=3, porder=2, bcm=(1, 1, 1, 1)),
+    "euler2d_channel_p2_n3": lambda: as_euler(ns2d_channel(n=3, porder=2, bcm=(1, 6, 7, 2))),
 }
 FULL_LIMIT = 400_000          # store arrays up to this many entries in full
 
