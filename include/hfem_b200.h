@@ -86,7 +86,7 @@ int hfem_set_app(hfem_ctx* ctx, int appname);
 
 /* Physics: physicsparam = [gamma, eps, Re, Pr, Mach, tau] (compressible
  * Navier-Stokes, constant tau, constant viscosity), tdep/fc_u/fc_q/time as
- * appstruct (digasopre.h:7-91).  appname 1 (NS) is the one supported. */
+ * appstruct (digasopre.h:7-91); the equations are chosen by hfem_set_app. */
 int hfem_set_physics(hfem_ctx* ctx, const double* physicsparam, int tdep, double fc_u, double fc_q, double time);
 
 /* Solution state sol.UDG (npv x nc x ne), sol.UH (nch x nf*npf) and the time
