@@ -8,7 +8,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhfem_b200.so")
 SOURCES = ["hfem_capi.cu"]
-HEADERS = ["elem_kernels.cuh", "krylov_kernels.cuh", "ns_flux.cuh", "schur_kernels.cuh", "krylov_seg.cuh", "schur_tc.cuh", "elem_kernel_v2.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "177"]
 
@@ -17,7 +16,8 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(SRC, f) for f in SOURCES + HEADERS]
+    headers = [f for f in os.listdir(SRC) if f.endswith((".cuh", ".h"))]
+    deps = [os.path.join(SRC, f) for f in SOURCES + headers]
     deps.append(os.path.join(HERE, "..", "include", "hfem_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

@@ -25,6 +25,7 @@
 #include "elem_kernel_v2.cuh"
 #include "schur_tc.cuh"
 #include "bilu0.cuh"
+#include "inverse_blocked.cuh"
 
 using namespace hfem;
 
@@ -111,6 +112,7 @@ struct Launch {
     size_t elem2_smem;
     const void* elem2_fn;
     int inv_threads;
+    size_t inv_smem;
     const void *elem_fn, *schur_fn, *q_fn, *inv_fn;
     GemmLaunch g1, g2;
     void (*schur_tc)(dim3, size_t, cudaStream_t, const SchurTcArgs&);
@@ -121,7 +123,7 @@ struct Launch {
 
 template <int N>
 void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info) {
-    inverse_kernel<N><<<g, InvThreads<N>::value, 0, st>>>(ne, D, Ru, info);
+    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info);
 }
 
 template <class S>
@@ -160,8 +162,9 @@ Launch make_launch() {
     L.element2 = launch_element2<S>;
     L.elem2_smem = sizeof(ElemSmemV2<S>);
     L.elem2_fn = (const void*)element_kernel_v2<S>;
-    L.inv_threads = InvThreads<S::N>::value;
-    L.inv_fn = (const void*)inverse_kernel<S::N>;
+    L.inv_threads = InvBlk<S::N>::THREADS;
+    L.inv_smem = InvBlk<S::N>::SMEM;
+    L.inv_fn = (const void*)inverse_blocked_kernel<S::N>;
     L.g1 = GemmParams<typename SchurCfg<S>::g1>::make();
     L.g2 = GemmParams<typename SchurCfg<S>::g2>::make();
     L.schur_tc = launch_schur_tc<S>;
@@ -1391,7 +1394,8 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     // each CTA holds 256 of the SM's 512 tensor-memory columns
     c->grid_tc = std::max(1, std::min(d.ne, sms(device) * std::max(1, std::min(occ, 2))));
     occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.inv_fn, L.inv_threads, 0);
+    cudaFuncSetAttribute(L.inv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.inv_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.inv_fn, L.inv_threads, L.inv_smem);
     c->grid_inv = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
     if (pool_alloc(device, (void**)&c->rnorm, sizeof(double)) != cudaSuccess) {
         cudaStreamDestroy(c->own);

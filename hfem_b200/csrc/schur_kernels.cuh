@@ -1,6 +1,6 @@
 // Static condensation on sm_100a, FP64 (restating elementschur.cpp:6-329):
-//   1. inverse_kernel: D^-1 and D^-1 Ru by Gauss-Jordan with partial pivoting,
-//      register-resident (one thread owns one row of [D | Ru]);
+//   1. inverse_blocked_kernel (inverse_blocked.cuh): D^-1 and D^-1 Ru by blocked
+//      Gauss-Jordan with partial pivoting;
 //   2. batched_dgemm: D^-1 F and H - K (D^-1 F) on the FP64 tensor cores
 //      (mma.sync m8n8k4 f64), one CTA per 40-row stripe of one element;
 //   3. batched_dgemv: Rh - K (D^-1 Ru).
@@ -8,102 +8,6 @@
 #include <cuda_runtime.h>
 
 namespace hfem {
-
-// ------------------------------------------------------------ inverse
-// Gauss-Jordan on the rows of [D | Ru] with the pivot column rotated into
-// register 0 after every step, so each thread only ever indexes its row with
-// compile-time constants.  Row pivot[k] is chosen at step k (first row of
-// maximal |.| among rows not yet used, the LAPACK idamax rule).  Slot k of the
-// in-place result X holds the augmented column of row pivot[k], so with
-// P e_k = e_pivot[k]:  X = P D^-1 P, i.e. D^-1(k, l) = X(pivot[k], step(l)) where
-// step(l) is the step at which row l pivoted; the thread of row pivot[k] writes
-// its register m to D^-1(k, pivot[m]).  (D^-1 Ru)(k) is the extra column of row
-// pivot[k].  Writes D^-1 over D and D^-1 Ru over Ru.
-template <int N>
-struct InvThreads {
-    static constexpr int value = ((N + 31) / 32) * 32;
-};
-
-template <int N>
-__global__ void __launch_bounds__(InvThreads<N>::value) inverse_kernel(int ne, double* __restrict__ D,
-                                                                       double* __restrict__ Ru, int* __restrict__ info) {
-    constexpr int NTH = InvThreads<N>::value;
-    constexpr int NW = NTH / 32;
-    __shared__ double prow[N + 1];
-    __shared__ double wv[NW];
-    __shared__ int wi[NW];
-    __shared__ int qrow[N];
-    __shared__ int s_q;
-    const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
-    for (int e = blockIdx.x; e < ne; e += gridDim.x) {
-        double r[N + 1];
-        double* De = D + (size_t)e * N * N;
-        if (i < N) {
-#pragma unroll
-            for (int j = 0; j < N; j++) r[j] = De[i + N * j];
-            r[N] = Ru[(size_t)e * N + i];
-        }
-        bool used = i >= N;
-        int mystep = -1;
-        int bad = 0;
-        for (int k = 0; k < N; k++) {
-            double v = used ? -1.0 : fabs(r[0]);
-            int vi = used ? N : i;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_down_sync(0xffffffffu, v, o);
-                const int oi = __shfl_down_sync(0xffffffffu, vi, o);
-                if (ov > v || (ov == v && oi < vi)) { v = ov; vi = oi; }
-            }
-            if (lane == 0) { wv[warp] = v; wi[warp] = vi; }
-            __syncthreads();
-            if (i == 0) {
-                double b = wv[0];
-                int q = wi[0];
-                for (int w = 1; w < NW; w++)
-                    if (wv[w] > b || (wv[w] == b && wi[w] < q)) { b = wv[w]; q = wi[w]; }
-                s_q = (b > 0.0) ? q : -1;
-            }
-            __syncthreads();
-            const int q = s_q;
-            if (q < 0) { bad = k + 1; break; }
-            if (i == q) {
-                const double inv = 1.0 / r[0];
-#pragma unroll
-                for (int j = 0; j < N - 1; j++) r[j] = r[j + 1] * inv;
-                r[N - 1] = inv;
-                r[N] *= inv;
-#pragma unroll
-                for (int j = 0; j <= N; j++) prow[j] = r[j];
-                used = true;
-                mystep = k;
-                qrow[k] = i;
-            }
-            __syncthreads();
-            if (i != q && i < N) {
-                const double f = r[0];
-#pragma unroll
-                for (int j = 0; j < N - 1; j++) r[j] = fma(-f, prow[j], r[j + 1]);
-                r[N - 1] = -f * prow[N - 1];
-                r[N] = fma(-f, prow[N], r[N]);
-            }
-        }
-        if (bad) {
-            if (i == 0) info[e] = bad;
-            __syncthreads();
-            continue;
-        }
-        __syncthreads();
-        if (i < N) {
-            // row i of X is row mystep of D^-1; column m of X is column qrow[m]
-#pragma unroll
-            for (int m = 0; m < N; m++) De[mystep + N * qrow[m]] = r[m];
-            Ru[(size_t)e * N + mystep] = r[N];
-        }
-        if (i == 0) info[e] = 0;
-        __syncthreads();
-    }
-}
 
 // ------------------------------------------------------------ FP64 mma GEMM
 // D(8x8) += A(8x4, row) * B(4x8, col); lane l holds A(l/4, l%4), B(l%4, l/4),
