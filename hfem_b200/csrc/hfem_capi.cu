@@ -50,15 +50,18 @@ struct KernelTimer {
     X(3, 20, 10, 24, 12)
 
 // GEMM tile choices per shape (m-tiles, n-tiles per warp, warps): g1 for D^-1 F
-// (n x nb, K = n), g2 for H - K D^-1 F (nb x nb, K = n).
+// (n x nb, K = n), g2 for H - K D^-1 F (nb x nb, K = n); the fastest of the
+// candidates below on a B200, timed on 20k-51k-element meshes of each shape.
+// Small CTAs (1-3 warps, 2-stage) win: many resident CTAs hide the short
+// (K <= 100) main loops' fill and drain.
 template <class S> struct SchurCfg;
 template <> struct SchurCfg<Shape<2, 3, 2, 3, 2>> { using g1 = GemmCfg<2, 3, 1>; using g2 = GemmCfg<3, 3, 1>; };
-template <> struct SchurCfg<Shape<2, 6, 3, 6, 3>> { using g1 = GemmCfg<3, 5, 1>; using g2 = GemmCfg<5, 5, 1>; };
+template <> struct SchurCfg<Shape<2, 6, 3, 6, 3>> { using g1 = GemmCfg<3, 5, 1>; using g2 = GemmCfg<5, 3, 2>; };
 template <> struct SchurCfg<Shape<2, 10, 4, 12, 4>> { using g1 = GemmCfg<5, 3, 2>; using g2 = GemmCfg<6, 3, 2>; };
-template <> struct SchurCfg<Shape<2, 15, 5, 16, 5>> { using g1 = GemmCfg<4, 4, 2>; using g2 = GemmCfg<4, 4, 2>; };
-template <> struct SchurCfg<Shape<3, 4, 3, 4, 3>> { using g1 = GemmCfg<3, 4, 2>; using g2 = GemmCfg<4, 4, 2>; };
-template <> struct SchurCfg<Shape<3, 10, 6, 14, 6>> { using g1 = GemmCfg<7, 3, 5>; using g2 = GemmCfg<5, 3, 5>; };
-template <> struct SchurCfg<Shape<3, 20, 10, 24, 12>> { using g1 = GemmCfg<5, 5, 5>; using g2 = GemmCfg<5, 5, 5>; };
+template <> struct SchurCfg<Shape<2, 15, 5, 16, 5>> { using g1 = GemmCfg<4, 4, 2>; using g2 = GemmCfg<4, 2, 4>; };
+template <> struct SchurCfg<Shape<3, 4, 3, 4, 3>> { using g1 = GemmCfg<3, 4, 2>; using g2 = GemmCfg<4, 2, 4>; };
+template <> struct SchurCfg<Shape<3, 10, 6, 14, 6>> { using g1 = GemmCfg<4, 4, 2>; using g2 = GemmCfg<4, 2, 4>; };
+template <> struct SchurCfg<Shape<3, 20, 10, 24, 12>> { using g1 = GemmCfg<5, 3, 3>; using g2 = GemmCfg<5, 3, 2>; };
 
 struct GemmLaunch {
     int bm, bn, threads;
@@ -68,20 +71,20 @@ struct GemmLaunch {
                 long long, double, double*, int, long long);
 };
 
-template <class G, int MT, int WN, int NW>
+template <class G, int MT, int WN, int NW, int BK, int ST>
 void run_gemm(cudaStream_t st, int batch, int M, int N, int K, double alpha, const double* A, int lda, long long sA,
               const double* B, int ldb, long long sB, double beta, double* C, int ldc, long long sC) {
     const int tiles = ((M + G::BM - 1) / G::BM) * ((N + G::BN - 1) / G::BN);
-    batched_dgemm_kernel<MT, WN, NW><<<(unsigned)(tiles * batch), G::THREADS, G::SMEM, st>>>(
+    batched_dgemm_kernel<MT, WN, NW, BK, ST><<<(unsigned)(tiles * batch), G::THREADS, G::SMEM, st>>>(
         M, N, K, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC);
 }
 
 template <class G> struct GemmParams;
-template <int MT, int WN, int NW> struct GemmParams<GemmCfg<MT, WN, NW>> {
+template <int MT, int WN, int NW, int BK, int ST> struct GemmParams<GemmCfg<MT, WN, NW, BK, ST>> {
     static GemmLaunch make() {
-        using G = GemmCfg<MT, WN, NW>;
-        return GemmLaunch{G::BM, G::BN, G::THREADS, G::SMEM, (const void*)batched_dgemm_kernel<MT, WN, NW>,
-                          run_gemm<G, MT, WN, NW>};
+        using G = GemmCfg<MT, WN, NW, BK, ST>;
+        return GemmLaunch{G::BM, G::BN, G::THREADS, G::SMEM, (const void*)batched_dgemm_kernel<MT, WN, NW, BK, ST>,
+                          run_gemm<G, MT, WN, NW, BK, ST>};
     }
 };
 
@@ -95,6 +98,8 @@ const std::vector<GemmLaunch>& gemm_candidates() {
         GemmParams<GemmCfg<4, 4, 2>>::make(), GemmParams<GemmCfg<3, 4, 2>>::make(),
         GemmParams<GemmCfg<7, 3, 5>>::make(), GemmParams<GemmCfg<5, 3, 5>>::make(),
         GemmParams<GemmCfg<5, 5, 5>>::make(), GemmParams<GemmCfg<4, 2, 4>>::make(),
+        GemmParams<GemmCfg<5, 4, 2>>::make(), GemmParams<GemmCfg<5, 3, 3>>::make(),
+        GemmParams<GemmCfg<5, 5, 5, 12, 4>>::make(), GemmParams<GemmCfg<5, 3, 2, 20, 3>>::make(),
     };
     return v;
 }

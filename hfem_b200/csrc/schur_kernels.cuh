@@ -24,11 +24,12 @@ __device__ __forceinline__ void dmma8x8x4(double& c0, double& c1, double a, doub
 // leading dimensions (A: 8*MT padded to 4 mod 16 doubles, B: 20) make the
 // fragment loads bank-conflict free.  Grid: ceil(M/BM) * ceil(N/BN) * batch CTAs,
 // element-major (the tiles of one element run together and share it in L2).
-template <int MT, int WN, int NW>
+template <int MT, int WN, int NW, int BK_ = 20, int STAGES_ = 2>
 struct GemmCfg {
-    static constexpr int BM = 8 * MT, BN = 8 * WN * NW, BK = 20, STAGES = 2;
+    static constexpr int BM = 8 * MT, BN = 8 * WN * NW, BK = BK_, STAGES = STAGES_;
+    static_assert(BK % 4 == 0 && STAGES >= 2, "k stages of whole DMMA steps, at least double buffered");
     static constexpr int LDA = ((BM + 11) / 16) * 16 + 4;     // >= BM, == 4 (mod 16)
-    static constexpr int LDB = BK;
+    static constexpr int LDB = (BK % 16 == 4 || BK % 16 == 12) ? BK : BK + 4;   // == 4 or 12 (mod 16)
     static constexpr int THREADS = 32 * NW;
     static constexpr int ASZ = LDA * BK, BSZ = LDB * BN;
     static constexpr size_t SMEM = sizeof(double) * (size_t)STAGES * (ASZ + BSZ);
@@ -42,17 +43,23 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
     const int n = valid ? 8 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem), "r"(n));
 }
+// 16-byte variant (both addresses 16-byte aligned); zero-fills when !valid.
+__device__ __forceinline__ void cp_async16z(double* smem, const double* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(n));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
 
-template <int MT, int WN, int NW>
+template <int MT, int WN, int NW, int BK_ = 20, int STAGES_ = 2>
 __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, int K, double alpha,
                                                                 const double* __restrict__ A, int lda, long long sA,
                                                                 const double* __restrict__ B, int ldb, long long sB,
                                                                 double beta, double* __restrict__ C, int ldc,
                                                                 long long sC) {
-    using G = GemmCfg<MT, WN, NW>;
+    using G = GemmCfg<MT, WN, NW, BK_, STAGES_>;
     extern __shared__ __align__(16) double gsm[];
     const int tilesM = (M + G::BM - 1) / G::BM, tilesN = (N + G::BN - 1) / G::BN;
     const int e = blockIdx.x / (tilesM * tilesN), tile = blockIdx.x % (tilesM * tilesN);
@@ -65,45 +72,74 @@ __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, in
 
     auto stage_a = [&](int st) { return gsm + st * (G::ASZ + G::BSZ); };
     auto stage_b = [&](int st) { return gsm + st * (G::ASZ + G::BSZ) + G::ASZ; };
+    // pairs of doubles per copy when every column of A and B starts 16-byte
+    // aligned and the copied extents (M rows of A, K rows of B) are even
+    const bool pairs = ((M | K | lda | ldb) & 1) == 0 && ((reinterpret_cast<size_t>(Ae) | reinterpret_cast<size_t>(Be)) & 15) == 0;
     auto load = [&](int st, int k0) {
         double* As = stage_a(st);
         double* Bs = stage_b(st);
-        for (int t = tid; t < G::BM * G::BK; t += G::THREADS) {
-            const int m = t % G::BM, k = t / G::BM;
-            const bool ok = (m0 + m < M) && (k0 + k < K);
-            cp_async8(&As[m + G::LDA * k], Ae + (ok ? (m0 + m) + (size_t)lda * (k0 + k) : 0), ok);
-        }
-        for (int t = tid; t < G::BK * G::BN; t += G::THREADS) {
-            const int k = t % G::BK, n = t / G::BK;
-            const bool ok = (n0 + n < N) && (k0 + k < K);
-            cp_async8(&Bs[k + G::LDB * n], Be + (ok ? (k0 + k) + (size_t)ldb * (n0 + n) : 0), ok);
+        if (pairs) {
+            for (int t = tid; t < (G::BM / 2) * G::BK; t += G::THREADS) {
+                const int m = 2 * (t % (G::BM / 2)), k = t / (G::BM / 2);
+                const bool ok = (m0 + m < M) && (k0 + k < K);
+                cp_async16z(&As[m + G::LDA * k], Ae + (ok ? (m0 + m) + (size_t)lda * (k0 + k) : 0), ok);
+            }
+            for (int t = tid; t < (G::BK / 2) * G::BN; t += G::THREADS) {
+                const int k = 2 * (t % (G::BK / 2)), n = t / (G::BK / 2);
+                const bool ok = (n0 + n < N) && (k0 + k < K);
+                cp_async16z(&Bs[k + G::LDB * n], Be + (ok ? (k0 + k) + (size_t)ldb * (n0 + n) : 0), ok);
+            }
+        } else {
+            for (int t = tid; t < G::BM * G::BK; t += G::THREADS) {
+                const int m = t % G::BM, k = t / G::BM;
+                const bool ok = (m0 + m < M) && (k0 + k < K);
+                cp_async8(&As[m + G::LDA * k], Ae + (ok ? (m0 + m) + (size_t)lda * (k0 + k) : 0), ok);
+            }
+            for (int t = tid; t < G::BK * G::BN; t += G::THREADS) {
+                const int k = t % G::BK, n = t / G::BK;
+                const bool ok = (n0 + n < N) && (k0 + k < K);
+                cp_async8(&Bs[k + G::LDB * n], Be + (ok ? (k0 + k) + (size_t)ldb * (n0 + n) : 0), ok);
+            }
         }
     };
 
+    // the accumulators start from beta C (loaded while the first stage is in
+    // flight) and take alpha A B, so the epilogue only stores
+    load(0, 0);
+    cp_async_commit();
     double acc[MT][WN][2];
 #pragma unroll
     for (int a = 0; a < MT; a++)
 #pragma unroll
-        for (int b = 0; b < WN; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+        for (int b = 0; b < WN; b++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int m = m0 + 8 * a + gr, n = n0 + 8 * (warp * WN + b) + 2 * gc + h;
+                acc[a][b][h] = (beta != 0.0 && m < M && n < N) ? beta * Ce[m + (size_t)ldc * n] : 0.0;
+            }
     const int nk = (K + G::BK - 1) / G::BK;
-    load(0, 0);
-    cp_async_commit();
+    // STAGES - 1 k stages in flight; one commit group per stage (empty past K)
+#pragma unroll
+    for (int st = 1; st < G::STAGES - 1; st++) {
+        if (st < nk) load(st, st * G::BK);
+        cp_async_commit();
+    }
     for (int kt = 0; kt < nk; kt++) {
-        if (kt + 1 < nk) {
-            load((kt + 1) & 1, (kt + 1) * G::BK);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        cp_async_wait<G::STAGES - 2>();
         __syncthreads();
-        const double* As = stage_a(kt & 1);
-        const double* Bs = stage_b(kt & 1);
+        // every thread is past stage kt - 1: its slot takes stage kt + STAGES - 1
+        {
+            const int nx = kt + G::STAGES - 1;
+            if (nx < nk) load(nx % G::STAGES, nx * G::BK);
+            cp_async_commit();
+        }
+        const double* As = stage_a(kt % G::STAGES);
+        const double* Bs = stage_b(kt % G::STAGES);
 #pragma unroll
         for (int ks = 0; ks < G::BK; ks += 4) {
             double af[MT], bf[WN];
 #pragma unroll
-            for (int a = 0; a < MT; a++) af[a] = As[(8 * a + gr) + G::LDA * (ks + gc)];
+            for (int a = 0; a < MT; a++) af[a] = alpha * As[(8 * a + gr) + G::LDA * (ks + gc)];
 #pragma unroll
             for (int b = 0; b < WN; b++) bf[b] = Bs[(ks + gc) + G::LDB * (8 * (warp * WN + b) + gr)];
 #pragma unroll
@@ -111,7 +147,6 @@ __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, in
 #pragma unroll
                 for (int b = 0; b < WN; b++) dmma8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
         }
-        __syncthreads();
     }
 #pragma unroll
     for (int a = 0; a < MT; a++)
@@ -120,10 +155,7 @@ __global__ void __launch_bounds__(32 * NW) batched_dgemm_kernel(int M, int N, in
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int m = m0 + 8 * a + gr, n = n0 + 8 * (warp * WN + b) + 2 * gc + h;
-                if (m < M && n < N) {
-                    double* c = &Ce[m + (size_t)ldc * n];
-                    *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[a][b][h];
-                }
+                if (m < M && n < N) Ce[m + (size_t)ldc * n] = acc[a][b][h];
             }
 }
 
