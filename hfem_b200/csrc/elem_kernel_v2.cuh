@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         __syncthreads();
         for (int t = tid; t < NPV * ND + NDF * ND; t += NT) {
             double* col = (t < NPV * ND) ? &Cm[NPV * t] : &Em[NPV * (t - NPV * ND)];
-            chol_solve_col<NPV>(M, col);
+            chol_solve_col_reg<NPV>(M, col);
         }
         __syncthreads();
         for (int t = tid; t < NGV * NPV * ND; t += NT) {
@@ -338,33 +338,46 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             __syncthreads();
             double* BK = Bs;                              // KFD x NPV  (ld C3::LDBK)
             double* BH = Bs + C3<S>::LDBK * C3<S>::NKP;   // KFD x NDF  (ld C3::LDBK)
-            for (int t = tid; t < C3<S>::KFD * (C3<S>::NKP + C3<S>::NHP); t += NT) {
-                const int k = t % C3<S>::KFD, n = t / C3<S>::KFD;
-                const int q = k % NGF, dp = k / NGF, gg = q + NGF * fc;
-                double v = 0.0;
-                if (dp <= ND && k < NGF * ND1) {
-                    if (n < C3<S>::NKP) {                 // K columns a
-                        const int a = n;
-                        if (a < NPV) {
-                            if (dp == 0) {
-                                const int p = sm.pos[fc * NPV + a];
-                                v = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
-                            } else {
-                                v = sMiCf[gg + NA * (a + NPV * (dp - 1))];
+            // U entries per thread are read before any is stored (the global
+            // reads of one batch are in flight together)
+            constexpr int TB = C3<S>::KFD * (C3<S>::NKP + C3<S>::NHP), UB = 8;
+            for (int base = tid; base < TB; base += UB * NT) {
+                double v[UB];
+#pragma unroll
+                for (int u = 0; u < UB; u++) {
+                    const int t = base + u * NT;
+                    const int k = t % C3<S>::KFD, n = t / C3<S>::KFD;
+                    const int q = k % NGF, dp = k / NGF, gg = q + NGF * fc;
+                    double x = 0.0;
+                    if (t < TB && dp <= ND && k < NGF * ND1) {
+                        if (n < C3<S>::NKP) {                 // K columns a
+                            const int a = n;
+                            if (a < NPV) {
+                                if (dp == 0) {
+                                    const int p = sm.pos[fc * NPV + a];
+                                    x = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
+                                } else {
+                                    x = sMiCf[gg + NA * (a + NPV * (dp - 1))];
+                                }
+                            }
+                        } else {                              // H columns f2
+                            const int f2 = n - C3<S>::NKP;
+                            if (f2 < NDF) {
+                                if (dp == 0) x = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
+                                else x = -sMiEf[gg + NA * (f2 + NDF * (dp - 1))];
                             }
                         }
-                        BK[k + C3<S>::LDBK * a] = v;
-                    } else {                              // H columns f2
-                        const int f2 = n - C3<S>::NKP;
-                        if (f2 < NDF) {
-                            if (dp == 0) v = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
-                            else v = -sMiEf[gg + NA * (f2 + NDF * (dp - 1))];
-                        }
-                        BH[k + C3<S>::LDBK * f2] = v;
                     }
-                } else {
-                    if (n < C3<S>::NKP) BK[k + C3<S>::LDBK * n] = 0.0;
-                    else BH[k + C3<S>::LDBK * (n - C3<S>::NKP)] = 0.0;
+                    v[u] = x;
+                }
+#pragma unroll
+                for (int u = 0; u < UB; u++) {
+                    const int t = base + u * NT;
+                    if (t < TB) {
+                        const int k = t % C3<S>::KFD, n = t / C3<S>::KFD;
+                        if (n < C3<S>::NKP) BK[k + C3<S>::LDBK * n] = v[u];
+                        else BH[k + C3<S>::LDBK * (n - C3<S>::NKP)] = v[u];
+                    }
                 }
             }
             __syncthreads();
@@ -429,19 +442,34 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         {
             double* Phi = Bs;                              // KV x NPV   (ld LDBD)
             double* Psi = Bs + C3<S>::LDBD * C3<S>::NKP;   // KQ x NDF   (ld LDBD)
-            for (int t = tid; t < C3<S>::KV3 * (C3<S>::NKP + C3<S>::NHP); t += NT) {
-                const int k = t % C3<S>::KV3, n = t / C3<S>::KV3;
-                const int g = k % NGV, dp = k / NGV;
-                if (n < C3<S>::NKP) {
-                    double v = 0.0;
-                    if (n < NPV && k < NGV * ND1)
-                        v = (dp == 0) ? T.shapvt[g + NGV * n] : sMiC[g + NGV * (n + NPV * (dp - 1))];
-                    Phi[k + C3<S>::LDBD * n] = v;
-                } else {
-                    const int f2 = n - C3<S>::NKP;
-                    double v = 0.0;
-                    if (f2 < NDF && k < NGV * ND) v = sMiE[g + NGV * (f2 + NDF * dp)];
-                    Psi[k + C3<S>::LDBD * f2] = v;
+            constexpr int TV = C3<S>::KV3 * (C3<S>::NKP + C3<S>::NHP), UV = 8;
+            for (int base = tid; base < TV; base += UV * NT) {
+                double v[UV];
+#pragma unroll
+                for (int u = 0; u < UV; u++) {
+                    const int t = base + u * NT;
+                    const int k = t % C3<S>::KV3, n = t / C3<S>::KV3;
+                    const int g = k % NGV, dp = k / NGV;
+                    double x = 0.0;
+                    if (t < TV) {
+                        if (n < C3<S>::NKP) {
+                            if (n < NPV && k < NGV * ND1)
+                                x = (dp == 0) ? T.shapvt[g + NGV * n] : sMiC[g + NGV * (n + NPV * (dp - 1))];
+                        } else {
+                            const int f2 = n - C3<S>::NKP;
+                            if (f2 < NDF && k < NGV * ND) x = sMiE[g + NGV * (f2 + NDF * dp)];
+                        }
+                    }
+                    v[u] = x;
+                }
+#pragma unroll
+                for (int u = 0; u < UV; u++) {
+                    const int t = base + u * NT;
+                    if (t < TV) {
+                        const int k = t % C3<S>::KV3, n = t / C3<S>::KV3;
+                        if (n < C3<S>::NKP) Phi[k + C3<S>::LDBD * n] = v[u];
+                        else Psi[k + C3<S>::LDBD * (n - C3<S>::NKP)] = v[u];
+                    }
                 }
             }
             __syncthreads();
@@ -493,27 +521,48 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
 #pragma unroll
                         for (int h = 0; h < 2; h++) {
                             const int a = 8 * b + 2 * gc + h;
-                            if (a < NPV) {
-                                const int kcol = a + NPV * k;
-                                double v = acc[b][h];
-                                for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
-                                    v += Ke[j + NCH * sm.inc_f[i * S::MAXINC + c2] + (size_t)NB * kcol];
-                                De[i + NPV * (j + NCU * kcol)] = v;
-                            }
+                            if (a < NPV) De[i + NPV * (j + NCU * (a + NPV * k))] = acc[b][h];
                         }
 #pragma unroll
                     for (int b = 0; b < C3<S>::NTH; b++)
 #pragma unroll
                         for (int h = 0; h < 2; h++) {
                             const int f2 = 8 * b + 2 * gc + h;
-                            if (f2 < NDF) {
-                                const int hcol = k + NCH * f2;
-                                double v = accf[b][h];
-                                for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
-                                    v += He[j + NCH * sm.inc_f[i * S::MAXINC + c2] + (size_t)NB * hcol];
-                                Fe[i + NPV * (j + NCU * hcol)] = v;
-                            }
+                            if (f2 < NDF) Fe[i + NPV * (j + NCU * (k + NCH * f2))] = accf[b][h];
                         }
+                }
+            }
+            __syncthreads();
+            // lifted trace terms, D += P K and F += P H (P: face dof -> element
+            // node), entry by entry in the face order of each node; U entries per
+            // thread are gathered before any is stored, so many loads are in flight
+            constexpr int TOT = N * (N + NB), U = 4;
+            for (int base = tid; base < TOT; base += U * NT) {
+                double v[U];
+#pragma unroll
+                for (int q = 0; q < U; q++) {
+                    const int t = base + q * NT;
+                    v[q] = 0.0;
+                    if (t < TOT) {
+                        const bool isD = t < N * N;
+                        const int u = isD ? t : t - N * N;
+                        const int i = u % NPV, j = (u / NPV) % NCU, col = u / N;
+                        const double* src = (isD ? Ke : He) + j + (size_t)NB * col;
+                        double x = isD ? De[u] : Fe[u];
+                        const int ni = sm.inc_n[i];
+#pragma unroll
+                        for (int c2 = 0; c2 < S::MAXINC; c2++)
+                            if (c2 < ni) x += src[NCH * sm.inc_f[i * S::MAXINC + c2]];
+                        v[q] = x;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < U; q++) {
+                    const int t = base + q * NT;
+                    if (t < TOT) {
+                        if (t < N * N) De[t] = v[q];
+                        else Fe[t - N * N] = v[q];
+                    }
                 }
             }
         }

@@ -221,6 +221,36 @@ __device__ __forceinline__ void chol_solve_col(const double* l, double* x) {
     }
 }
 
+// The same two triangular solves with the column held in registers: the
+// column's shared-memory words are read once and written once (threads own
+// columns NPV doubles apart, so every shared access of a column is bank
+// conflicted), and the dependent chains run on registers.
+template <int NPV>
+__device__ __forceinline__ void chol_solve_col_reg(const double* lm, double* col) {
+    // factor entries are read where they are used (not hoisted), which keeps
+    // the register footprint to the column itself
+    const volatile double* l = lm;
+    double x[NPV];
+#pragma unroll
+    for (int i = 0; i < NPV; i++) x[i] = col[i];
+#pragma unroll
+    for (int i = 0; i < NPV; i++) {
+        double t = x[i];
+#pragma unroll
+        for (int k = 0; k < i; k++) t -= l[i + NPV * k] * x[k];
+        x[i] = t / l[i + NPV * i];
+    }
+#pragma unroll
+    for (int i = NPV - 1; i >= 0; i--) {
+        double t = x[i];
+#pragma unroll
+        for (int k = i + 1; k < NPV; k++) t -= l[k + NPV * i] * x[k];
+        x[i] = t / l[i + NPV * i];
+    }
+#pragma unroll
+    for (int i = 0; i < NPV; i++) col[i] = x[i];
+}
+
 // ------------------------------------------------------------ element kernel
 template <class S>
 struct ElemSmem {
