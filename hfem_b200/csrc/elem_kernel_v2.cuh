@@ -48,8 +48,11 @@ struct V2 {
     static constexpr int LDAF = ((8 * MTF + 11) / 16) * 16 + 4;
     static constexpr int QSZ = S::NPV * S::NPV * (1 + S::ND) + S::NPV * S::NDF * S::ND + S::NGV * S::NC +
                                S::NA * (S::NC + S::NCH);
-    static constexpr int UN = QSZ > C3<S>::BKH ? (QSZ > C3<S>::BDF ? QSZ : C3<S>::BDF)
-                                               : (C3<S>::BKH > C3<S>::BDF ? C3<S>::BKH : C3<S>::BDF);
+    // one face's flux-Jacobian slices, staged beside its B operands
+    static constexpr int FSL = S::NGF * S::NCH * (S::NC + S::NCU);
+    static constexpr int BKF = C3<S>::BKH + FSL;
+    static constexpr int UN = QSZ > BKF ? (QSZ > C3<S>::BDF ? QSZ : C3<S>::BDF)
+                                        : (BKF > C3<S>::BDF ? BKF : C3<S>::BDF);
     static constexpr int WS = S::WS + C3<S>::WY;              // workspace doubles per CTA slot
 };
 
@@ -319,16 +322,18 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         }
         // Y, stored so that row (i,j,k) and column (g,d') of the volume GEMMs are
         // separable: Ys[(i + NPV j) + N (g + NGV (NCU d' + k))]
-        for (int t = tid; t < NGV * NCU * NC; t += NT) {
-            const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
-            double w[ND1];
+        // one thread per (i, g, j), i fastest, so the stores of a warp are runs of
+        // consecutive words and its wrl reads are shared by the lanes of one (g, j)
+        for (int t = tid; t < NPV * NGV * NCU; t += NT) {
+            const int i = t % NPV, g = (t / NPV) % NGV, j = t / (NPV * NGV);
+            double av[ND1];
 #pragma unroll
-            for (int r = 0; r < ND1; r++) w[r] = wrl[g + NGV * (r + ND1 * (j + NCU * c))];
+            for (int r = 0; r < ND1; r++) av[r] = sm.Av[i + C2::LDAV * (g + NGV * r)];
 #pragma unroll 4
-            for (int i = 0; i < NPV; i++) {
+            for (int c = 0; c < NC; c++) {
                 double y = 0.0;
 #pragma unroll
-                for (int r = 0; r < ND1; r++) y += sm.Av[i + C2::LDAV * (g + NGV * r)] * w[r];
+                for (int r = 0; r < ND1; r++) y += av[r] * wrl[g + NGV * (r + ND1 * (j + NCU * c))];
                 Ys[(i + NPV * j) + (size_t)N * (g + NGV * c)] = y;
             }
         }
@@ -380,24 +385,47 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                     }
                 }
             }
+            // the face's slices of the flux Jacobians: sfu[q + NGF (j + NCH c)],
+            // sfuh[q + NGF (j + NCH m)]
+            double* sfu = Bs + C3<S>::BKH;
+            double* sfuh = sfu + NGF * NCH * NC;
+            {
+                constexpr int TS = NGF * NCH * (NC + NCU), US = 8;
+                for (int base = tid; base < TS; base += US * NT) {
+                    double v[US];
+#pragma unroll
+                    for (int u = 0; u < US; u++) {
+                        const int t = base + u * NT;
+                        const int q = t % NGF, jc = t / NGF;
+                        v[u] = 0.0;
+                        if (t < TS)
+                            v[u] = (jc < NCH * NC) ? fnu_s[q + NGF * fc + NA * jc]
+                                                   : fnuh_s[q + NGF * fc + NA * (jc - NCH * NC)];
+                    }
+#pragma unroll
+                    for (int u = 0; u < US; u++)
+                        if (base + u * NT < TS) sfu[base + u * NT] = v[u];
+                }
+            }
             __syncthreads();
             constexpr int MTK = (NPF * NCH * NCU + 7) / 8;
             for (int mt = warp; mt < MTK; mt += NT / 32) {
                 const int r = 8 * mt + gr;
                 const bool rv = r < NPF * NCH * NCU;
-                const int ip = r % NPF, j = (r / NPF) % NCH, m = r / (NPF * NCH);
+                // j fastest: the 8 rows of a tile are 8 consecutive words of a K/H column
+                const int j = r % NCH, ip = (r / NCH) % NPF, m = r / (NPF * NCH);
                 double aK[C3<S>::KFD / 4], aH[C3<S>::KFD / 4];
 #pragma unroll
                 for (int ks = 0; ks < C3<S>::KFD / 4; ks++) {
-                    const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF, gg = q + NGF * fc;
+                    const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF;
                     double vK = 0.0, vH = 0.0;
                     if (rv && k < NGF * ND1) {
                         const double sf = sm.Af[ip + C2::LDAF * q];
                         if (dp == 0) {
-                            vK = sf * fnu_s[gg + NA * (j + NCH * m)];
-                            vH = sf * fnuh_s[gg + NA * (j + NCH * m)];
+                            vK = sf * sfu[q + NGF * (j + NCH * m)];
+                            vH = sf * sfuh[q + NGF * (j + NCH * m)];
                         } else {
-                            vK = sf * fnu_s[gg + NA * (j + NCH * (NCU * dp + m))];
+                            vK = sf * sfu[q + NGF * (j + NCH * (NCU * dp + m))];
                             vH = vK;
                         }
                     }
