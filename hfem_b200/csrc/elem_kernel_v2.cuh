@@ -320,21 +320,20 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             Rhe[t] = -s;
             Roe[t] = -s;
         }
-        // Y, stored so that row (i,j,k) and column (g,d') of the volume GEMMs are
-        // separable: Ys[(i + NPV j) + N (g + NGV (NCU d' + k))]
-        // one thread per (i, g, j), i fastest, so the stores of a warp are runs of
-        // consecutive words and its wrl reads are shared by the lanes of one (g, j)
-        for (int t = tid; t < NPV * NGV * NCU; t += NT) {
-            const int i = t % NPV, g = (t / NPV) % NGV, j = t / (NPV * NGV);
-            double av[ND1];
+        // Y, point index fastest: Ys[g + NGV (c + NC (i + NPV j))], c = NCU d' + k.
+        // One thread per (g, j, c) with g fastest: its wrl words are read once and
+        // the stores of a warp are runs of consecutive words.
+        for (int t = tid; t < NGV * NCU * NC; t += NT) {
+            const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
+            double w[ND1];
 #pragma unroll
-            for (int r = 0; r < ND1; r++) av[r] = sm.Av[i + C2::LDAV * (g + NGV * r)];
+            for (int r = 0; r < ND1; r++) w[r] = wrl[g + NGV * (r + ND1 * (j + NCU * c))];
 #pragma unroll 4
-            for (int c = 0; c < NC; c++) {
+            for (int i = 0; i < NPV; i++) {
                 double y = 0.0;
 #pragma unroll
-                for (int r = 0; r < ND1; r++) y += av[r] * wrl[g + NGV * (r + ND1 * (j + NCU * c))];
-                Ys[(i + NPV * j) + (size_t)N * (g + NGV * c)] = y;
+                for (int r = 0; r < ND1; r++) y += sm.Av[i + C2::LDAV * (g + NGV * r)] * w[r];
+                Ys[g + NGV * (c + NC * (i + NPV * j))] = y;
             }
         }
         // ---- K and H face by face: rows (ip, j, m), k = (q, d'), generated A = shapfg(ip,q) x fhn
@@ -464,9 +463,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                     }
             }
                 };
-        for (int fc = 0; fc < NFE; fc++) face_rows(fc, fnu, fnuh);
-        __syncthreads();
         // ---- D_vol = Y' Phi and F_vol = Y'_q Psi, B operands in shared memory
+        // (right after Y is written, while it is still in L2), then the faces
         {
             double* Phi = Bs;                              // KV x NPV   (ld LDBD)
             double* Psi = Bs + C3<S>::LDBD * C3<S>::NKP;   // KQ x NDF   (ld LDBD)
@@ -508,7 +506,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 const int r = 8 * mt + gr;
                 const bool rv = r < NPV * NCU * NCU;
                 const int i = r % NPV, j = (r / NPV) % NCU, k = r / (NPV * NCU);
-                const double* yrow = Ys + (i + NPV * j) + (size_t)N * NGV * k;
+                const double* yrow = Ys + NGV * (k + NC * (i + NPV * j));
                 double acc[C3<S>::NTK][2];
 #pragma unroll
                 for (int b = 0; b < C3<S>::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
@@ -518,7 +516,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
 #pragma unroll
                 for (int ks = 0; ks < C3<S>::KV3 / 4; ks++) {
                     const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
-                    av[ks] = (rv && kk < NGV * ND1) ? yrow[(size_t)N * (g + NGV * NCU * dp)] : 0.0;
+                    av[ks] = (rv && kk < NGV * ND1) ? yrow[g + NGV * NCU * dp] : 0.0;
                 }
 #pragma unroll
                 for (int ks = 0; ks < C3<S>::KV3 / 4; ks++) {
@@ -534,7 +532,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
 #pragma unroll
                 for (int ks = 0; ks < C3<S>::KQ3 / 4; ks++) {
                     const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
-                    aq[ks] = (rv && kk < NGV * ND) ? yrow[(size_t)N * (g + NGV * NCU * (d + 1))] : 0.0;
+                    aq[ks] = (rv && kk < NGV * ND) ? yrow[g + NGV * NCU * (d + 1)] : 0.0;
                 }
 #pragma unroll
                 for (int ks = 0; ks < C3<S>::KQ3 / 4; ks++) {
@@ -560,6 +558,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                         }
                 }
             }
+            for (int fc = 0; fc < NFE; fc++) face_rows(fc, fnu, fnuh);
             __syncthreads();
             // lifted trace terms, D += P K and F += P H (P: face dof -> element
             // node), entry by entry in the face order of each node; U entries per
