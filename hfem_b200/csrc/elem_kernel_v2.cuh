@@ -309,6 +309,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         __syncthreads();
 
         double* Ke = A.K + (size_t)e * NB * N;
+        double* De = A.D + (size_t)e * N * N;
+        double* Fe = A.F + (size_t)e * N * NB;
         double* He = A.H + (size_t)e * NB * NB;
         double* Rhe = A.Rh + (size_t)e * NB;
         double* Roe = A.Ro + (size_t)e * NB;
@@ -338,7 +340,9 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         }
         // ---- K and H face by face: rows (ip, j, m), k = (q, d'), generated A = shapfg(ip,q) x fhn
         // (fnu_s/fnuh_s: the face flux Jacobians, fhat or, on boundary faces later, fb)
-        auto face_rows = [&](int fc, const double* fnu_s, const double* fnuh_s) {
+        // lift: also add the rows to the element equations of the face's nodes
+        // (D += P K, F += P H) by reductions in L2, face after face
+        auto face_rows = [&](int fc, const double* fnu_s, const double* fnuh_s, bool lift) {
             __syncthreads();
             double* BK = Bs;                              // KFD x NPV  (ld C3::LDBK)
             double* BH = Bs + C3<S>::LDBK * C3<S>::NKP;   // KFD x NDF  (ld C3::LDBK)
@@ -413,6 +417,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 const bool rv = r < NPF * NCH * NCU;
                 // j fastest: the 8 rows of a tile are 8 consecutive words of a K/H column
                 const int j = r % NCH, ip = (r / NCH) % NPF, m = r / (NPF * NCH);
+                const int inode = sm.perm[fc * NPF + ip];
                 double aK[C3<S>::KFD / 4], aH[C3<S>::KFD / 4];
 #pragma unroll
                 for (int ks = 0; ks < C3<S>::KFD / 4; ks++) {
@@ -444,7 +449,10 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
                         const int a = 8 * b + 2 * gc + h;
-                        if (rv && a < NPV) Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = acc[b][h];
+                        if (rv && a < NPV) {
+                            Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = acc[b][h];
+                            if (lift) atomicAdd(&De[inode + NPV * (j + NCU * (a + NPV * m))], acc[b][h]);
+                        }
                     }
                 double acch[C3<S>::NTH][2];
 #pragma unroll
@@ -459,7 +467,10 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
 #pragma unroll
                     for (int h = 0; h < 2; h++) {
                         const int f2 = 8 * b + 2 * gc + h;
-                        if (rv && f2 < NDF) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[b][h];
+                        if (rv && f2 < NDF) {
+                            He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[b][h];
+                            if (lift) atomicAdd(&Fe[inode + NPV * (j + NCU * (m + NCH * f2))], acch[b][h]);
+                        }
                     }
             }
                 };
@@ -499,8 +510,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                 }
             }
             __syncthreads();
-            double* De = A.D + (size_t)e * N * N;
-            double* Fe = A.F + (size_t)e * N * NB;
+
             constexpr int MTD = (NPV * NCU * NCU + 7) / 8;
             for (int mt = warp; mt < MTD; mt += NT / 32) {
                 const int r = 8 * mt + gr;
@@ -558,40 +568,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                         }
                 }
             }
-            for (int fc = 0; fc < NFE; fc++) face_rows(fc, fnu, fnuh);
+            for (int fc = 0; fc < NFE; fc++) face_rows(fc, fnu, fnuh, true);
             __syncthreads();
-            // lifted trace terms, D += P K and F += P H (P: face dof -> element
-            // node), entry by entry in the face order of each node; U entries per
-            // thread are gathered before any is stored, so many loads are in flight
-            constexpr int TOT = N * (N + NB), U = 4;
-            for (int base = tid; base < TOT; base += U * NT) {
-                double v[U];
-#pragma unroll
-                for (int q = 0; q < U; q++) {
-                    const int t = base + q * NT;
-                    v[q] = 0.0;
-                    if (t < TOT) {
-                        const bool isD = t < N * N;
-                        const int u = isD ? t : t - N * N;
-                        const int i = u % NPV, j = (u / NPV) % NCU, col = u / N;
-                        const double* src = (isD ? Ke : He) + j + (size_t)NB * col;
-                        double x = isD ? De[u] : Fe[u];
-                        const int ni = sm.inc_n[i];
-#pragma unroll
-                        for (int c2 = 0; c2 < S::MAXINC; c2++)
-                            if (c2 < ni) x += src[NCH * sm.inc_f[i * S::MAXINC + c2]];
-                        v[q] = x;
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < U; q++) {
-                    const int t = base + q * NT;
-                    if (t < TOT) {
-                        if (t < N * N) De[t] = v[q];
-                        else Fe[t - N * N] = v[q];
-                    }
-                }
-            }
         }
         __syncthreads();
         double ru2 = 0.0;
@@ -618,7 +596,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
                     Rhe[j + NCH * (fc * NPF + ip)] = -s;
                     Roe[j + NCH * (fc * NPF + ip)] = -s;
                 }
-                face_rows(fc, fnub, fnuhb);
+                face_rows(fc, fnub, fnuhb, false);
             }
         }
     }
