@@ -150,25 +150,140 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         geometry<S>(T, sm.x, sm.jac, sm.Xx, sm.jacf, sm.nl);
         __syncthreads();
         qmatrices<S>(T, A.fc_q, sm.jac, sm.Xx, sm.jacf, sm.nl, M, Cm, Em);
-        for (int t = tid; t < NGV * NC; t += NT) {
-            const int g = t % NGV, c = t / NGV;
-            double s = 0.0;
-            for (int a = 0; a < NPV; a++) s += T.shapvt[g + NGV * a] * sm.u[a + NPV * c];
-            ug[t] = s;
-        }
-        for (int t = tid; t < NA * (NC + NCH); t += NT) {
-            const int gg = t % NA, c = t / NA, fc = gg / NGF, q = gg % NGF;
-            double s = 0.0;
-            if (c < NC) {
-                for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * sm.u[sm.perm[fc * NPF + m] + NPV * c];
-                ugf[gg + NA * c] = s;
-            } else {
-                for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * sm.uhe[fc * NPF + m + NDF * (c - NC)];
-                uhg[gg + NA * (c - NC)] = s;
+        __syncthreads();
+        const double* P = A.pparam ? A.pparam + 8 * A.eprob[e] : A.param;
+        const int tdep = A.pparam ? (int)P[6] : A.tdep;
+        const double fc_u = A.pparam ? P[7] : A.fc_u;
+        const int* bfe = A.bf ? A.bf + (size_t)e * NFE : nullptr;
+        // warp 0 factors M while the other warps evaluate the states at the points
+        // and the pointwise fluxes, which do not depend on M
+        if (warp == 0) {
+            cholesky_warp<NPV>(M);
+        } else {
+            constexpr int NT1 = NT - 32;
+            const int tid1 = tid - 32;
+            for (int t = tid1; t < NGV * NC; t += NT1) {
+                const int g = t % NGV, c = t / NGV;
+                double s = 0.0;
+                for (int a = 0; a < NPV; a++) s += T.shapvt[g + NGV * a] * sm.u[a + NPV * c];
+                ug[t] = s;
+            }
+            for (int t = tid1; t < NA * (NC + NCH); t += NT1) {
+                const int gg = t % NA, c = t / NA, fc = gg / NGF, q = gg % NGF;
+                double s = 0.0;
+                if (c < NC) {
+                    for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * sm.u[sm.perm[fc * NPF + m] + NPV * c];
+                    ugf[gg + NA * c] = s;
+                } else {
+                    for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * sm.uhe[fc * NPF + m + NDF * (c - NC)];
+                    uhg[gg + NA * (c - NC)] = s;
+                }
+            }
+            asm volatile("bar.sync 1, %0;" ::"r"(NT1) : "memory");
+            // pointwise fluxes: one work item per (point, differentiated variable k);
+            // a one-derivative dual pass gives f and df/dw_k at that point.
+            for (int t = tid1; t < (NGV + NA) * NC; t += NT1) {
+                using DD = Dual<1>;
+                const int p = t % (NGV + NA), k = t / (NGV + NA);
+                const bool vol = p < NGV;
+                const int g = vol ? p : p - NGV;
+                DD w[NC], f[ND * NCU];
+#pragma unroll
+                for (int c = 0; c < NC; c++) {
+                    const double val = vol ? ug[g + NGV * c] : ((c < NCU) ? uhg[g + NA * c] : ugf[g + NA * c]);
+                    w[c].v = val;
+                    w[c].d[0] = (c == k) ? 1.0 : 0.0;
+                }
+                ns_flux_dual<ND>(P, w, f, !A.inviscid);
+                if (vol) {
+                    const double jg = sm.jac[g];
+#pragma unroll
+                    for (int j = 0; j < NCU; j++) {
+                        if (k == 0) {
+                            double s = 0.0;
+                            if (tdep) {
+                                double tt = 0.0;
+                                for (int a = 0; a < NPV; a++) tt += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
+                                s = tt - ug[g + NGV * j] * fc_u;
+                            }
+                            sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
+#pragma unroll
+                            for (int m = 0; m < ND; m++) {
+                                double fx = 0.0;
+#pragma unroll
+                                for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
+                                sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
+                            }
+                        }
+                        const double su = (tdep && k == j) ? -fc_u : 0.0;
+                        wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
+#pragma unroll
+                        for (int m = 0; m < ND; m++) {
+                            double tt = 0.0;
+#pragma unroll
+                            for (int d = 0; d < ND; d++) tt += f[d * NCU + j].d[0] * sm.Xx[g + NGV * (d + ND * m)];
+                            wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -tt;
+                        }
+                    }
+                } else {
+                    // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
+                    const double tau = P[5];
+                    const double jf = sm.jacf[g];
+#pragma unroll
+                    for (int j = 0; j < NCU; j++) {
+                        if (k == 0) {
+                            double tt = tau * (ugf[g + NA * j] - uhg[g + NA * j]);
+#pragma unroll
+                            for (int d = 0; d < ND; d++) tt += f[d * NCU + j].v * sm.nl[g + NA * d];
+                            sm.fn[g + NA * j] = tt * jf;
+                        }
+                        double dn = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[0] * sm.nl[g + NA * d];
+                        if (k < NCU) {
+                            fnuh[g + NA * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
+                            fnu[g + NA * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
+                        } else {
+                            fnu[g + NA * (j + NCH * k)] = dn * jf;
+                        }
+                    }
+                }
+            }
+            // boundary faces: fb and its Jacobians at their points (one item per point and variable)
+            if (bfe) {
+                for (int t = tid1; t < NFE * NGF * (NC + NCH); t += NT1) {
+                    const int fc = t / (NGF * (NC + NCH)), r = t % (NGF * (NC + NCH));
+                    if (bfe[fc] >= 0) continue;
+                    using DD = Dual<1>;
+                    const int q = r % NGF, k = r / NGF, gg = q + NGF * fc;
+                    DD w[NC], uhd[NCH], fb[NCH];
+#pragma unroll
+                    for (int c = 0; c < NC; c++) {
+                        w[c].v = ugf[gg + NA * c];
+                        w[c].d[0] = (c == k) ? 1.0 : 0.0;
+                    }
+#pragma unroll
+                    for (int c = 0; c < NCH; c++) {
+                        uhd[c].v = uhg[gg + NA * c];
+                        uhd[c].d[0] = (NC + c == k) ? 1.0 : 0.0;
+                    }
+                    double nlq[ND];
+#pragma unroll
+                    for (int d = 0; d < ND; d++) nlq[d] = sm.nl[gg + NA * d];
+                    const int ib = -bfe[fc] - 1;
+                    if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb, !A.inviscid)) {
+                        for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
+                    }
+                    const double jf = sm.jacf[gg];
+#pragma unroll
+                    for (int j = 0; j < NCH; j++) {
+                        if (k == 0) fnb[gg + NA * j] = fb[j].v * jf;
+                        if (k < NC) fnub[gg + NA * (j + NCH * k)] = fb[j].d[0] * jf;
+                        else fnuhb[gg + NA * (j + NCH * (k - NC))] = fb[j].d[0] * jf;
+                    }
+                }
             }
         }
-        __syncthreads();
-        cholesky_warp<NPV>(M);
         __syncthreads();
         for (int t = tid; t < NPV * ND + NDF * ND; t += NT) {
             double* col = (t < NPV * ND) ? &Cm[NPV * t] : &Em[NPV * (t - NPV * ND)];
@@ -198,113 +313,6 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
             double s = 0.0;
             for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * Em[sm.perm[fc * NPF + m] + NPV * fd];
             sMiEf[t] = s;
-        }
-        const double* P = A.pparam ? A.pparam + 8 * A.eprob[e] : A.param;
-        const int tdep = A.pparam ? (int)P[6] : A.tdep;
-        const double fc_u = A.pparam ? P[7] : A.fc_u;
-        // pointwise fluxes: one work item per (point, differentiated variable k);
-        // a one-derivative dual pass gives f and df/dw_k at that point.
-        for (int t = tid; t < (NGV + NA) * NC; t += NT) {
-            using DD = Dual<1>;
-            const int p = t % (NGV + NA), k = t / (NGV + NA);
-            const bool vol = p < NGV;
-            const int g = vol ? p : p - NGV;
-            DD w[NC], f[ND * NCU];
-#pragma unroll
-            for (int c = 0; c < NC; c++) {
-                const double val = vol ? ug[g + NGV * c] : ((c < NCU) ? uhg[g + NA * c] : ugf[g + NA * c]);
-                w[c].v = val;
-                w[c].d[0] = (c == k) ? 1.0 : 0.0;
-            }
-            ns_flux_dual<ND>(P, w, f, !A.inviscid);
-            if (vol) {
-                const double jg = sm.jac[g];
-#pragma unroll
-                for (int j = 0; j < NCU; j++) {
-                    if (k == 0) {
-                        double s = 0.0;
-                        if (tdep) {
-                            double tt = 0.0;
-                            for (int a = 0; a < NPV; a++) tt += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
-                            s = tt - ug[g + NGV * j] * fc_u;
-                        }
-                        sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
-#pragma unroll
-                        for (int m = 0; m < ND; m++) {
-                            double fx = 0.0;
-#pragma unroll
-                            for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
-                            sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
-                        }
-                    }
-                    const double su = (tdep && k == j) ? -fc_u : 0.0;
-                    wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
-#pragma unroll
-                    for (int m = 0; m < ND; m++) {
-                        double tt = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++) tt += f[d * NCU + j].d[0] * sm.Xx[g + NGV * (d + ND * m)];
-                        wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -tt;
-                    }
-                }
-            } else {
-                // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
-                const double tau = P[5];
-                const double jf = sm.jacf[g];
-#pragma unroll
-                for (int j = 0; j < NCU; j++) {
-                    if (k == 0) {
-                        double tt = tau * (ugf[g + NA * j] - uhg[g + NA * j]);
-#pragma unroll
-                        for (int d = 0; d < ND; d++) tt += f[d * NCU + j].v * sm.nl[g + NA * d];
-                        sm.fn[g + NA * j] = tt * jf;
-                    }
-                    double dn = 0.0;
-#pragma unroll
-                    for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[0] * sm.nl[g + NA * d];
-                    if (k < NCU) {
-                        fnuh[g + NA * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
-                        fnu[g + NA * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
-                    } else {
-                        fnu[g + NA * (j + NCH * k)] = dn * jf;
-                    }
-                }
-            }
-        }
-        // boundary faces: fb and its Jacobians at their points (one item per point and variable)
-        const int* bfe = A.bf ? A.bf + (size_t)e * NFE : nullptr;
-        if (bfe) {
-            for (int t = tid; t < NFE * NGF * (NC + NCH); t += NT) {
-                const int fc = t / (NGF * (NC + NCH)), r = t % (NGF * (NC + NCH));
-                if (bfe[fc] >= 0) continue;
-                using DD = Dual<1>;
-                const int q = r % NGF, k = r / NGF, gg = q + NGF * fc;
-                DD w[NC], uhd[NCH], fb[NCH];
-#pragma unroll
-                for (int c = 0; c < NC; c++) {
-                    w[c].v = ugf[gg + NA * c];
-                    w[c].d[0] = (c == k) ? 1.0 : 0.0;
-                }
-#pragma unroll
-                for (int c = 0; c < NCH; c++) {
-                    uhd[c].v = uhg[gg + NA * c];
-                    uhd[c].d[0] = (NC + c == k) ? 1.0 : 0.0;
-                }
-                double nlq[ND];
-#pragma unroll
-                for (int d = 0; d < ND; d++) nlq[d] = sm.nl[gg + NA * d];
-                const int ib = -bfe[fc] - 1;
-                if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb, !A.inviscid)) {
-                    for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
-                }
-                const double jf = sm.jacf[gg];
-#pragma unroll
-                for (int j = 0; j < NCH; j++) {
-                    if (k == 0) fnb[gg + NA * j] = fb[j].v * jf;
-                    if (k < NC) fnub[gg + NA * (j + NCH * k)] = fb[j].d[0] * jf;
-                    else fnuhb[gg + NA * (j + NCH * (k - NC))] = fb[j].d[0] * jf;
-                }
-            }
         }
         __syncthreads();
 
