@@ -44,7 +44,7 @@ struct V2 {
     static constexpr int MTF = (S::NPF + 7) / 8;              // m-tiles of shapfg
     static constexpr int KV = ((S::NQ + 3) / 4) * 4;          // padded k of shapvg
     static constexpr int KF = ((S::NGF + 3) / 4) * 4;         // padded k of shapfg
-    static constexpr int LDAV = ((8 * MTV + 11) / 16) * 16 + 4;
+    static constexpr int LDAV = S::NPV | 1;                   // odd: lanes along q hit distinct banks
     static constexpr int LDAF = ((8 * MTF + 11) / 16) * 16 + 4;
     static constexpr int QSZ = S::NPV * S::NPV * (1 + S::ND) + S::NPV * S::NDF * S::ND + S::NGV * S::NC +
                                S::NA * (S::NC + S::NCH);
