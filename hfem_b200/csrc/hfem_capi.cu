@@ -26,6 +26,7 @@
 #include "schur_tc.cuh"
 #include "bilu0.cuh"
 #include "inverse_blocked.cuh"
+#include "schur_fused.cuh"
 
 using namespace hfem;
 
@@ -124,6 +125,9 @@ struct Launch {
     size_t tc_smem;
     const void* tc_fn;
     void (*scatter_h)(dim3, cudaStream_t, const ScatterArgs&);
+    void (*schur_fused)(cudaStream_t, int, const double*, const double*, const double*, double*, double*);
+    size_t fused_smem;
+    const void* fused_fn;
 };
 
 template <int N>
@@ -146,6 +150,22 @@ void launch_scatter_h(dim3 g, cudaStream_t st, const ScatterArgs& a) {
 template <class S>
 void launch_schur_tc(dim3 g, size_t sm, cudaStream_t st, const SchurTcArgs& a) {
     schur_tc_kernel<S::N, S::NB><<<g, TC_THREADS, sm, st>>>(a);
+}
+
+// strip width and warps of the fused FP64 condensation per shape
+template <class S>
+struct FusedPick {
+    static constexpr int BN = S::NB >= 40 ? 40 : ((S::NB + 7) / 8) * 8;
+    static constexpr int MT = (S::N + 7) / 8;
+    static constexpr int NW = MT >= 4 ? 4 : MT;
+    using Cfg = FusedCfg<S::N, S::NB, BN, NW>;
+};
+template <class S>
+void launch_schur_fused(cudaStream_t st, int ne, const double* Dinv, const double* F, const double* K, double* H,
+                        double* DinvF) {
+    using P = FusedPick<S>;
+    schur_fused_kernel<S::N, S::NB, P::BN, P::NW>
+        <<<(unsigned)(ne * P::Cfg::STRIPS), P::Cfg::THREADS, P::Cfg::SMEM, st>>>(ne, Dinv, F, K, H, DinvF);
 }
 
 template <class S>
@@ -176,6 +196,9 @@ Launch make_launch() {
     L.tc_smem = TcCfg<S::N, S::NB>::SMEM;
     L.tc_fn = (const void*)schur_tc_kernel<S::N, S::NB>;
     L.scatter_h = launch_scatter_h<S>;
+    L.schur_fused = launch_schur_fused<S>;
+    L.fused_smem = FusedPick<S>::Cfg::SMEM;
+    L.fused_fn = (const void*)schur_fused_kernel<S::N, S::NB, FusedPick<S>::BN, FusedPick<S>::NW>;
     return L;
 }
 
@@ -520,7 +543,13 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
             c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
-        if (c->precision == 0) {
+        if (c->precision == 0 && c->g1_sel < 0 && c->g2_sel < 0) {
+            // both products in one kernel (tilings chosen by hfem_set_gemm_tiles
+            // or hfem_autotune run the two batched GEMMs instead)
+            Timed t(c, "schur_fused");
+            c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
+            if ((rc = check_launch(c, "schur_fused"))) return rc;
+        } else if (c->precision == 0) {
             const GemmLaunch& g1 = c->g1_sel >= 0 ? gemm_candidates()[c->g1_sel] : c->L->g1;
             const GemmLaunch& g2 = c->g2_sel >= 0 ? gemm_candidates()[c->g2_sel] : c->L->g2;
             {
@@ -1392,6 +1421,7 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
     cudaFuncSetAttribute(L.tc_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.tc_smem);
+    cudaFuncSetAttribute(L.fused_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.fused_smem);
     for (const GemmLaunch& g : gemm_candidates())
         cudaFuncSetAttribute(g.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
     occ = 0;
