@@ -309,8 +309,11 @@ int fail(hfem_ctx* c, int code, const char* fmt, ...) {
 // cudaMalloc trims and retries once.
 struct DevicePool {
     std::mutex m;
+    std::mutex trim;                                              // held while cached blocks are released
     std::map<std::pair<int, size_t>, std::vector<void*>> free;   // (device, class) -> idle blocks
     std::map<void*, std::pair<int, size_t>> live;                // block -> (device, class)
+    std::map<int, size_t> cached_on;                              // device -> idle bytes
+    std::map<int, size_t> cap;                                    // device -> most idle bytes kept
     size_t cached = 0;
 };
 
@@ -330,15 +333,21 @@ size_t size_class(size_t bytes) {
     return (bytes + step - 1) / step * step;
 }
 
+// Releases the idle blocks of one device (all devices: -1).  The releases run
+// under P.trim, so a thread whose allocation failed while another thread was
+// releasing waits for those releases before it retries.
 size_t pool_trim_device(int device) {
     DevicePool& P = pool();
+    std::lock_guard<std::mutex> t(P.trim);
     std::vector<void*> drop;
     {
         std::lock_guard<std::mutex> g(P.m);
         for (auto it = P.free.begin(); it != P.free.end();) {
             if (device < 0 || it->first.first == device) {
                 for (void* q : it->second) drop.push_back(q);
-                P.cached -= it->first.second * it->second.size();
+                const size_t b = it->first.second * it->second.size();
+                P.cached -= b;
+                P.cached_on[it->first.first] -= b;
                 it = P.free.erase(it);
             } else {
                 ++it;
@@ -347,6 +356,18 @@ size_t pool_trim_device(int device) {
     }
     for (void* q : drop) cudaFree(q);
     return drop.size();
+}
+
+// Idle bytes the pool keeps per device: a quarter of its memory, so a long
+// run of contexts of changing sizes cannot park the whole device in the cache.
+size_t pool_cap(int device) {
+    DevicePool& P = pool();
+    auto it = P.cap.find(device);
+    if (it != P.cap.end()) return it->second;
+    cudaDeviceProp prop;
+    const size_t c = cudaGetDeviceProperties(&prop, device) == cudaSuccess ? prop.totalGlobalMem / 4 : (size_t)8 << 30;
+    P.cap[device] = c;
+    return c;
 }
 
 cudaError_t pool_alloc(int device, void** p, size_t bytes) {
@@ -359,12 +380,13 @@ cudaError_t pool_alloc(int device, void** p, size_t bytes) {
             *p = it->second.back();
             it->second.pop_back();
             P.cached -= cls;
+            P.cached_on[device] -= cls;
             P.live[*p] = {device, cls};
             return cudaSuccess;
         }
     }
     cudaError_t e = cudaMalloc(p, cls);
-    if (e != cudaSuccess) {
+    for (int attempt = 0; e != cudaSuccess && attempt < 2; attempt++) {
         cudaGetLastError();
         pool_trim_device(device);
         e = cudaMalloc(p, cls);
@@ -383,10 +405,16 @@ void pool_free(void* p) {
         std::lock_guard<std::mutex> g(P.m);
         auto it = P.live.find(p);
         if (it != P.live.end()) {
-            P.free[it->second].push_back(p);
-            P.cached += it->second.second;
-            P.live.erase(it);
-            return;
+            const int dev = it->second.first;
+            const size_t cls = it->second.second;
+            if (P.cached_on[dev] + cls <= pool_cap(dev)) {
+                P.free[it->second].push_back(p);
+                P.cached += cls;
+                P.cached_on[dev] += cls;
+                P.live.erase(it);
+                return;
+            }
+            P.live.erase(it);      // over the cap: released at once
         }
     }
     cudaFree(p);

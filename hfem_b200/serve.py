@@ -28,12 +28,13 @@ from __future__ import annotations
 import math
 import time
 from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field, replace
 
 import numpy as np
 
 from .batch import BatchSolver
-from .core import HDGSolver
+from .core import HDGSolver, load_library
 from .gen.problem import ns2d_vortex
 
 
@@ -84,10 +85,11 @@ def build_problem(r: Request):
 
 def footprint_bytes(prob) -> int:
     """Device bytes one problem holds inside a context (the per-element
-    D, D^-1 F, K, H blocks dominate; Krylov basis of restart 50 per face)."""
+    D, F, D^-1 F, K, H blocks dominate; Krylov basis of restart 50 per face),
+    with 1/8 added for the allocator's size classes and per-context buffers."""
     n, nb, ne, nf, bsz = prob.n_local, prob.n_trace, prob.mesh.ne, prob.mesh.nf, prob.bsz
-    per_elem = 8 * (n * n + 2 * n * nb + nb * nb + 2 * n + 3 * nb + 3 * prob.master.npv * prob.nc)
-    per_face = 8 * (8 * bsz * bsz + 60 * bsz)
+    per_elem = 9 * (n * n + 3 * n * nb + nb * nb + 2 * n + 3 * nb + 3 * prob.master.npv * prob.nc)
+    per_face = 9 * (8 * bsz * bsz + 60 * bsz)
     return ne * per_elem + nf * per_face
 
 
@@ -131,9 +133,22 @@ class _Group:
         self.members = []        # requests in the current context, in pack order
         self.joining = []        # admitted, not yet packed
         self.solver = None
+        self.waited = 0          # group iterations the joining requests have waited
 
     def live(self):
         return [r for r in self.members if r.live]
+
+    def join_due(self, join_fraction, max_wait):
+        """Pack the joining requests now?  Always when nothing is live; else once
+        they hold join_fraction of the live elements or have waited max_wait
+        iterations (a repack costs about half an iteration, so admissions are
+        batched instead of repacking at every iteration boundary)."""
+        if not self.joining:
+            return False
+        live = sum(r.prob.mesh.ne for r in self.live())
+        if live == 0:
+            return True
+        return (sum(r.prob.mesh.ne for r in self.joining) >= join_fraction * live or self.waited >= max_wait)
 
     def retired_fraction(self):
         tot = sum(r.prob.mesh.ne for r in self.members)
@@ -155,31 +170,42 @@ class _Group:
                 r.cur = replace(r.cur, udg=udg[old.eoff[i]:old.eoff[i + 1]].copy(),
                                 uh=uh[old.hoff[i]:old.hoff[i + 1]].copy())
         t1 = time.perf_counter()
+        # in-flight states (u and uhat only, a small share of a context) are set
+        # aside on the device and the old context is closed before the new one is
+        # built, so a repack never holds two contexts' element blocks at once
+        saved = []
+        if old is not None and keep and on_device:
+            import torch
+            src_u, src_h = old.s.device_tensor("udg"), old.s.device_tensor("uh")
+            su = src_u.numel() // old.eoff[-1]
+            sh = src_h.numel() // old.hoff[-1]
+            for r in keep:
+                i = old_pos[id(r)]
+                saved.append((src_u[old.eoff[i] * su:old.eoff[i + 1] * su].clone(),
+                              src_h[old.hoff[i] * sh:old.hoff[i + 1] * sh].clone()))
+            torch.cuda.synchronize(device)
+        if old is not None:
+            old.close()
         self.members = keep + self.joining
         self.joining = []
+        self.waited = 0
         self.solver = None
         if self.members:
             # in-flight requests start from their packed state on the host side
             # and get their current state by device-to-device copies below
             self.solver = BatchSolver([r.cur for r in self.members], device=device, stream=stream)
-            if old is not None and keep and on_device:
+            if saved:
                 import torch
-                src_u, src_h = old.s.device_tensor("udg"), old.s.device_tensor("uh")
                 dst_u, dst_h = self.solver.s.device_tensor("udg"), self.solver.s.device_tensor("uh")
-                su = src_u.numel() // old.eoff[-1]
-                sh = src_h.numel() // old.hoff[-1]
-                for j, r in enumerate(keep):
-                    i = old_pos[id(r)]
-                    e0, e1, n0 = old.eoff[i], old.eoff[i + 1], self.solver.eoff[j]
-                    h0, h1, m0 = old.hoff[i], old.hoff[i + 1], self.solver.hoff[j]
-                    dst_u[n0 * su:(n0 + e1 - e0) * su].copy_(src_u[e0 * su:e1 * su])
-                    dst_h[m0 * sh:(m0 + h1 - h0) * sh].copy_(src_h[h0 * sh:h1 * sh])
+                for j, (u, h) in enumerate(saved):
+                    n0, m0 = self.solver.eoff[j], self.solver.hoff[j]
+                    dst_u[n0 * su:n0 * su + u.numel()].copy_(u)
+                    dst_h[m0 * sh:m0 * sh + h.numel()].copy_(h)
                 torch.cuda.synchronize(device)
+                del saved
             # q of joining requests from their (u, uhat); in-flight ones already
             # satisfy q = getQ(u, uhat), so recomputing them is a no-op up to rounding
             self.solver.s.getQ()
-        if old is not None:
-            old.close()
         if phases is not None:
             phases["repack_readback"] = phases.get("repack_readback", 0.0) + (t1 - t0)
             phases["repack_build"] = phases.get("repack_build", 0.0) + (time.perf_counter() - t1)
@@ -190,16 +216,38 @@ class _Group:
 
 
 def serve(requests, tol=1e-10, hbm_budget=None, max_newton=20, device=0, clock=time.perf_counter,
-          keep_states=False, stream=None, repack_fraction=0.5, gmres_tol=1e-10, restart=50, repack_on_device=True):
-    """Continuous batching over `requests` (sorted by arrival); returns ServeStats."""
+          keep_states=False, stream=None, repack_fraction=0.5, gmres_tol=1e-10, restart=50, repack_on_device=True,
+          join_fraction=0.5, max_wait=3, workers=3):
+    """Continuous batching over `requests` (sorted by arrival); returns ServeStats.
+
+    Admitted requests join their order's context at an iteration boundary: at
+    once (join_fraction 0, max_wait 0) or batched (the defaults) -- see
+    _Group.join_due.  `workers` host threads drive the orders' groups
+    concurrently (0: one after another)."""
     if hbm_budget is None:
+        import ctypes
         import torch
         free, _ = torch.cuda.mem_get_info(device)
-        hbm_budget = int(0.8 * free)
+        lib = load_library()
+        lib.hfem_pool_cached_bytes.restype = ctypes.c_longlong
+        lib.hfem_pool_cached_bytes.argtypes = []
+        # blocks idle in the library's pool are reclaimable: they count as free
+        hbm_budget = int(0.8 * (free + lib.hfem_pool_cached_bytes()))
     for r in requests:
         build_problem(r)
         r.live, r.iters, r.cur = True, 0, r.prob
     pending = deque(sorted(requests, key=lambda r: r.arrival))
+    pool = ThreadPoolExecutor(max_workers=workers) if workers and workers > 1 else None
+    try:
+        return _serve_loop(requests, pending, pool, tol, hbm_budget, max_newton, device, clock, keep_states, stream,
+                           repack_fraction, gmres_tol, restart, repack_on_device, join_fraction, max_wait)
+    finally:
+        if pool is not None:
+            pool.shutdown(wait=True)
+
+
+def _serve_loop(requests, pending, pool, tol, hbm_budget, max_newton, device, clock, keep_states, stream,
+                repack_fraction, gmres_tol, restart, repack_on_device, join_fraction, max_wait):
     groups = {}
     phases = {"repack": 0.0, "retire": 0.0, "assemble": 0.0, "gmres": 0.0, "gmres_iterations": 0, "line_search": 0.0}
     used = peak = 0
@@ -223,16 +271,31 @@ def serve(requests, tol=1e-10, hbm_budget=None, max_newton=20, device=0, clock=t
                 time.sleep(max(0.0, min(0.005, pending[0].arrival - now)))
             continue
         for g in busy:
-            if g.joining or g.retired_fraction() > repack_fraction:
+            if g.join_due(join_fraction, max_wait) or g.retired_fraction() > repack_fraction:
                 tr = time.perf_counter()
                 if g.solver is not None:
                     _merge(phases, g.solver.phases)
                 used -= g.repack(device, stream, phases, repack_on_device)
                 phases["repack"] += time.perf_counter() - tr
-            b = g.solver
+        # one Newton iteration of every busy group; each group's context has its
+        # own stream, and with `workers` each group is driven by its own host
+        # thread (the library calls release the interpreter lock), so the groups'
+        # launches and host round trips overlap
+        runs = []
+        for g in busy:
+            if g.joining:
+                g.waited += 1
             active = np.array([r.live for r in g.members])
             batch_sizes.append(int(active.sum()))
-            old, new = b.newton_iteration(tol, active, gmres_tol=gmres_tol, restart=restart)
+            runs.append((g, active))
+        if pool is not None and len(runs) > 1:
+            futs = [pool.submit(g.solver.newton_iteration, tol, a, gmres_tol=gmres_tol, restart=restart)
+                    for g, a in runs]
+            results = [f.result() for f in futs]
+        else:
+            results = [g.solver.newton_iteration(tol, a, gmres_tol=gmres_tol, restart=restart) for g, a in runs]
+        for (g, active), (old, new) in zip(runs, results):
+            b = g.solver
             iterations += 1
             finished = []
             for i, r in enumerate(g.members):

@@ -93,7 +93,9 @@ def _requests():
 
 def test_served_result_equals_alone():
     mix = _requests()
-    st = serve(mix, tol=1e-10, keep_states=True, clock=_StepClock(0.05), hbm_budget=1 << 34)
+    # immediate admission, so later arrivals join groups in flight
+    st = serve(mix, tol=1e-10, keep_states=True, clock=_StepClock(0.05), hbm_budget=1 << 34, join_fraction=0.0,
+               max_wait=0)
     assert st.completed == len(mix)
     alone = _requests()
     sequential(alone, tol=1e-10, keep_states=True, clock=_StepClock(100.0))
@@ -113,3 +115,16 @@ def test_admission_waits_for_memory():
     st = serve(mix, tol=1e-10, clock=_StepClock(0.05), hbm_budget=budget)
     assert st.completed == len(mix) and st.max_rnorm < 1e-10
     assert st.peak_bytes <= budget
+
+
+def test_served_result_equals_alone_batched_admission():
+    # the default policy: admissions batched, groups driven by concurrent host threads
+    mix = _requests()
+    st = serve(mix, tol=1e-10, keep_states=True, clock=_StepClock(0.05), hbm_budget=1 << 34)
+    assert st.completed == len(mix)
+    alone = _requests()
+    sequential(alone, tol=1e-10, keep_states=True, clock=_StepClock(100.0))
+    for a, m in zip(alone, mix):
+        assert a.rnorm < 1e-10 and m.rnorm < 1e-10, (a.rid, a.rnorm, m.rnorm)
+        assert _rel(m.udg, a.udg) < 1e-8, a.rid
+        assert _rel(m.uh, a.uh) < 1e-8, a.rid
