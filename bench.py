@@ -558,6 +558,7 @@ def run_batched_task(args):
                      "tiles": {f"{k[0]}d_p{k[1]}": v for k, v in m.tiles.items()}}
         if prec == 1:
             out[name]["dtype"] = "tf32 Schur GEMMs, f64 element LU / residual"
+            out[name]["fp64_shapes"] = [f"{k[0]}d_p{k[1]}" for k in m.fp64_shapes]
         m.close()
     out["value"] = out["graph_mixed"]["value"]
     out["speedup_graph_mixed_vs_plain_fp64"] = out["graph_mixed"]["value"] / out["plain_fp64"]["value"]

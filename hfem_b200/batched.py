@@ -74,7 +74,10 @@ def autotune(solver, key, device=0, reps=3, cache=CACHE, refresh=False):
 
 
 class MixedOrderAssembly:
-    """All meshes' assembly as one graph launch (one context per element shape)."""
+    """All meshes' assembly as one graph launch (one context per element shape).
+
+    precision 1 with tune: the TF32 condensation on the shapes where it is
+    faster than the tuned FP64 kernels (the others stay FP64, `fp64_shapes`)."""
 
     def __init__(self, probs, device=0, precision=0, tune=True, stream=None):
         import torch
@@ -86,12 +89,16 @@ class MixedOrderAssembly:
         self.keys = sorted(self.groups)
         self.solvers = []
         self.tiles = {}
+        self.fp64_shapes = []      # shapes left in FP64 by a mixed-precision build
         for k in self.keys:
             b = BatchSolver([probs[i] for i in self.groups[k]], device=device, stream=self.stream.cuda_stream)
-            b.s.set_precision(precision)
             b.s.getQ()
-            if tune and precision == 0:
+            if tune:
                 self.tiles[k] = autotune(b.s, f"{k[0]}d_p{k[1]}", device=device)[:2]
+            b.s.set_precision(precision)
+            if tune and precision == 1 and not self._tf32_pays(b):
+                b.s.set_precision(0)         # this shape's tuned FP64 condensation is faster
+                self.fp64_shapes.append(k)
             self.solvers.append(b)
         self.ne = sum(p.mesh.ne for p in probs)
         lib = _lib()
@@ -102,6 +109,22 @@ class MixedOrderAssembly:
             msg = lib.hfem_last_error(self.solvers[0].s.h).decode()
             raise HfemError(f"graph capture failed ({rc}): {msg}")
         self.graph = g
+
+    @staticmethod
+    def _tf32_pays(b, reps=2):
+        """Time the condensation of one shape both ways (the TF32 tensor-core
+        kernel against the tuned FP64 kernels); True when TF32 is faster."""
+        def cond_ms(prec):
+            b.s.set_precision(prec)
+            b.s.assembleLinearSystem()
+            b.s.set_timing(True)
+            for _ in range(reps):
+                b.s.assembleLinearSystem()
+            kt = b.s.kernel_times()
+            b.s.set_timing(False)
+            return sum(v[0] for k, v in kt.items() if k in ("schur_tc", "schur_fused", "gemm_DinvF", "gemm_schur"))
+        t_fp64, t_tf32 = cond_ms(0), cond_ms(1)
+        return t_tf32 < t_fp64
 
     def launch(self):
         """Enqueue one assembly pass over every mesh (one graph launch)."""

@@ -1993,6 +1993,18 @@ int hfem_autotune(hfem_ctx* c, int reps, int* best, double* ms) {
             if (ms) ms[which * cand.size() + k] = per;
             if (per < bt[which]) bt[which] = per, bi[which] = (int)k;
         }
+    // the fused kernel does both products: kept when it beats the best pair
+    {
+        c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);   // warm-up
+        if ((rc = check_launch(c, "autotune"))) return rc;
+        CK(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < reps; r++) c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
+        CK(cudaEventRecord(e1, c->stream));
+        CK(cudaEventSynchronize(e1));
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, e0, e1));
+        if ((double)t / reps <= bt[0] + bt[1]) bi[0] = bi[1] = -1;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->g1_sel = bi[0];

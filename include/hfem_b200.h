@@ -186,8 +186,10 @@ int hfem_assemble_finish(hfem_ctx* ctx, double* rnorm);
 
 /* Batched-GEMM tilings compiled into the library (any is valid for any
  * shape); hfem_autotune times them all on the context's own operands and
- * keeps the fastest for D^-1 F and for H - K D^-1 F (best[2], ms[2 * count]
- * may be NULL); hfem_set_gemm_tiles applies a stored choice (-1: default).
+ * keeps the fastest for D^-1 F and for H - K D^-1 F, or the fused kernel that
+ * does both (best = {-1, -1}) when it is faster than that pair (best[2],
+ * ms[2 * count] may be NULL; ms holds the pairs' timings);
+ * hfem_set_gemm_tiles applies a stored choice (-1, -1: the fused kernel).
  * No counterpart in the reference (its BLAS picks its own kernels). */
 int hfem_gemm_candidates(void);
 int hfem_autotune(hfem_ctx* ctx, int reps, int* best, double* ms);

@@ -65,7 +65,8 @@ def test_autotune_picks_valid_tilings(tmp_path):
     Hg0 = s.download("Hg")
     g1, g2, ms = autotune(s, "3d_p3", cache=str(tmp_path / "t.json"))
     assert ms is not None and np.all(ms > 0)
-    assert ms[0, g1] == ms[0].min() and ms[1, g2] == ms[1].min()
+    if (g1, g2) != (-1, -1):         # (-1, -1): the fused kernel beat the best pair
+        assert ms[0, g1] == ms[0].min() and ms[1, g2] == ms[1].min()
     r = s.assembleLinearSystem()
     assert abs(r - ref) <= 1e-13 * ref
     assert np.max(np.abs(s.download("Hg") - Hg0)) <= 1e-13 * np.max(np.abs(Hg0))
