@@ -8,8 +8,9 @@ assembly + static condensation + scatter into the face-block system
 (assembleLinearSystem), with the solution resident on the device.
 
   metric  assembly+Schur elements/s (FP64), whole job (sum over GPUs)
-  e2e     the same step through the C ABI with the state copied from pinned
-          host memory every step and the residual norm read back
+  e2e     the same step through the C ABI (hfem_assemble_host) with the state
+          copied from pinned host memory every step, the copies overlapped with
+          the element kernel piece by piece, and the residual norm read back
   roofline of the dominant kernel against the measured FP64 roof
   cpu_baseline  the reference's own C++ (oracle/_ref/hfem_ref, built from the
           reference sources) on the host cores, as a reported baseline
@@ -225,16 +226,9 @@ def run_gpu(args, rank, world, local_rank):
     h_udg = torch.from_numpy(np.ascontiguousarray(udg_q)).pin_memory()
     h_uh = torch.from_numpy(np.ascontiguousarray(uh0)).pin_memory()
     h_sh = torch.from_numpy(np.ascontiguousarray(prob.sh)).pin_memory()
-    import ctypes as C
-    lib = solver.lib
-    dp = C.POINTER(C.c_double)
-
     def e2e_step():
-        rc = lib.hfem_set_solution(solver.h, C.cast(h_udg.data_ptr(), dp), C.cast(h_uh.data_ptr(), dp),
-                                   C.cast(h_sh.data_ptr(), dp))
-        if rc != 0:
-            raise RuntimeError(lib.hfem_last_error(solver.h).decode())
-        return solver.assembleLinearSystem()
+        # hfem_assemble_host: the state's copies overlap the element kernel piece by piece
+        return solver.assemble_from_host(h_udg.data_ptr(), h_uh.data_ptr(), h_sh.data_ptr(), chunks=args.e2e_chunks)
 
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
@@ -576,6 +570,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (TF32 Schur) leg")
+    ap.add_argument("--e2e-chunks", type=int, default=8, help="pieces of the element-wise state copied ahead of the element kernel in the e2e leg")
     ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve", "batched"])
     ap.add_argument("--batched-meshes", type=int, default=64)
     ap.add_argument("--precond", type=int, default=2, choices=[-1, 0, 2],

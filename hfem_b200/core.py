@@ -56,6 +56,7 @@ def load_library(path: str = LIB):
     lib.hfem_set_physics.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_double]
     lib.hfem_set_solution.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.hfem_set_solution_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.hfem_assemble_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double)]
     lib.hfem_get_solution.argtypes = [C.c_void_p, _dp, _dp]
     lib.hfem_getq.argtypes = [C.c_void_p]
     lib.hfem_assemble.argtypes = [C.c_void_p, _dp]
@@ -196,6 +197,16 @@ class HDGSolver:
     def assembleLinearSystem(self):
         rn = C.c_double()
         self._chk(self.lib.hfem_assemble(self.h, C.byref(rn)), "assembleLinearSystem")
+        return rn.value
+
+    def assemble_from_host(self, udg_ptr, uh_ptr, sh_ptr=None, chunks=4):
+        """set_solution + assembleLinearSystem with the host-to-device copies of
+        the element-wise state overlapped with the element kernel (pointers to
+        host memory, pinned for the overlap; e.g. torch pinned tensors' data_ptr)."""
+        rn = C.c_double()
+        self._chk(self.lib.hfem_assemble_host(self.h, C.c_void_p(udg_ptr), C.c_void_p(uh_ptr),
+                                              C.c_void_p(sh_ptr) if sh_ptr else None, int(chunks), C.byref(rn)),
+                  "assemble_host")
         return rn.value
 
     def computeResidualNorm(self):

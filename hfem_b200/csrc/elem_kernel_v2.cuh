@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel_v2(ElemArgs A) {
         }
     }
 
-    for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
+    for (int e = A.e_begin + blockIdx.x; e < A.ne; e += gridDim.x) {
         __syncthreads();
         const double* xg = A.dgnodes + (size_t)e * NPV * ND;
         const double* ugl = A.udg + (size_t)e * NPV * NC;

@@ -68,6 +68,7 @@ struct ElemArgs {
     const int* bcm;
     const double* bcs;
     int inviscid;               // 1: Euler flux (app.appname 0)
+    int e_begin = 0;            // element range [e_begin, ne) of this launch (element_kernel_v2)
 };
 
 constexpr int NT = 256;         // threads per CTA for element kernels

@@ -222,6 +222,12 @@ struct hfem_ctx {
     std::string err;
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
     int grid_elem = 0, grid_schur = 0, grid_inv = 0, grid_tc = 0;
+    // element-wise state arriving in pieces (hfem_assemble_host): the element
+    // kernel of piece k waits for chunk_ev[k]
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;
+    std::vector<int> chunk_lo;              // first element of each piece, plus ne
+    int pending_chunks = 0;
     int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
     int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
     // boundary faces (mesh.bf, app.bcm, app.bcs); bf == NULL: no boundary faces
@@ -560,8 +566,21 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
     const dim3 ge(c->grid_elem);
     {
         Timed t(c, "element");
-        c->L->element2(ge, c->L->elem2_smem, c->stream, elem_args(c));
-        if ((rc = check_launch(c, "element"))) return rc;
+        if (c->pending_chunks > 0) {
+            // one launch per piece of the state, each after that piece's copy
+            for (int k = 0; k < c->pending_chunks; k++) {
+                CK(cudaStreamWaitEvent(c->stream, c->chunk_ev[k + 1], 0));
+                ElemArgs a = elem_args(c);
+                a.e_begin = c->chunk_lo[k];
+                a.ne = c->chunk_lo[k + 1];
+                c->L->element2(ge, c->L->elem2_smem, c->stream, a);
+                if ((rc = check_launch(c, "element"))) return rc;
+            }
+            c->pending_chunks = 0;
+        } else {
+            c->L->element2(ge, c->L->elem2_smem, c->stream, elem_args(c));
+            if ((rc = check_launch(c, "element"))) return rc;
+        }
     }
     ScatterArgs sa = scatter_args(c);
     if (matrix) {
@@ -1494,6 +1513,8 @@ int hfem_destroy(hfem_ctx* c) {
         cudaEventDestroy(p.second.second);
     }
     if (c->bilu_exec) cudaGraphExecDestroy(c->bilu_exec);
+    for (cudaEvent_t ev : c->chunk_ev) cudaEventDestroy(ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
     return 0;
@@ -1679,6 +1700,51 @@ int hfem_set_solution(hfem_ctx* c, const double* udg, const double* uh, const do
     if (rc) return rc;
     CK(cudaStreamSynchronize(c->stream));
     return 0;
+}
+
+int hfem_assemble_host(hfem_ctx* c, const double* udg, const double* uh, const double* sh, int chunks,
+                       double* rnorm) {
+    if (!c || !udg || !uh || chunks < 1) return c ? fail(c, HFEM_E_ARG, "null array or chunks < 1") : HFEM_E_ARG;
+    const hfem_dims& d = c->dims;
+    const size_t per_e = (size_t)d.npv * c->nc, nuh = (size_t)d.nf * c->bsz;
+    chunks = std::max(1, std::min(chunks, d.ne));
+    int rc;
+    CK(cudaSetDevice(c->device));
+    if (!c->udg) {
+        if ((rc = dalloc(c, &c->udg, d.ne * per_e)) || (rc = dalloc(c, &c->uh, nuh)) ||
+            (rc = dalloc(c, &c->sh, d.ne * per_e)))
+            return rc;
+    }
+    if (!c->copy_stream) CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    while ((int)c->chunk_ev.size() < chunks + 1) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        c->chunk_ev.push_back(ev);
+    }
+    // the copies overwrite the state only after the work queued before them
+    CK(cudaEventRecord(c->chunk_ev[0], c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->chunk_ev[0], 0));
+    CK(cudaMemcpyAsync(c->uh, uh, sizeof(double) * nuh, cudaMemcpyHostToDevice, c->copy_stream));
+    c->chunk_lo.assign(chunks + 1, 0);
+    for (int k = 0; k < chunks; k++) {
+        const int e0 = (int)((long long)d.ne * k / chunks), e1 = (int)((long long)d.ne * (k + 1) / chunks);
+        c->chunk_lo[k] = e0;
+        c->chunk_lo[k + 1] = e1;
+        const size_t off = (size_t)e0 * per_e, cnt = (size_t)(e1 - e0) * per_e;
+        CK(cudaMemcpyAsync(c->udg + off, udg + off, sizeof(double) * cnt, cudaMemcpyHostToDevice, c->copy_stream));
+        if (sh) CK(cudaMemcpyAsync(c->sh + off, sh + off, sizeof(double) * cnt, cudaMemcpyHostToDevice, c->copy_stream));
+        else CK(cudaMemsetAsync(c->sh + off, 0, sizeof(double) * cnt, c->copy_stream));
+        CK(cudaEventRecord(c->chunk_ev[k + 1], c->copy_stream));
+    }
+    c->pending_chunks = chunks;
+    c->have_sol = true;
+    c->assembled = false;
+    rc = run_assembly(c, true, rnorm);
+    if (rc) {
+        c->pending_chunks = 0;
+        cudaStreamSynchronize(c->copy_stream);
+    }
+    return rc;
 }
 
 int hfem_set_solution_device(hfem_ctx* c, const double* udg, const double* uh, const double* sh) {

@@ -96,6 +96,15 @@ int hfem_get_solution(hfem_ctx* ctx, double* udg, double* uh);
 /* Same, with device pointers already on the context's device. */
 int hfem_set_solution_device(hfem_ctx* ctx, const double* udg, const double* uh, const double* sh);
 
+/* hfem_set_solution followed by hfem_assemble, with the copies overlapped: uh
+ * first, then udg and sh in `chunks` pieces of elements on a second stream; the
+ * element kernel of each piece starts as soon as that piece has arrived (the
+ * host arrays should be pinned for the copies to run asynchronously).  Same
+ * results as the two calls.  No counterpart in the reference (its state is
+ * already in host memory). */
+int hfem_assemble_host(hfem_ctx* ctx, const double* udg, const double* uh, const double* sh, int chunks,
+                       double* rnorm);
+
 /* q from (u, uh) on every element.  Replaces getQ
  * (assembly/elementassembly.cpp:1414-1479) as called by solveProblem
  * (solvers/dgsolvers.cpp:464-474). */
