@@ -228,6 +228,9 @@ struct hfem_ctx {
     std::vector<cudaEvent_t> chunk_ev;
     std::vector<int> chunk_lo;              // first element of each piece, plus ne
     int pending_chunks = 0;
+    double* seg_partk = nullptr;            // CGS2 partial dots, npieces x (restart + 1)
+    size_t seg_partk_n = 0;
+    int seg_hP = 0;
     int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
     int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
     // boundary faces (mesh.bf, app.bcm, app.bcs); bf == NULL: no boundary faces
@@ -1181,14 +1184,29 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
     if ((rc = ensure_krylov(c, restart))) return rc;
     const int P = single ? 1 : c->nprob;
     const unsigned char* mv_act = single ? nullptr : c->seg_act;   // row -> problem map only with a problem map
-    if (c->seg_restart < restart) {
-        if ((rc = dalloc(c, &c->seg_h, (size_t)(restart + 2) * P))) return rc;
+    if (c->seg_restart < restart || c->seg_hP < P) {
+        // Hessenberg column (restart + 2 rows) and the second projection of
+        // CGS2 (restart + 1 rows), P problems each
+        if ((rc = dalloc(c, &c->seg_h, (size_t)(2 * restart + 3) * P))) return rc;
         if ((rc = dalloc(c, &c->seg_y, (size_t)restart * P))) return rc;
         c->seg_restart = restart;
+        c->seg_hP = P;
     }
     const long long n = nvec(c);
     const int g = sms(c->device) * 4;
     const bool prec = precond == 2;
+    // classical Gram-Schmidt with one reorthogonalisation (CGS2): 5 launches per
+    // Arnoldi step instead of j + 3 for modified Gram-Schmidt.  It wins while
+    // the steps are launch-bound, for small systems (measured on B200: 2D p=2,
+    // 37k unknowns, 9.1 -> 5.9 ms per 62 steps); for larger ones the fused MGS
+    // steps, which move the same bytes with more memory parallelism, win (3D
+    // p=3, 2.5M unknowns: 33 ms with MGS, 75 ms with CGS2 per 69 steps; batches
+    // of 2D requests, 0.3-2M unknowns, were slower with CGS2 too).
+    const bool cgs2 = restart + 1 <= 64 && n <= (1ll << 17);
+    if (cgs2 && c->seg_partk_n < (size_t)c->npieces * (restart + 1)) {
+        if ((rc = dalloc(c, &c->seg_partk, (size_t)c->npieces * (restart + 1)))) return rc;
+        c->seg_partk_n = (size_t)c->npieces * (restart + 1);
+    }
     if (prec) {
         Timed t(c, "bj_inverse");
         const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
@@ -1215,6 +1233,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
     const SegPieces SP{c->npieces, c->seg_pstart, c->seg_pseg, c->seg_p0, c->seg_ticket, c->seg_part, c->seg_act};
     const int np = c->npieces;
     double* d_h = c->seg_h;                   // Hessenberg column, entry (i, p) at i * P + p
+    double* d_h2 = c->seg_h + (size_t)(restart + 2) * P;   // CGS2's second projection, same layout
     std::vector<unsigned char> act(P, 1);
     auto set_act = [&]() -> int {
         CK(cudaMemcpyAsync(c->seg_act, act.data(), P, cudaMemcpyHostToDevice, c->stream));
@@ -1225,7 +1244,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
     };
     if ((rc = set_act())) return rc;
     axpy_dot(nullptr, nullptr, c->pb, c->pb, c->seg_nrm, 1);
-    std::vector<double> nrmb(P), beta(P), hcol((size_t)(restart + 2) * P);
+    std::vector<double> nrmb(P), beta(P), hcol((size_t)(restart + 2) * P), h2col((size_t)(restart + 1) * P);
     CK(cudaMemcpyAsync(nrmb.data(), c->seg_nrm, sizeof(double) * P, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     for (double& v : nrmb)
@@ -1267,16 +1286,31 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
             if ((rc = matvec_warp(c, vj, vn, prec, mv_act))) return rc;
             {
                 Timed t(c, "orthogonalise_seg");
-                for (int i = 0; i <= j; i++)
-                    axpy_dot(i ? d_h + (size_t)(i - 1) * P : nullptr, i ? c->V + (size_t)(i - 1) * n : nullptr, vn,
-                             c->V + (size_t)i * n, d_h + (size_t)i * P, 0);
-                axpy_dot(d_h + (size_t)j * P, vj, vn, vn, d_h + (size_t)(j + 1) * P, 1);
+                if (cgs2) {
+                    const int k = j + 1;
+                    seg_multidot_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, n, k, P, c->V, vn, c->seg_partk, d_h);
+                    seg_update_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, n, k, P, c->V, d_h, vn, nullptr);
+                    seg_multidot_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, n, k, P, c->V, vn, c->seg_partk,
+                                                                           d_h2);
+                    seg_update_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, n, k, P, c->V, d_h2, vn,
+                                                                         d_h + (size_t)(j + 1) * P);
+                } else {
+                    for (int i = 0; i <= j; i++)
+                        axpy_dot(i ? d_h + (size_t)(i - 1) * P : nullptr, i ? c->V + (size_t)(i - 1) * n : nullptr,
+                                 vn, c->V + (size_t)i * n, d_h + (size_t)i * P, 0);
+                    axpy_dot(d_h + (size_t)j * P, vj, vn, vn, d_h + (size_t)(j + 1) * P, 1);
+                }
                 seg_scale_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, d_h + (size_t)(j + 1) * P, vn, vn);
             }
             if ((rc = check_launch(c, "arnoldi"))) return rc;
             CK(cudaMemcpyAsync(hcol.data(), d_h, sizeof(double) * (size_t)(j + 2) * P, cudaMemcpyDeviceToHost,
                                c->stream));
+            if (cgs2)
+                CK(cudaMemcpyAsync(h2col.data(), d_h2, sizeof(double) * (size_t)(j + 1) * P, cudaMemcpyDeviceToHost,
+                                   c->stream));
             CK(cudaStreamSynchronize(c->stream));
+            if (cgs2)
+                for (size_t q = 0; q < (size_t)(j + 1) * P; q++) hcol[q] += h2col[q];
             bool changed = false;
             for (int p = 0; p < P; p++) {
                 if (!incycle[p]) continue;
@@ -1503,7 +1537,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
-                    c->seg_ticket, c->seg_part, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
+                    c->seg_ticket, c->seg_part, c->seg_partk, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
                     c->d_lvl_lo, c->d_lvl_up};
     for (void* p : ptrs)

@@ -89,6 +89,85 @@ __global__ void __launch_bounds__(SEG_THREADS) seg_axpy_dot_kernel(SegPieces P, 
     seg_finish(P, piece, seg, s, out, sq, red);
 }
 
+// Classical Gram-Schmidt projections, all at once:
+//   out[i * nseg + seg] = <V_i, w>  for i < k   (V_i: column i of stride n)
+// Each CTA keeps its piece of w in registers (SEG_PIECE / SEG_THREADS per
+// thread), reduces the k piece partials in a fixed tree into part[i * npieces +
+// piece], and the last CTA of the segment sums them in piece order.
+__global__ void __launch_bounds__(SEG_THREADS) seg_multidot_kernel(SegPieces P, long long n, int k, int nseg,
+                                                                   const double* __restrict__ V,
+                                                                   const double* __restrict__ w,
+                                                                   double* __restrict__ partk,
+                                                                   double* __restrict__ out) {
+    constexpr int R = SEG_PIECE / SEG_THREADS;
+    __shared__ double red[SEG_THREADS / 32];
+    __shared__ int last;
+    const int piece = blockIdx.x;
+    const int seg = P.pseg[piece];
+    if (P.act && !P.act[seg]) return;
+    const long long i0 = P.pstart[piece], i1 = P.pstart[piece + 1];
+    double wr[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const long long idx = i0 + threadIdx.x + (long long)SEG_THREADS * r;
+        wr[r] = idx < i1 ? w[idx] : 0.0;
+    }
+    for (int i = 0; i < k; i++) {
+        const double* vi = V + (size_t)i * n;
+        double s = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const long long idx = i0 + threadIdx.x + (long long)SEG_THREADS * r;
+            if (idx < i1) s += vi[idx] * wr[r];
+        }
+        s = seg_block_sum(s, red);
+        if (threadIdx.x == 0) partk[(size_t)i * P.npieces + piece] = s;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const int need = P.seg_p0[seg + 1] - P.seg_p0[seg];
+        last = (atomicAdd(&P.ticket[seg], 1) == need - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int p0 = P.seg_p0[seg], p1 = P.seg_p0[seg + 1];
+    for (int i = 0; i < k; i++) {
+        double t = 0.0;
+        for (int q = p0 + threadIdx.x; q < p1; q += SEG_THREADS) t += __ldcg(&partk[(size_t)i * P.npieces + q]);
+        t = seg_block_sum(t, red);
+        if (threadIdx.x == 0) out[(size_t)i * nseg + seg] = t;
+    }
+    if (threadIdx.x == 0) P.ticket[seg] = 0;
+}
+
+// w -= sum_{i<k} h[i * nseg + seg] V_i, and with nrm != NULL also
+// nrm[seg] = |w| after the update (per-segment reduction as above).
+__global__ void __launch_bounds__(SEG_THREADS) seg_update_kernel(SegPieces P, long long n, int k, int nseg,
+                                                                 const double* __restrict__ V,
+                                                                 const double* __restrict__ h, double* w,
+                                                                 double* __restrict__ nrm) {
+    __shared__ double red[SEG_THREADS / 32];
+    __shared__ double hs[64];
+    const int piece = blockIdx.x;
+    const int seg = P.pseg[piece];
+    if (P.act && !P.act[seg]) return;
+    for (int i = threadIdx.x; i < k; i += SEG_THREADS) hs[i] = h[(size_t)i * nseg + seg];
+    __syncthreads();
+    const long long i0 = P.pstart[piece], i1 = P.pstart[piece + 1];
+    double s = 0.0;
+    for (long long idx = i0 + threadIdx.x; idx < i1; idx += SEG_THREADS) {
+        double a = 0.0;
+        for (int i = 0; i < k; i++) a += hs[i] * V[(size_t)i * n + idx];
+        const double v = w[idx] - a;
+        w[idx] = v;
+        s += v * v;
+    }
+    if (!nrm) return;
+    s = seg_block_sum(s, red);
+    seg_finish(P, piece, seg, s, nrm, 1, red);
+}
+
 // y = x / nrm[seg] where nrm[seg] != 0 (y may alias x).
 __global__ void __launch_bounds__(SEG_THREADS) seg_scale_kernel(SegPieces P, const double* __restrict__ nrm,
                                                                 const double* x, double* y) {
