@@ -989,6 +989,48 @@ int ensure_krylov(hfem_ctx* c, int restart) {
     return 0;
 }
 
+// Diagonal block of every face row -> contiguous blocks (for the blocked inverse).
+__global__ void gather_diag_kernel(int nrows, int b2, const int* __restrict__ rowstart, const double* __restrict__ Hg,
+                                   double* __restrict__ out) {
+    const long long tot = (long long)nrows * b2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x)
+        out[t] = Hg[(size_t)rowstart[t / b2] * b2 + t % b2];
+}
+
+template <int B>
+int bj_blocked(hfem_ctx* c) {
+    cudaFuncSetAttribute(inverse_blocked_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)InvBlk<B>::SMEM);
+    const int nf = c->dims.nf;
+    gather_diag_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(nf, B * B, c->rowstart, c->Hg, c->Minv);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, inverse_blocked_kernel<B>, InvBlk<B>::THREADS, InvBlk<B>::SMEM);
+    const int grid = std::max(1, std::min(nf, sms(c->device) * std::max(occ, 1)));
+    // the kernel also solves with a right-hand side: c->w is free here and its
+    // result is ignored
+    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->binfo);
+    return check_launch(c, "bj_inverse");
+}
+
+// Block-Jacobi factor: Minv_i = inv(Hg_ii) for every face row (binfo[i] = 1 +
+// pivot step of a singular block).  Block sizes with a blocked Gauss-Jordan
+// instance take it (diagonal blocks gathered first); the others the one-CTA-
+// per-block kernel.
+int bj_factor(hfem_ctx* c) {
+    Timed t(c, "bj_inverse");
+    switch (c->bsz) {
+        case 12: return bj_blocked<12>(c);
+        case 16: return bj_blocked<16>(c);
+        case 20: return bj_blocked<20>(c);
+        case 30: return bj_blocked<30>(c);
+        case 50: return bj_blocked<50>(c);
+        default: break;
+    }
+    const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
+    bj_inverse_kernel<<<std::min(c->dims.nf, sms(c->device) * 8), 64, smem, c->stream>>>(
+        c->dims.nf, c->bsz, c->rowstart, c->Hg, c->Minv, c->binfo);
+    return check_launch(c, "bj_inverse");
+}
+
 int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int* conv, int* iters,
                    double* hist, int hist_len);
 
@@ -1012,11 +1054,7 @@ int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int
         if ((rc = bilu0_factor(c))) return rc;
         if ((rc = bilu0_apply(c, c->Rg, c->pb))) return rc;
     } else if (prec) {
-        Timed t(c, "bj_inverse");
-        const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
-        bj_inverse_kernel<<<std::min(c->dims.nf, sms(c->device) * 8), 64, smem, c->stream>>>(
-            c->dims.nf, c->bsz, c->rowstart, c->Hg, c->Minv, c->binfo);
-        if ((rc = check_launch(c, "bj_inverse"))) return rc;
+        if ((rc = bj_factor(c))) return rc;
         std::vector<int> bi(c->dims.nf);
         CK(cudaMemcpyAsync(bi.data(), c->binfo, sizeof(int) * bi.size(), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
@@ -1208,11 +1246,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
         c->seg_partk_n = (size_t)c->npieces * (restart + 1);
     }
     if (prec) {
-        Timed t(c, "bj_inverse");
-        const size_t smem = sizeof(double) * ((size_t)c->bsz * c->bsz + c->bsz) + sizeof(int) * c->bsz;
-        bj_inverse_kernel<<<std::min(c->dims.nf, sms(c->device) * 8), 64, smem, c->stream>>>(
-            c->dims.nf, c->bsz, c->rowstart, c->Hg, c->Minv, c->binfo);
-        if ((rc = check_launch(c, "bj_inverse"))) return rc;
+        if ((rc = bj_factor(c))) return rc;
         std::vector<int> bi(c->dims.nf);
         CK(cudaMemcpyAsync(bi.data(), c->binfo, sizeof(int) * bi.size(), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
