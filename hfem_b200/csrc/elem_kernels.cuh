@@ -1,18 +1,13 @@
-// HDG element kernels for sm_100a: local assembly, static condensation,
-// face-block scatter, q recovery and solution update.
-//
-// One CTA owns one element at a time (persistent grid, elements strided by
-// gridDim.x).  Small per-element data live in shared memory; the larger
-// per-element intermediates live in a per-CTA global workspace slot that stays
-// L2-resident while the CTA works on the element.  Outputs are written exactly
-// once per entry; no atomics, so results are bit-reproducible run to run.
+// Shared pieces of the HDG element kernels for sm_100a: element shapes and
+// arguments, geometry and q-equation matrices, the Cholesky helpers, the
+// face-block scatter, the residual norm, q recovery and the solution update.
+// The element assembly itself is element_kernel_v2 (elem_kernel_v2.cuh).
 //
 // Structure of the element blocks (restating elementassembly.cpp faceint
 // 717-1321): every face contribution to the element equations is the
 // trace-equation entry lifted to the element node that carries the face dof,
 //   D = D_vol + P K,   F = F_vol + P H,   Ru = Ru_vol + P Rh,
-// where P (npv x ndf) is the incidence perm[fdof] = node.  So K, H, Rh are
-// computed first and D, F, Ru gather them.
+// where P (npv x ndf) is the incidence perm[fdof] = node.
 #pragma once
 #include <cuda_runtime.h>
 #include "ns_flux.cuh"
@@ -57,7 +52,7 @@ struct ElemArgs {
     double fc_u, fc_q;
     int ne;
     double *D, *F, *K, *H, *Ru, *Rh, *Ro, *ru2;
-    double* ws;                 // gridDim.x slots of Shape::WS doubles
+    double* ws;                 // gridDim.x workspace slots of V2<S>::WS doubles (element_kernel_v2)
     // several problems in one mesh (NULL = the uniform values above): element ->
     // problem, and per problem [gamma, eps, Re, Pr, Mach, tau, tdep, fc_u]
     const int* eprob;
@@ -250,501 +245,6 @@ __device__ __forceinline__ void chol_solve_col_reg(const double* lm, double* col
     }
 #pragma unroll
     for (int i = 0; i < NPV; i++) col[i] = x[i];
-}
-
-// ------------------------------------------------------------ element kernel
-template <class S>
-struct ElemSmem {
-    double x[S::NPV * S::ND];
-    double u[S::NPV * S::NC];
-    double uhe[S::NDF * S::NCH];
-    double shu[S::NPV * S::NCU];
-    double jac[S::NGV], Xx[S::NGV * S::ND * S::ND];
-    double jacf[S::NA], nl[S::NA * S::ND];
-    double M[S::NPV * S::NPV];
-    double C[S::NPV * S::NPV * S::ND];
-    double E[S::NPV * S::NDF * S::ND];
-    double ug[S::NGV * S::NC];
-    double ugf[S::NA * S::NC];
-    double uhg[S::NA * S::NCH];
-    double wrk[S::NQ * S::NCU];
-    double fn[S::NA * S::NCH];
-    double shapvg[S::NPV * S::NQ];
-    double red[NT / 32];
-    int perm[S::NDF];
-    int inc_n[S::NPV];
-    int inc_f[S::NPV * S::MAXINC];
-};
-
-template <class S>
-__global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
-    constexpr int ND = S::ND, NPV = S::NPV, NPF = S::NPF, NGV = S::NGV, NGF = S::NGF, NFE = S::NFE;
-    constexpr int NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, ND1 = S::ND1, N = S::N, NB = S::NB;
-    constexpr int NA = S::NA, NQ = S::NQ, NPF2 = NPF * NPF;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    ElemSmem<S>& sm = *reinterpret_cast<ElemSmem<S>*>(smem_raw);
-    const Tables& T = A.T;
-    const int tid = threadIdx.x;
-
-    double* ws = A.ws + (size_t)blockIdx.x * S::WS;
-    double* wrl = ws;                               // [g + NGV*(r + ND1*(j + NCU*k))]
-    double* sMiC = wrl + S::W_WRL;                  // [g + NGV*(a + NPV*d)]
-    double* sMiE = sMiC + S::W_SMIC;                // [g + NGV*(fn + NDF*d)]  (carries the minus sign)
-    double* sMiCf = sMiE + S::W_SMIE;               // [g' + NA*(a + NPV*d)]
-    double* sMiEf = sMiCf + S::W_SMICF;             // [g' + NA*(fn + NDF*d)]
-    double* fnu = sMiEf + S::W_SMIEF;               // [g' + NA*(j + NCH*k)]
-    double* fnuh = fnu + S::W_FNU;                  // [g' + NA*(j + NCH*k)]
-
-    // master tables that every element reuses
-    for (int t = tid; t < NPV * NQ; t += NT) sm.shapvg[t] = T.shapvg[t];
-    for (int t = tid; t < NDF; t += NT) sm.perm[t] = T.perm[t];
-    __syncthreads();
-    for (int i = tid; i < NPV; i += NT) {           // node -> incident face dofs, ascending
-        int c = 0;
-        for (int f = 0; f < NDF; f++)
-            if (sm.perm[f] == i && c < S::MAXINC) sm.inc_f[i * S::MAXINC + c++] = f;
-        sm.inc_n[i] = c;
-    }
-
-    for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
-        __syncthreads();
-        // ---- gather element data
-        const double* xg = A.dgnodes + (size_t)e * NPV * ND;
-        const double* ugl = A.udg + (size_t)e * NPV * NC;
-        const double* shg = A.sh + (size_t)e * NPV * NC;
-        for (int t = tid; t < NPV * ND; t += NT) sm.x[t] = xg[t];
-        for (int t = tid; t < NPV * NC; t += NT) sm.u[t] = ugl[t];
-        for (int t = tid; t < NPV * NCU; t += NT) sm.shu[t] = shg[t];
-        for (int t = tid; t < NDF * NCH; t += NT) {
-            const int fn = t / NCH, c = t % NCH;
-            sm.uhe[fn + NDF * c] = A.uh[(size_t)A.elcon[(size_t)e * NDF + fn] * NCH + c];
-        }
-        __syncthreads();
-        geometry<S>(T, sm.x, sm.jac, sm.Xx, sm.jacf, sm.nl);
-        __syncthreads();
-        qmatrices<S>(T, A.fc_q, sm.jac, sm.Xx, sm.jacf, sm.nl, sm.M, sm.C, sm.E);
-        // solution at volume / face points
-        for (int t = tid; t < NGV * NC; t += NT) {
-            const int g = t % NGV, c = t / NGV;
-            double s = 0.0;
-            for (int a = 0; a < NPV; a++) s += T.shapvt[g + NGV * a] * sm.u[a + NPV * c];
-            sm.ug[t] = s;
-        }
-        for (int t = tid; t < NA * (NC + NCH); t += NT) {
-            const int gg = t % NA, c = t / NA, fc = gg / NGF, q = gg % NGF;
-            double s = 0.0;
-            if (c < NC) {
-                for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.u[sm.perm[fc * NPF + m] + NPV * c];
-                sm.ugf[gg + NA * c] = s;
-            } else {
-                for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.uhe[fc * NPF + m + NDF * (c - NC)];
-                sm.uhg[gg + NA * (c - NC)] = s;
-            }
-        }
-        __syncthreads();
-        cholesky_warp<NPV>(sm.M);
-        __syncthreads();
-        // M^-1 C, M^-1 E in place (one right-hand side per thread)
-        for (int t = tid; t < NPV * ND + NDF * ND; t += NT) {
-            double* col = (t < NPV * ND) ? &sm.C[NPV * t] : &sm.E[NPV * (t - NPV * ND)];
-            chol_solve_col<NPV>(sm.M, col);
-        }
-        __syncthreads();
-        // q sensitivities at volume and face points
-        for (int t = tid; t < NGV * NPV * ND; t += NT) {
-            const int g = t % NGV, ad = t / NGV;   // ad = a + NPV*d
-            double s = 0.0;
-            for (int b = 0; b < NPV; b++) s += T.shapvt[g + NGV * b] * sm.C[b + NPV * ad];
-            sMiC[t] = s;
-        }
-        for (int t = tid; t < NGV * NDF * ND; t += NT) {
-            const int g = t % NGV, fd = t / NGV;   // fd = fn + NDF*d
-            double s = 0.0;
-            for (int b = 0; b < NPV; b++) s += T.shapvt[g + NGV * b] * sm.E[b + NPV * fd];
-            sMiE[t] = -s;
-        }
-        for (int t = tid; t < NA * NPV * ND; t += NT) {
-            const int gg = t % NA, ad = t / NA, fc = gg / NGF, q = gg % NGF;
-            double s = 0.0;
-            for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.C[sm.perm[fc * NPF + m] + NPV * ad];
-            sMiCf[t] = s;
-        }
-        for (int t = tid; t < NA * NDF * ND; t += NT) {
-            const int gg = t % NA, fd = t / NA, fc = gg / NGF, q = gg % NGF;
-            double s = 0.0;
-            for (int m = 0; m < NPF; m++) s += T.shapft[q + NGF * m] * sm.E[sm.perm[fc * NPF + m] + NPV * fd];
-            sMiEf[t] = s;
-        }
-        // pointwise fluxes: volume points (threads [0, NGV)), face points ([NGV, NGV+NA))
-        if (tid < NGV + NA) {
-            using DD = Dual<NC>;
-            DD w[NC], f[ND * NCU];
-            const bool vol = tid < NGV;
-            const int g = vol ? tid : tid - NGV;
-#pragma unroll
-            for (int k = 0; k < NC; k++) {
-                double val;
-                if (vol) val = sm.ug[g + NGV * k];
-                else val = (k < NCU) ? sm.uhg[g + NA * k] : sm.ugf[g + NA * k];
-                w[k] = dc<NC>(val);
-                w[k].d[k] = 1.0;
-            }
-            ns_flux_dual<ND>(A.param, w, f);
-            if (vol) {
-                const double jg = sm.jac[g];
-#pragma unroll
-                for (int j = 0; j < NCU; j++) {
-                    double s = 0.0;
-                    if (A.tdep) {
-                        double t = 0.0;
-                        for (int a = 0; a < NPV; a++) t += T.shapvt[g + NGV * a] * sm.shu[a + NPV * j];
-                        s = t - sm.ug[g + NGV * j] * A.fc_u;
-                    }
-                    sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
-#pragma unroll
-                    for (int m = 0; m < ND; m++) {
-                        double fx = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
-                        sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
-                    }
-#pragma unroll
-                    for (int k = 0; k < NC; k++) {
-                        const double su = (A.tdep && k == j) ? -A.fc_u : 0.0;
-                        wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
-#pragma unroll
-                        for (int m = 0; m < ND; m++) {
-                            double t = 0.0;
-#pragma unroll
-                            for (int d = 0; d < ND; d++) t += f[d * NCU + j].d[k] * sm.Xx[g + NGV * (d + ND * m)];
-                            wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -t;
-                        }
-                    }
-                }
-            } else {
-                // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
-                const double tau = A.param[5];
-                const double jf = sm.jacf[g];
-#pragma unroll
-                for (int j = 0; j < NCU; j++) {
-                    double t = tau * (sm.ugf[g + NA * j] - sm.uhg[g + NA * j]);
-#pragma unroll
-                    for (int d = 0; d < ND; d++) t += f[d * NCU + j].v * sm.nl[g + NA * d];
-                    sm.fn[g + NA * j] = t * jf;
-#pragma unroll
-                    for (int k = 0; k < NC; k++) {
-                        double dn = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[k] * sm.nl[g + NA * d];
-                        if (k < NCU) {
-                            fnuh[g + NA * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
-                            fnu[g + NA * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
-                        } else {
-                            fnu[g + NA * (j + NCH * k)] = dn * jf;
-                        }
-                    }
-                }
-            }
-        }
-        __syncthreads();
-
-        // ---- trace-equation blocks K (nb x n), H (nb x nb), Rh (nb)
-        double* Ke = A.K + (size_t)e * NB * N;
-        double* He = A.H + (size_t)e * NB * NB;
-        double* Rhe = A.Rh + (size_t)e * NB;
-        double* Roe = A.Ro + (size_t)e * NB;
-        for (int t = tid; t < NB * N; t += NT) {
-            const int r = t % NB, c = t / NB;
-            const int j = r % NCH, fdof = r / NCH, fc = fdof / NPF, ip = fdof % NPF;
-            const int a = c % NPV, m = c / NPV;
-            double s = 0.0;
-            for (int kk = 0; kk < NPF; kk++)
-                if (sm.perm[fc * NPF + kk] == a)
-                    for (int q = 0; q < NGF; q++)
-                        s += T.sfsf[(ip + NPF * kk) + NPF2 * q] * fnu[q + NGF * fc + NA * (j + NCH * m)];
-            for (int q = 0; q < NGF; q++) {
-                const int gg = q + NGF * fc;
-                double v = 0.0;
-#pragma unroll
-                for (int d = 0; d < ND; d++) v += fnu[gg + NA * (j + NCH * (NCU * (1 + d) + m))] * sMiCf[gg + NA * (a + NPV * d)];
-                s += T.shapfg[ip + NPF * q] * v;
-            }
-            Ke[t] = s;
-        }
-        for (int t = tid; t < NB * NB; t += NT) {
-            const int r = t % NB, c = t / NB;
-            const int j = r % NCH, fdof = r / NCH, fc = fdof / NPF, ip = fdof % NPF;
-            const int m = c % NCH, fdof2 = c / NCH;
-            double s = 0.0;
-            if (fdof2 / NPF == fc) {
-                const int kk = fdof2 % NPF;
-                for (int q = 0; q < NGF; q++)
-                    s += T.sfsf[(ip + NPF * kk) + NPF2 * q] * fnuh[q + NGF * fc + NA * (j + NCH * m)];
-            }
-            double s2 = 0.0;
-            for (int q = 0; q < NGF; q++) {
-                const int gg = q + NGF * fc;
-                double v = 0.0;
-#pragma unroll
-                for (int d = 0; d < ND; d++) v += fnu[gg + NA * (j + NCH * (NCU * (1 + d) + m))] * sMiEf[gg + NA * (fdof2 + NDF * d)];
-                s2 += T.shapfg[ip + NPF * q] * v;
-            }
-            He[t] = s - s2;
-        }
-        for (int t = tid; t < NB; t += NT) {
-            const int j = t % NCH, fdof = t / NCH, fc = fdof / NPF, ip = fdof % NPF;
-            double s = 0.0;
-            for (int q = 0; q < NGF; q++) s += T.shapfg[ip + NPF * q] * sm.fn[q + NGF * fc + NA * j];
-            Rhe[t] = -s;
-            Roe[t] = -s;
-        }
-        __syncthreads();
-
-        // ---- element blocks D (n x n), F (n x nb), Ru (n): volume part + lifted trace part
-        double* De = A.D + (size_t)e * N * N;
-        double* Fe = A.F + (size_t)e * N * NB;
-        for (int col = tid; col < NCU * NPV * NCU + NCU * NCU * NDF; col += NT) {
-            double acc[NPV];
-#pragma unroll
-            for (int i = 0; i < NPV; i++) acc[i] = 0.0;
-            if (col < NCU * NPV * NCU) {            // D column (j, a, k) -> rows (i, j)
-                const int j = col % NCU, a = (col / NCU) % NPV, k = col / (NCU * NPV);
-                for (int r = 0; r < ND1; r++)
-                    for (int g = 0; g < NGV; g++) {
-                        double w = wrl[g + NGV * (r + ND1 * (j + NCU * k))] * T.shapvt[g + NGV * a];
-#pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            w += wrl[g + NGV * (r + ND1 * (j + NCU * (NCU * (1 + d) + k)))] * sMiC[g + NGV * (a + NPV * d)];
-                        const int q = g + NGV * r;
-#pragma unroll
-                        for (int i = 0; i < NPV; i++) acc[i] += sm.shapvg[i + NPV * q] * w;
-                    }
-                const int kcol = a + NPV * k;
-#pragma unroll
-                for (int i = 0; i < NPV; i++) {
-                    double s = acc[i];
-                    for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
-                        s += Ke[j + NCH * sm.inc_f[i * S::MAXINC + c2] + NB * kcol];
-                    De[i + NPV * (j + NCU * kcol)] = s;
-                }
-            } else {                                 // F column (j, k, fn2)
-                const int cc = col - NCU * NPV * NCU;
-                const int j = cc % NCU, k = (cc / NCU) % NCU, fn2 = cc / (NCU * NCU);
-                for (int r = 0; r < ND1; r++)
-                    for (int g = 0; g < NGV; g++) {
-                        double w = 0.0;
-#pragma unroll
-                        for (int d = 0; d < ND; d++)
-                            w += wrl[g + NGV * (r + ND1 * (j + NCU * (NCU * (1 + d) + k)))] * sMiE[g + NGV * (fn2 + NDF * d)];
-                        const int q = g + NGV * r;
-#pragma unroll
-                        for (int i = 0; i < NPV; i++) acc[i] += sm.shapvg[i + NPV * q] * w;
-                    }
-                const int hcol = k + NCH * fn2;
-#pragma unroll
-                for (int i = 0; i < NPV; i++) {
-                    double s = acc[i];
-                    for (int c2 = 0; c2 < sm.inc_n[i]; c2++)
-                        s += He[j + NCH * sm.inc_f[i * S::MAXINC + c2] + NB * hcol];
-                    Fe[i + NPV * (j + NCU * hcol)] = s;
-                }
-            }
-        }
-        double ru2 = 0.0;
-        for (int t = tid; t < N; t += NT) {
-            const int i = t % NPV, j = t / NPV;
-            double s = 0.0;
-            for (int q = 0; q < NQ; q++) s += sm.shapvg[i + NPV * q] * sm.wrk[q + NQ * j];
-            for (int c2 = 0; c2 < sm.inc_n[i]; c2++) s += Rhe[j + NCH * sm.inc_f[i * S::MAXINC + c2]];
-            A.Ru[(size_t)e * N + t] = s;
-            ru2 += s * s;
-        }
-        const double tot = block_sum(ru2, sm.red);
-        if (tid == 0) A.ru2[e] = tot;
-    }
-}
-
-// --------------------------------------------------------- condensation
-struct SchurArgs {
-    int ne;
-    double *D, *F, *K, *H, *Ru, *Rh;     // F -> D^-1 F in place, Ru -> D^-1 Ru, H and Rh condensed
-    int* info;                            // per element: 0 or 1 + singular pivot index
-};
-
-// CTA-wide C (M x Ncol) = beta C + alpha A (M x Kd) B (Kd x Ncol), column-major, generic pointers.
-// 64 x 64 output tiles, 16-deep k panels staged in shared memory, 4 x 4 per thread.
-__device__ void cta_gemm(int M, int Ncol, int Kd, double alpha, const double* A, int lda, const double* B, int ldb,
-                         double beta, double* C, int ldc, double* tile /* 2*16*64 */) {
-    constexpr int BM = 64, BN = 64, BK = 16;
-    double* As = tile;
-    double* Bs = tile + BK * BM;
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    for (int m0 = 0; m0 < M; m0 += BM)
-        for (int n0 = 0; n0 < Ncol; n0 += BN) {
-            double acc[4][4];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-            for (int k0 = 0; k0 < Kd; k0 += BK) {
-                __syncthreads();
-                for (int t = tid; t < BK * BM; t += blockDim.x) {
-                    const int m = t % BM, k = t / BM;
-                    As[k * BM + m] = (m0 + m < M && k0 + k < Kd) ? A[(m0 + m) + (size_t)lda * (k0 + k)] : 0.0;
-                }
-                for (int t = tid; t < BK * BN; t += blockDim.x) {
-                    const int k = t % BK, n = t / BK;
-                    Bs[k * BN + n] = (n0 + n < Ncol && k0 + k < Kd) ? B[(k0 + k) + (size_t)ldb * (n0 + n)] : 0.0;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int k = 0; k < BK; k++) {
-                    double a[4], b[4];
-#pragma unroll
-                    for (int i = 0; i < 4; i++) a[i] = As[k * BM + ty + 16 * i];
-#pragma unroll
-                    for (int j = 0; j < 4; j++) b[j] = Bs[k * BN + tx + 16 * j];
-#pragma unroll
-                    for (int i = 0; i < 4; i++)
-#pragma unroll
-                        for (int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
-                    if (m < M && n < Ncol) {
-                        double* c = &C[m + (size_t)ldc * n];
-                        *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[i][j];
-                    }
-                }
-        }
-    __syncthreads();
-}
-
-// Static condensation per element (elementschur.cpp:6-329): D^-1 by Gauss-Jordan with
-// partial pivoting in shared memory, F <- D^-1 F, H <- H - K D^-1 F, Ru <- D^-1 Ru,
-// Rh <- Rh - K D^-1 Ru.
-template <int N, int NB>
-__global__ void __launch_bounds__(NT) schur_kernel(SchurArgs A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* Ai = reinterpret_cast<double*>(smem_raw);          // N x N
-    constexpr int PW = 32;                                       // F panel width
-    double* panel = Ai + N * N;                                  // N x PW
-    double* tile = panel + N * PW;                               // 2*16*64
-    double* vec = tile + 2 * 16 * 64;                            // N
-    __shared__ int piv[N];
-    __shared__ int s_p;
-    __shared__ double s_red[NT / 32];
-    __shared__ int s_redi[NT / 32];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-
-    for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
-        __syncthreads();
-        const double* De = A.D + (size_t)e * N * N;
-        for (int t = tid; t < N * N; t += NT) Ai[t] = De[t];
-        __syncthreads();
-        int bad = 0;
-        for (int k = 0; k < N; k++) {
-            // pivot: first row of maximal |A(i,k)|, i >= k (LAPACK idamax tie rule)
-            double best = -1.0;
-            int bi = N;
-            for (int i = k + tid; i < N; i += NT) {
-                const double v = fabs(Ai[i + N * k]);
-                if (v > best) { best = v; bi = i; }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_down_sync(0xffffffffu, best, o);
-                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-            }
-            if (lane == 0) { s_red[wid] = best; s_redi[wid] = bi; }
-            __syncthreads();
-            if (tid == 0) {
-                double b = s_red[0];
-                int p = s_redi[0];
-                for (int w = 1; w < NT / 32; w++)
-                    if (s_red[w] > b || (s_red[w] == b && s_redi[w] < p)) { b = s_red[w]; p = s_redi[w]; }
-                s_p = p;
-                piv[k] = p;
-            }
-            __syncthreads();
-            const int p = s_p;
-            if (Ai[p + N * k] == 0.0) { bad = k + 1; break; }
-            if (p != k)
-                for (int c = tid; c < N; c += NT) {
-                    const double t = Ai[k + N * c];
-                    Ai[k + N * c] = Ai[p + N * c];
-                    Ai[p + N * c] = t;
-                }
-            __syncthreads();
-            const double dinv = 1.0 / Ai[k + N * k];
-            // column k of the eliminated rows, saved before the row update
-            for (int i = tid; i < N; i += NT) vec[i] = (i == k) ? 0.0 : Ai[i + N * k];
-            __syncthreads();
-            for (int c = tid; c < N; c += NT) Ai[k + N * c] = (c == k ? 1.0 : Ai[k + N * c]) * dinv;
-            __syncthreads();
-            for (int t = tid; t < N * N; t += NT) {
-                const int i = t % N, c = t / N;
-                if (i != k) {
-                    const double base = (c == k) ? 0.0 : Ai[i + N * c];
-                    Ai[i + N * c] = base - vec[i] * Ai[k + N * c];
-                }
-            }
-            __syncthreads();
-        }
-        if (bad) {
-            if (tid == 0) A.info[e] = bad;
-            continue;
-        }
-        // undo the row interchanges on the columns of the inverse
-        for (int k = N - 1; k >= 0; k--) {
-            const int p = piv[k];
-            if (p != k)
-                for (int i = tid; i < N; i += NT) {
-                    const double t = Ai[i + N * k];
-                    Ai[i + N * k] = Ai[i + N * p];
-                    Ai[i + N * p] = t;
-                }
-            __syncthreads();
-        }
-        if (tid == 0) A.info[e] = 0;
-        // F <- D^-1 F, panel by panel (in place in global memory)
-        double* Fe = A.F + (size_t)e * N * NB;
-        for (int c0 = 0; c0 < NB; c0 += PW) {
-            const int w = min(PW, NB - c0);
-            for (int t = tid; t < N * w; t += NT) panel[t] = Fe[(t % N) + (size_t)N * (c0 + t / N)];
-            __syncthreads();
-            for (int t = tid; t < N * w; t += NT) {
-                const int i = t % N, c = t / N;
-                double s = 0.0;
-                for (int k = 0; k < N; k++) s += Ai[i + N * k] * panel[k + N * c];
-                Fe[i + (size_t)N * (c0 + c)] = s;
-            }
-            __syncthreads();
-        }
-        // Ru <- D^-1 Ru
-        double* Rue = A.Ru + (size_t)e * N;
-        for (int t = tid; t < N; t += NT) vec[t] = Rue[t];
-        __syncthreads();
-        for (int i = tid; i < N; i += NT) {
-            double s = 0.0;
-            for (int k = 0; k < N; k++) s += Ai[i + N * k] * vec[k];
-            Rue[i] = s;
-        }
-        __syncthreads();
-        // H <- H - K (D^-1 F);  Rh <- Rh - K (D^-1 Ru)
-        const double* Ke = A.K + (size_t)e * NB * N;
-        cta_gemm(NB, NB, N, -1.0, Ke, NB, Fe, N, 1.0, A.H + (size_t)e * NB * NB, NB, tile);
-        double* Rhe = A.Rh + (size_t)e * NB;
-        for (int r = tid; r < NB; r += NT) {
-            double s = 0.0;
-            for (int k = 0; k < N; k++) s += Ke[r + (size_t)NB * k] * Rue[k];
-            Rhe[r] -= s;
-        }
-    }
 }
 
 // --------------------------------------------------------------- scatter

@@ -107,11 +107,8 @@ const std::vector<GemmLaunch>& gemm_candidates() {
 
 struct Launch {
     int nd, npv, npf, ngv, ngf;
-    size_t ws;                  // workspace doubles per CTA slot (element_kernel)
     size_t ws2;                 // workspace doubles per CTA slot (element_kernel_v2)
-    size_t elem_smem, schur_smem, q_smem;
-    void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
-    void (*schur)(dim3, size_t, cudaStream_t, const SchurArgs&);
+    size_t q_smem;
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
     void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
     void (*element2)(dim3, size_t, cudaStream_t, const ElemArgs&);
@@ -119,7 +116,7 @@ struct Launch {
     const void* elem2_fn;
     int inv_threads;
     size_t inv_smem;
-    const void *elem_fn, *schur_fn, *q_fn, *inv_fn;
+    const void *q_fn, *inv_fn;
     GemmLaunch g1, g2;
     void (*schur_tc)(dim3, size_t, cudaStream_t, const SchurTcArgs&);
     size_t tc_smem;
@@ -136,11 +133,7 @@ void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int*
 }
 
 template <class S>
-void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel<S><<<g, NT, sm, st>>>(a); }
-template <class S>
 void launch_element2(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel_v2<S><<<g, NT, sm, st>>>(a); }
-template <class S>
-void launch_schur(dim3 g, size_t sm, cudaStream_t st, const SchurArgs& a) { schur_kernel<S::N, S::NB><<<g, NT, sm, st>>>(a); }
 template <class S>
 void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
 template <class S>
@@ -172,16 +165,9 @@ template <class S>
 Launch make_launch() {
     Launch L;
     L.nd = S::ND; L.npv = S::NPV; L.npf = S::NPF; L.ngv = S::NGV; L.ngf = S::NGF;
-    L.ws = S::WS;
     L.ws2 = V2<S>::WS;
-    L.elem_smem = sizeof(ElemSmem<S>);
-    L.schur_smem = sizeof(double) * ((size_t)S::N * S::N + (size_t)S::N * 32 + 2 * 16 * 64 + S::N);
     L.q_smem = sizeof(QSmem<S>);
-    L.element = launch_element<S>;
-    L.schur = launch_schur<S>;
     L.getq = launch_getq<S>;
-    L.elem_fn = (const void*)element_kernel<S>;
-    L.schur_fn = (const void*)schur_kernel<S::N, S::NB>;
     L.q_fn = (const void*)getq_kernel<S>;
     L.inverse = launch_inverse<S::N>;
     L.element2 = launch_element2<S>;
@@ -221,7 +207,7 @@ struct hfem_ctx {
     cudaStream_t own = nullptr, stream = nullptr;
     std::string err;
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
-    int grid_elem = 0, grid_schur = 0, grid_inv = 0, grid_tc = 0;
+    int grid_elem = 0, grid_inv = 0, grid_tc = 0;
     // element-wise state arriving in pieces (hfem_assemble_host): the element
     // kernel of piece k waits for chunk_ev[k]
     cudaStream_t copy_stream = nullptr;
@@ -1523,16 +1509,11 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     }
     c->stream = c->own;
     const Launch& L = *c->L;
-    cudaFuncSetAttribute(L.elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
     cudaFuncSetAttribute(L.elem2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem2_smem);
-    cudaFuncSetAttribute(L.schur_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.schur_smem);
     cudaFuncSetAttribute(L.q_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.q_smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem2_fn, NT, L.elem2_smem);
     c->grid_elem = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
-    occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.schur_fn, NT, L.schur_smem);
-    c->grid_schur = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
     cudaFuncSetAttribute(L.tc_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.tc_smem);
@@ -2273,6 +2254,11 @@ int device_buffer(hfem_ctx* c, int what, const double** src, size_t* need) {
         case 7: *src = c->x; *need = (size_t)d.nf * c->bsz; break;
         case 8: *src = c->udg; *need = (size_t)d.ne * d.npv * c->nc; break;
         case 9: *src = c->uh; *need = (size_t)d.nf * d.npf * c->nch; break;
+        case 10: *src = c->K; *need = (size_t)d.ne * c->nb * c->n; break;
+        case 11: *src = c->F; *need = (size_t)d.ne * c->n * c->nb; break;
+        case 12: *src = c->Ro; *need = (size_t)d.ne * c->nb; break;
+        case 13: *src = c->D; *need = (size_t)d.ne * c->n * c->n; break;
+        case 14: *src = c->ru2; *need = (size_t)d.ne; break;
         default: return fail(c, HFEM_E_ARG, "unknown buffer %d", what);
     }
     if (!*src) return fail(c, HFEM_E_STATE, "nothing computed for buffer %d yet", what);
@@ -2377,12 +2363,15 @@ int hfem_fp64_peak(int device, double* tflops) {
 // RMM allocator, where a raw cudaMalloc synchronises the device and fragments
 // the pool), serving loops that reserve HBM once at admission and may not
 // allocate per request, and host codes that register a fixed set of buffers.
-// The element kernel's per-CTA workspace lives in the file-scope array below
-// instead of a context buffer.  Its size is fixed at HFEM_NOALLOC_SCRATCH_BYTES
-// (32 MiB) on every GPU that loads this library, for the life of the process.
+// It runs the kernels of hfem_assemble (element_kernel_v2, the blocked
+// Gauss-Jordan inverse, the fused condensation and Rh - K D^-1 Ru), so its
+// blocks equal that path's; only the element kernel's per-CTA workspace lives
+// in the file-scope array below instead of a context buffer.  The array's size
+// is fixed at HFEM_NOALLOC_SCRATCH_BYTES (32 MiB) on every GPU that loads this
+// library, for the life of the process; it caps the element kernel's grid at
+// the number of workspace slots that fit (fewer CTAs for large element shapes,
+// same results).
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 #define HFEM_NOALLOC_SCRATCH_BYTES (32u << 20)
 static __device__ __align__(256) double g_noalloc_scratch[HFEM_NOALLOC_SCRATCH_BYTES / sizeof(double)];
 
@@ -2390,30 +2379,42 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+// per (device, element shape): attributes set and grid sizes computed once
+struct NoallocGrids {
+    bool ready = false;
+    int elem = 0, inv = 0;
+};
+NoallocGrids g_noalloc_grids[kMaxDevices][16];
 }  // namespace
 
 extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt, const double* shapvg,
                                      const double* shapvgdotshapvl, const double* shapft, const double* shapfg,
                                      const double* shapfgdotshapfc, const int* perm, const double* dgnodes,
                                      const int* elcon, const double* udg, const double* uh, const double* sh,
-                                     const double* physicsparam, int tdep, double fc_u, double fc_q, double* D,
-                                     double* DinvF, double* K, double* H, double* DinvRu, double* Rh,
-                                     double* Rh_uncondensed, double* ru2, int* info, void* stream) {
+                                     const double* physicsparam, int tdep, double fc_u, double fc_q, const int* bf,
+                                     const int* bcm, const double* bcs, int appname, double* D, double* DinvF,
+                                     double* K, double* H, double* DinvRu, double* Rh, double* Rh_uncondensed,
+                                     double* ru2, int* info, void* stream) {
     if (!dims || !shapvt || !shapvg || !shapvgdotshapvl || !shapft || !shapfg || !shapfgdotshapfc || !perm ||
         !dgnodes || !elcon || !udg || !uh || !sh || !physicsparam || !D || !DinvF || !K || !H || !DinvRu || !Rh ||
-        !Rh_uncondensed || !ru2 || !info)
+        !Rh_uncondensed || !ru2 || !info || (bf && (!bcm || !bcs)) || (appname != 0 && appname != 1))
         return HFEM_E_ARG;
     const hfem_dims& d = *dims;
     if (d.ne <= 0) return HFEM_E_ARG;
-    const Launch* L = nullptr;
-    for (const Launch& x : launches())
-        if (x.nd == d.nd && x.npv == d.npv && x.npf == d.npf && x.ngv == d.ngv && x.ngf == d.ngf) L = &x;
-    if (!L) return HFEM_E_UNSUPPORTED;
-    const size_t slot_bytes = L->ws * sizeof(double);
-    if (slot_bytes > HFEM_NOALLOC_SCRATCH_BYTES) return HFEM_E_ARG;   // one element's workspace exceeds the scratch
+    int li = -1;
+    const std::vector<Launch>& all = launches();
+    for (size_t k = 0; k < all.size(); k++)
+        if (all[k].nd == d.nd && all[k].npv == d.npv && all[k].npf == d.npf && all[k].ngv == d.ngv &&
+            all[k].ngf == d.ngf)
+            li = (int)k;
+    if (li < 0) return HFEM_E_UNSUPPORTED;
+    const Launch* L = &all[li];
+    const size_t slot_bytes = L->ws2 * sizeof(double);
+    if (slot_bytes > HFEM_NOALLOC_SCRATCH_BYTES) return HFEM_E_ARG;   // one CTA's workspace exceeds the scratch
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HFEM_E_CUDA;
     double* scratch = nullptr;
+    int ge = 0, gi = 0;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
         if (!g_noalloc_ptr[dev]) {
@@ -2424,18 +2425,29 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
             }
         }
         scratch = g_noalloc_ptr[dev];
+        NoallocGrids& G = g_noalloc_grids[dev][li];
+        if (!G.ready) {
+            if (cudaFuncSetAttribute(L->elem2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->elem2_smem) !=
+                    cudaSuccess ||
+                cudaFuncSetAttribute(L->inv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->inv_smem) !=
+                    cudaSuccess ||
+                cudaFuncSetAttribute(L->fused_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->fused_smem) !=
+                    cudaSuccess)
+                return HFEM_E_CUDA;
+            int occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->elem2_fn, NT, L->elem2_smem);
+            const int slots = (int)(HFEM_NOALLOC_SCRATCH_BYTES / slot_bytes);
+            G.elem = std::max(1, std::min(slots, sms(dev) * std::max(occ, 1)));
+            occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->inv_fn, L->inv_threads, L->inv_smem);
+            G.inv = sms(dev) * std::max(occ, 1);
+            G.ready = true;
+        }
+        ge = std::min(d.ne, G.elem);
+        gi = std::min(d.ne, G.inv);
     }
-    if (cudaFuncSetAttribute(L->elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->elem_smem) != cudaSuccess ||
-        cudaFuncSetAttribute(L->schur_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->schur_smem) != cudaSuccess)
-        return HFEM_E_CUDA;
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->elem_fn, NT, L->elem_smem);
-    const int slots = (int)(HFEM_NOALLOC_SCRATCH_BYTES / slot_bytes);
-    const int ge = std::max(1, std::min(std::min(d.ne, slots), sms(dev) * std::max(occ, 1)));
-    occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->schur_fn, NT, L->schur_smem);
-    const int gs = std::max(1, std::min(d.ne, sms(dev) * std::max(occ, 1)));
     cudaStream_t st = (cudaStream_t)stream;
+    const int n = L->npv * (d.nd + 2), nb = (d.nd + 2) * d.npf * (d.nd + 1);
 
     ElemArgs a;
     a.T = Tables{shapvt, shapvg, shapvgdotshapvl, shapft, shapfg, shapfgdotshapfc, perm};
@@ -2449,19 +2461,23 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.fc_u = fc_u;
     a.fc_q = fc_q;
     a.ne = d.ne;
+    // F is formed in the DinvF buffer and condensed there in place
     a.D = D; a.F = DinvF; a.K = K; a.H = H;
     a.Ru = DinvRu; a.Rh = Rh; a.Ro = Rh_uncondensed; a.ru2 = ru2;
     a.ws = scratch;
     a.eprob = nullptr;
     a.pparam = nullptr;
-    a.bf = nullptr;
-    a.bcm = nullptr;
-    a.bcs = nullptr;
-    a.inviscid = 0;
-    L->element(dim3(ge), L->elem_smem, st, a);
+    a.bf = bf;
+    a.bcm = bcm;
+    a.bcs = bcs;
+    a.inviscid = appname == 0;
+    L->element2(dim3(ge), L->elem2_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
-    SchurArgs s{d.ne, D, DinvF, K, H, DinvRu, Rh, info};
-    L->schur(dim3(gs), L->schur_smem, st, s);
+    L->inverse(dim3(gi), st, d.ne, D, DinvRu, info);
+    if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
+    L->schur_fused(st, d.ne, D, DinvF, K, H, DinvF);
+    if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
+    batched_dgemv_kernel<<<sms(dev) * 8, 256, 0, st>>>(d.ne, nb, n, -1.0, K, (long long)nb * n, DinvRu, n, Rh, nb);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     return 0;
 }

@@ -6,6 +6,8 @@
 // through a 2-stage cp.async ring in k tiles of 20; the B operand (the F strip,
 // then the X strip) sits in shared memory whole.  Warp w owns m-tiles w, w+NW,
 // ... of every job and all BN/8 n-tiles.  H's accumulators start from H.
+// DinvF may be F itself: a CTA has its whole F strip in shared memory before it
+// writes the X strip over it, and strips are disjoint.
 #pragma once
 #include <cuda_runtime.h>
 #include "schur_kernels.cuh"
@@ -32,9 +34,9 @@ struct FusedCfg {
 
 template <int N, int NB, int BN, int NW>
 __global__ void __launch_bounds__(32 * NW) schur_fused_kernel(int ne, const double* __restrict__ Dinv,
-                                                              const double* __restrict__ F,
+                                                              const double* F,
                                                               const double* __restrict__ K, double* __restrict__ H,
-                                                              double* __restrict__ DinvF) {
+                                                              double* DinvF) {
     using C = FusedCfg<N, NB, BN, NW>;
     extern __shared__ __align__(16) double fsm[];
     double* Bs = fsm;                                  // LDB x BN: the F strip, then the X strip

@@ -235,7 +235,11 @@ int hfem_gmres_problems(hfem_ctx* ctx, int precond, int restart, double tol, int
 /* Download device results for inspection (host buffers of the given length):
  * what = 0 Hg (nblocks*bsz^2), 1 Rg (nf*bsz), 2 Rr = sum of uncondensed Rh
  * (nf*bsz), 3 DinvRu (n*ne), 4 DinvF (n*nb*ne), 5 condensed element H
- * (nb*nb*ne), 6 condensed element Rh (nb*ne), 7 GMRES solution x (nf*bsz). */
+ * (nb*nb*ne), 6 condensed element Rh (nb*ne), 7 GMRES solution x (nf*bsz),
+ * 10 element K (nb*n*ne), 11 element F before condensation (n*nb*ne),
+ * 12 element Rh before condensation (nb*ne), 13 element D^-1 after an
+ * assembly (n*n*ne; D itself after a residual-only pass), 14 ||Ru_e||^2 before
+ * condensation (ne). */
 int hfem_download(hfem_ctx* ctx, int what, double* host, size_t count);
 
 /* Per-kernel device time (ms) accumulated since the last reset, when timing
@@ -253,26 +257,35 @@ int hfem_fp64_peak(int device, double* tflops);
  * programs whose device memory comes from their own caching pool (PyTorch,
  * RMM), where a raw cudaMalloc would synchronise the device and fragment the
  * pool, and serving loops that reserve HBM once and must not allocate per
- * request.  Every pointer except physicsparam (6 doubles, host) is device
- * memory on the calling thread's current device; the caller passes all inputs
- * (master tables, dgnodes, elcon, udg with q, uh, sh) and all outputs, per
- * element: D (n^2, before condensation), DinvF (n*nb), K (nb*n), H (nb^2,
+ * request.  It runs the same kernels as hfem_assemble's element pass, so its
+ * blocks equal that path's.  Every pointer except physicsparam (6 doubles,
+ * host) is device memory on the calling thread's current device, under that
+ * device's primary context (the one the CUDA runtime and PyTorch use).  The
+ * caller passes all inputs -- master tables, dgnodes, elcon, udg with q, uh, sh
+ * and, for a bounded mesh, bf (ne x nfe, element-major, < 0 on boundary
+ * -(ib + 1)), bcm (condition types 1, 2, 5, 6 or 7 per boundary) and bcs
+ * (nch states per boundary) as hfem_set_boundary takes them (bf = NULL: no
+ * boundary faces); appname 1 Navier-Stokes, 0 Euler -- and all outputs, per
+ * element: D (n^2; receives D^-1), DinvF (n*nb), K (nb*n), H (nb^2,
  * condensed), DinvRu (n), Rh (nb, condensed), Rh_uncondensed (nb), ru2
- * (||Ru||^2 before condensation), info (0, or 1 + pivot of a singular D).
+ * (||Ru||^2 before condensation), info (0, or 1 + pivot step of a singular D).
  * The element workspace comes from one fixed 32 MiB device array that every
- * GPU loading the library holds until exit; shapes whose per-CTA workspace
- * exceeds it are rejected with HFEM_E_ARG.  The first call on a device looks
- * up that array's address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls share the array and nothing in it needs to
- * start at zero; calls that overlap on the GPU (different streams or threads
- * at once) race on it.  Launches on `stream` (cudaStream_t, NULL = legacy
- * default stream) and returns without synchronising. */
+ * GPU loading the library holds until exit; it bounds the element kernel's
+ * grid (large element shapes run on fewer CTAs), and shapes whose per-CTA
+ * workspace exceeds it are rejected with HFEM_E_ARG.  The first call on a
+ * device looks up that array's address (cudaGetSymbolAddress) and sets the
+ * kernels' launch attributes; make that first call before any stream capture.
+ * All calls share the array and nothing in it needs to start at zero; calls
+ * that overlap on the GPU (different streams or threads at once) race on it.
+ * Launches on `stream` (cudaStream_t, NULL = legacy default stream) and
+ * returns without synchronising. */
 int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt, const double* shapvg,
                           const double* shapvgdotshapvl, const double* shapft, const double* shapfg,
                           const double* shapfgdotshapfc, const int* perm, const double* dgnodes, const int* elcon,
                           const double* udg, const double* uh, const double* sh, const double* physicsparam,
-                          int tdep, double fc_u, double fc_q, double* D, double* DinvF, double* K, double* H,
-                          double* DinvRu, double* Rh, double* Rh_uncondensed, double* ru2, int* info, void* stream);
+                          int tdep, double fc_u, double fc_q, const int* bf, const int* bcm, const double* bcs,
+                          int appname, double* D, double* DinvF, double* K, double* H, double* DinvRu, double* Rh,
+                          double* Rh_uncondensed, double* ru2, int* info, void* stream);
 
 #ifdef __cplusplus
 }

@@ -305,9 +305,15 @@ def run_reference(prob, mode="assemble", ndump=0, newton=None, workdir=None):
     kw = {}
     if newton is not None:
         kw = dict(newton_maxiter=newton["maxiter"], gmres_tol=newton["tol"])
+    if mode == "dirk":
+        kw.update(dirk_stage=newton["stages"], dirk_order=newton["order"], dt_list=[newton["dt"]],
+                  newton_tol=newton["newton_tol"])
     write_inputs(inp, prob, **kw)
     if mode == "assemble":
         cmd = [REF_BIN, "assemble", inp, out, str(ndump)]
+    elif mode == "dirk":
+        cmd = [REF_BIN, "dirk", inp, out, str(newton["nsteps"]), str(newton["precond"]), str(newton["restart"]),
+               repr(newton["tol"])]
     else:
         cmd = [REF_BIN, "newton", inp, out, str(newton["maxiter"]), str(newton["precond"]),
                str(newton["restart"]), repr(newton["tol"])]
@@ -324,4 +330,6 @@ def run_reference(prob, mode="assemble", ndump=0, newton=None, workdir=None):
             for k in ("eD", "eF", "eK", "eH", "eRu", "eRh"):
                 res[k] = ld(k)
         return res
+    if mode == "dirk":
+        return {"udg_steps": ld("udg_steps").reshape(newton["nsteps"] + 1, *prob.udg.shape)}
     return {k: ld(k) for k in ("udg", "uh", "rnorm_hist", "gmres_iters", "gmres_hist")}

@@ -13,6 +13,11 @@
 //   hfem_ref newton <in> <out> <maxiter> <precond> <restart> <gmres_tol>
 //       the reference Newton driver solveNonlinearProblem (dgsolvers.cpp:106-205)
 //       after getQ; writes the final udg, uh and the residual / GMRES histories.
+//   hfem_ref dirk <in> <out> <nsteps> <precond> <restart> <gmres_tol>
+//       nsteps time steps of the reference's own DIRK driver solveUnsteadyProblem
+//       (dgsolvers.cpp:221-444; tableau, dt and Newton limits from the app file),
+//       one step per call (app.dt holds one step); writes UDG after getQ and after
+//       every step, nsteps + 1 states back to back.
 //   hfem_ref timing <in> <nelem> <reps>
 //       times assembleLinearSystem over the first nelem elements; prints JSON.
 //
@@ -157,6 +162,21 @@ int main(int argc, char** argv)
         vector<double> its(g_gmres_iters.begin(), g_gmres_iters.end());
         dump(out + "gmres_iters.bin", its.data(), its.size());
         dump(out + "gmres_hist.bin", g_gmres_hist.data(), g_gmres_hist.size());
+        return 0;
+    }
+    if (mode == "dirk") {
+        string out = argv[3];
+        const Int nsteps = atoi(argv[4]);
+        c.sys.preconditioner = atoi(argv[5]);
+        c.sys.restart = atoi(argv[6]);
+        c.sys.tol = atof(argv[7]);
+        g_sol = &c.sol;
+        vector<double> states(c.sol.UDG.begin(), c.sol.UDG.end());
+        for (Int s = 0; s < nsteps; s++) {
+            solveUnsteadyProblem(c.sys, &c.elem, c.mesh, m, c.sol, c.app, &c.temp, &c.ndims[0]);
+            states.insert(states.end(), c.sol.UDG.begin(), c.sol.UDG.end());
+        }
+        dump(out + "udg_steps.bin", states.data(), states.size());
         return 0;
     }
     if (mode == "timing") {

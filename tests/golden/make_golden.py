@@ -10,7 +10,13 @@ Each fixture holds the inputs (so the CPU tests also pin the generator) and
 the reference outputs: q from getQ, Hg / Rg / Rr, D^-1 Ru, D^-1 F, rNorm and the
 pre-condensation blocks of the first elements; large 3D arrays are stored as
 fixed random projections instead of in full.  The Newton fixture holds the
-reference driver's residual history and GMRES iteration counts.
+reference driver's residual history and GMRES iteration counts; the full-size
+2D workload (32 x 32 x 2 triangles, p = 2) gets one Newton step of the same
+driver, and the Taylor-Green fixture the kinetic-energy history of 20 steps of
+the reference's DIRK(3,3) driver (solveUnsteadyProblem).
+
+    python tests/golden/make_golden.py newton          # the Newton fixtures only
+    python tests/golden/make_golden.py dirk            # the DIRK fixture only
 """
 import os
 import sys
@@ -22,7 +28,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier  # noqa: E402
+from hfem_b200.diagnostics import kinetic_energy  # noqa: E402
+from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier, ns3d_tgv  # noqa: E402
 from oracle import run_reference  # noqa: E402
 
 CASES = {
@@ -41,15 +48,54 @@ FULL_LIMIT = 400_000          # store arrays up to this many entries in full
 
 
 
-def squeeze(name, a):
+def squeeze(name, a, limit=FULL_LIMIT):
     a = np.asarray(a)
-    if a.size <= FULL_LIMIT:
+    if a.size <= limit:
         return {name: a}
     p = np.random.default_rng(20261203).standard_normal((8, a.size))
     return {name + "_proj": p @ a.ravel(), name + "_absmax": np.array([np.max(np.abs(a))])}
 
 
+def newton_fixtures():
+    if not os.path.exists(os.path.join(HERE, "ns2d_p2_n4_newton.npz")):
+        prob = ns2d_vortex(n=4, porder=2)
+        ref = run_reference(prob, mode="newton", newton=dict(maxiter=2, precond=2, restart=50, tol=1e-10))
+        np.savez_compressed(os.path.join(HERE, "ns2d_p2_n4_newton.npz"), rnorm_hist=ref["rnorm_hist"],
+                            gmres_iters=ref["gmres_iters"], udg=ref["udg"], uh=ref["uh"])
+        print("newton", ref["rnorm_hist"], ref["gmres_iters"])
+    # the full-size 2D workload: 2,048 elements, one Newton step
+    prob = ns2d_vortex(n=32, porder=2)
+    ref = run_reference(prob, mode="newton", newton=dict(maxiter=1, precond=2, restart=50, tol=1e-10))
+    out = dict(rnorm_hist=ref["rnorm_hist"], gmres_iters=ref["gmres_iters"])
+    out.update(squeeze("udg", ref["udg"], limit=0))
+    out.update(squeeze("uh", ref["uh"], limit=0))
+    np.savez_compressed(os.path.join(HERE, "ns2d_p2_n32_newton1.npz"), **out)
+    print("newton n32", ref["rnorm_hist"], ref["gmres_iters"])
+
+
+DIRK_CASE = dict(n=4, porder=3, dt=0.01, nsteps=20)
+
+
+def dirk_fixture():
+    """Taylor-Green vortex, 4^3 x 6 tetrahedra, p = 3, DIRK(3,3), 20 steps of
+    dt = 0.01, each stage solved by Newton to 1e-10 with block-Jacobi GMRES(50)."""
+    c = DIRK_CASE
+    prob = ns3d_tgv(n=c["n"], porder=c["porder"], dt=c["dt"])
+    ref = run_reference(prob, mode="dirk", newton=dict(maxiter=10, precond=2, restart=50, tol=1e-10, stages=3,
+                                                       order=3, dt=c["dt"], newton_tol=1e-10, nsteps=c["nsteps"]))
+    steps = ref["udg_steps"]
+    ke = np.array([kinetic_energy(prob, u) for u in steps])
+    out = dict(ke=ke, **{k: np.array([v]) for k, v in c.items()})
+    out.update(squeeze("udg_final", steps[-1], limit=0))
+    np.savez_compressed(os.path.join(HERE, "tgv_p3_n4_dirk20.npz"), **out)
+    print("dirk", ke)
+
+
 def main(only=None):
+    if only and "newton" in only:
+        return newton_fixtures()
+    if only and "dirk" in only:
+        return dirk_fixture()
     for key, make in CASES.items():
         if only and key not in only:
             continue
@@ -63,11 +109,8 @@ def main(only=None):
         print(key, {k: v.shape for k, v in out.items()})
     if only:
         return
-    prob = ns2d_vortex(n=4, porder=2)
-    ref = run_reference(prob, mode="newton", newton=dict(maxiter=2, precond=2, restart=50, tol=1e-10))
-    np.savez_compressed(os.path.join(HERE, "ns2d_p2_n4_newton.npz"), rnorm_hist=ref["rnorm_hist"],
-                        gmres_iters=ref["gmres_iters"], udg=ref["udg"], uh=ref["uh"])
-    print("newton", ref["rnorm_hist"], ref["gmres_iters"])
+    newton_fixtures()
+    dirk_fixture()
 
 
 if __name__ == "__main__":

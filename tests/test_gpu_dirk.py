@@ -45,3 +45,39 @@ def test_dirk33_tgv_matches_oracle():
     assert np.max(np.abs(ke - ke_ref) / ke_ref) < 1e-9, (ke, ke_ref)
     assert np.max(np.abs(u - udg)) / np.max(np.abs(udg)) < 1e-8
     assert ke[-1] < ke[0]            # viscous decay
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "mixed"])
+def test_dirk33_tgv_p3_20_steps_match_reference_driver(precision):
+    """The Taylor-Green DIRK workload at the size the reference finishes in
+    minutes: 4^3 x 6 tetrahedra, p = 3, DIRK(3,3), 20 steps of dt = 0.01, each
+    stage solved by Newton to 1e-10.  The fixture holds the kinetic-energy
+    history of the reference's own driver (solveUnsteadyProblem, made by
+    tests/golden/make_golden.py).  Mixed precision here: FP32 block-Jacobi
+    inverses and the TF32 condensation GEMMs, with FP64 residuals, Arnoldi and
+    Newton updates.  Bar: kinetic energy within 1e-9 relative at every step;
+    final state within 1e-8 of the reference's (both converged to 1e-10)."""
+    import os
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tgv_p3_n4_dirk20.npz")))
+    dt, nsteps = float(g["dt"][0]), int(g["nsteps"][0])
+    prob = ns3d_tgv(n=int(g["n"][0]), porder=int(g["porder"][0]), dt=dt)
+    s = HDGSolver(prob)
+    try:
+        s.set_precision(precision)
+        s.getQ()
+        u, _ = s.get_solution()
+        ke, iters = [kinetic_energy(prob, u)], 0
+        for _ in range(nsteps):
+            iters += s.solveUnsteadyStep(dt, stages=3, order=3, newton_tol=1e-10)
+            u, _ = s.get_solution()
+            ke.append(kinetic_energy(prob, u))
+    finally:
+        s.close()
+    ke = np.array(ke)
+    err = float(np.max(np.abs(ke - g["ke"]) / g["ke"]))
+    print(f"TGV 4^3x6 p3, {nsteps} DIRK(3,3) steps, precision {precision}: {iters} Newton iterations, "
+          f"kinetic-energy rel err {err:.2e}")
+    assert err < 1e-9, (ke, g["ke"])
+    p = np.random.default_rng(20261203).standard_normal((8, u.size))
+    d = float(np.max(np.abs(p @ u.ravel() - g["udg_final_proj"])))
+    assert d <= 1e-8 * g["udg_final_absmax"][0] * np.sqrt(u.size), d

@@ -111,3 +111,26 @@ def test_newton_history_matches_reference():
     assert iters == [int(v) for v in g["gmres_iters"]]
     assert rel(udg.ravel(), g["udg"]) < 1e-12
     assert rel(uh.ravel(), g["uh"]) < 1e-12
+
+
+def projections(name, a):
+    """The fixed random projections make_golden.py stores for large arrays."""
+    p = np.random.default_rng(20261203).standard_normal((8, a.size))
+    return p @ np.ravel(a)
+
+
+def test_newton_step_full_size_2d_matches_reference():
+    """One Newton step of the reference driver on the full-size 2D workload
+    (32 x 32 x 2 triangles, p = 2, block-Jacobi GMRES(50) to 1e-10)."""
+    g = dict(np.load(os.path.join(HERE, "ns2d_p2_n32_newton1.npz")))
+    prob = ns2d_vortex(n=32, porder=2)
+    o = Oracle(prob)
+    udg = o.getq(prob.udg, prob.uh)
+    a = o.assemble(udg, prob.uh)
+    x, flag, gh = o.gmres(a["Hg"], a["Rg"], Minv=o.bj_inverse(a["Hg"]), restart=50, tol=1e-10)
+    assert flag == 0 and len(gh) == int(g["gmres_iters"][0])
+    udg, uh = o.update(udg, prob.uh, x, a["DinvRu"], a["DinvF"], 1.0)
+    hist = np.array([a["rnorm"], o.residual(udg, uh)])
+    assert np.max(np.abs(hist - g["rnorm_hist"])) <= 1e-12 * g["rnorm_hist"][0]
+    for k, v in (("udg", udg), ("uh", uh)):
+        assert np.max(np.abs(projections(k, v) - g[k + "_proj"])) <= 1e-12 * g[k + "_absmax"][0] * np.sqrt(v.size)
