@@ -23,7 +23,7 @@ ERRORS = {-1: "invalid argument", -2: "unsupported element", -3: "CUDA error", -
           -5: "inconsistent mesh", -6: "singular matrix", -7: "out of device memory"}
 
 DOWNLOAD = {"Hg": 0, "Rg": 1, "Rr": 2, "DinvRu": 3, "DinvF": 4, "H": 5, "Rh": 6, "x": 7, "udg": 8, "uh": 9,
-            "K": 10, "F": 11, "Ro": 12, "Dinv": 13, "ru2": 14}
+            "K": 10, "Ro": 12, "Dinv": 13, "ru2": 14}
 
 
 class HfemError(RuntimeError):
@@ -175,7 +175,7 @@ class HDGSolver:
         me, ne = self.prob.mesh, self.prob.mesh.ne
         sizes = {"Hg": int(me.rowstart[-1]) * self.bsz ** 2, "Rg": me.nf * self.bsz, "Rr": me.nf * self.bsz,
                  "DinvRu": ne * self.n, "DinvF": ne * self.n * self.nb, "H": ne * self.nb ** 2,
-                 "Rh": ne * self.nb, "x": me.nf * self.bsz, "K": ne * self.nb * self.n, "F": ne * self.n * self.nb,
+                 "Rh": ne * self.nb, "x": me.nf * self.bsz, "K": ne * self.nb * self.n,
                  "Ro": ne * self.nb, "Dinv": ne * self.n * self.n, "ru2": ne}
         out = np.empty(sizes[what])
         self._chk(self.lib.hfem_download(self.h, DOWNLOAD[what], _d(out), out.size), f"download {what}")
@@ -194,7 +194,7 @@ class HDGSolver:
 
     def download_elements(self, what, elems):
         """The per-element blocks of the listed elements of an element-major
-        buffer (H, Rh, DinvF, DinvRu, K, F, Ro, Dinv), gathered on the device,
+        buffer (H, Rh, DinvF, DinvRu, K, Ro, Dinv, ru2), gathered on the device,
         as an (len(elems), block size) array."""
         import torch
         t = self.device_tensor(what)

@@ -1,0 +1,562 @@
+// Element assembly on the FP64 tensor cores (sm_100a, mma.sync m8n8k4 f64).
+//
+// One CTA owns one element at a time (persistent grid, 2 CTAs per SM).  Every
+// contraction after the pointwise fluxes is a GEMM with rows over (test node,
+// equation, variable) and a B operand resident in shared memory (restating
+// elementassembly.cpp elementint 307-572 and faceint 717-1321):
+//   K_fc[(ip,j,m), a]  = sum_{q,d'} shapfg(ip,q) fhn(q; j, (d',m)) Phi_fc[(q,d'), a],
+//        Phi_fc[(q,0),a] = [a on fc] phi_pos(a)(q),  Phi_fc[(q,d+1),a] = (phi M^-1 C_d)(q; a)
+//   H_fc[(ip,j,m), f2] = sum_{q,d'} shapfg(ip,q) fhn'(q; j, (d',m)) Psi_fc[(q,d'), f2],
+//        d' = 0 uses fhn_uh and Psi_fc[(q,0),f2] = [f2 on fc] phi_f2(q); d' > 0 uses
+//        fhn_u(q; j, q_dm) and Psi_fc = -(phi M^-1 E_d)(q; f2)
+//   Y(i,g,j,c) = sum_r shapvg(i,(g,r)) wrl((g,r), j, c)       (the derivative index r)
+//   D_vol[(i,j,k), a]  = sum_{g,d'} Y(i,g,j,(d',k)) Phi[(g,d'), a],  Phi = [phi_a(g); (phi M^-1 C_d)(g;a)]
+//   F_vol[(i,j,k), f2] = sum_{g,d} Y(i,g,j,(d+1,k)) (-phi M^-1 E_d)(g; f2)
+// The B operands are formed in shared memory from M^-1 C and M^-1 E, which
+// stay in shared memory after the local Cholesky solves.  Of the lifted trace
+// terms, D += P K is added here by reductions in L2 (face after face, so each
+// sum has a fixed order), and F += P H of interior faces by the condensation
+// kernels when they load F (lift.cuh), where H is read anyway; boundary faces,
+// whose trace rows take the boundary flux while their element rows keep fhat,
+// are lifted here in full.  The face mass product uses shapfgdotshapfc = shapfg .* shapfc (its
+// definition, mkmasterelement.m:113-115) in factored form.
+#pragma once
+#include <cuda_runtime.h>
+#include "elem_kernels.cuh"
+#include "schur_kernels.cuh"
+
+namespace hfem {
+
+// Tiles of the row-major element GEMMs (K/H per face, D/F volume) and the
+// shared-memory and workspace budgets of one CTA.
+template <class S>
+struct EK {
+    static constexpr int NKP = ((S::NPV + 7) / 8) * 8;             // K columns (a), padded
+    static constexpr int NHP = ((S::NDF + 7) / 8) * 8;             // H columns (f2), padded
+    static constexpr int NTK = NKP / 8, NTH = NHP / 8;             // n-tiles
+    static constexpr int KFD = ((S::NGF * (S::ND + 1) + 3) / 4) * 4;  // face k = (q, d')
+    static constexpr int KV3 = ((S::NGV * (S::ND + 1) + 3) / 4) * 4;  // volume k = (g, d')
+    static constexpr int KQ3 = ((S::NGV * S::ND + 3) / 4) * 4;        // volume k = (g, d)
+    static constexpr int LDBK = ((KFD + 11) / 16) * 16 + 4;        // == 4 (mod 16): conflict-free B fragments
+    static constexpr int LDBD = ((KV3 + 11) / 16) * 16 + 4;
+    static constexpr int BKH = LDBK * (NKP + NHP);                 // one face's B operand
+    static constexpr int BDF = LDBD * (NKP + NHP);                 // the volume B operand
+    static constexpr int MTV = (S::NPV + 7) / 8;
+    static constexpr int MTF = (S::NPF + 7) / 8;
+    static constexpr int KV = ((S::NQ + 3) / 4) * 4;               // padded k of shapvg
+    static constexpr int KF = ((S::NGF + 3) / 4) * 4;              // padded k of shapfg
+    static constexpr int LDAV = S::NPV | 1;                        // odd: lanes along q hit distinct banks
+    static constexpr int LDAF = ((8 * MTF + 11) / 16) * 16 + 4;
+    // one face's flux-Jacobian slices: [q + NGF (j + NCH c)], c < NC for fhn_u / fb_u,
+    // then NGF NCH NCU entries for fhn_uh / fb_uh
+    static constexpr int FSL = S::NGF * S::NCH * (S::NC + S::NCU);
+    // shared-memory union: M^-1 C and M^-1 E, then either the q/flux phase
+    // scratch or the B operand of the GEMM being run
+    static constexpr int CME = S::NPV * S::NPV * S::ND + S::NPV * S::NDF * S::ND;
+    static constexpr int QPH = S::NPV * S::NPV + S::NGV * S::NC + S::NA * (S::NC + S::NCH) + S::NPV * S::NC +
+                               S::NDF * S::NCH + S::NPV * S::NCU;
+    static constexpr int GPH = BDF > BKH + FSL ? BDF : BKH + FSL;
+    static constexpr int UN = CME + (QPH > GPH ? QPH : GPH);
+    // global workspace per CTA slot (doubles): wrl, the interior and boundary
+    // face slices, the boundary flux values, Y
+    static constexpr int W_WRL = S::NQ * S::NCU * S::NC;
+    static constexpr int W_FSL = S::NFE * FSL;
+    static constexpr int W_FNB = S::NA * S::NCH;
+    static constexpr int W_Y = S::NPV * S::NGV * S::NCU * S::NC;
+    static constexpr int WS = W_WRL + 2 * W_FSL + W_FNB + W_Y;
+};
+
+template <class S>
+struct ElemSmem {
+    double x[S::NPV * S::ND];
+    double jac[S::NGV], Xx[S::NGV * S::ND * S::ND];
+    double jacf[S::NA], nl[S::NA * S::ND];
+    double wrk[S::NQ * S::NCU];
+    double fn[S::NA * S::NCH];
+    double rh[S::NB];                      // Rh with fhat on every face (the element equations' lift)
+    double Av[EK<S>::LDAV * EK<S>::KV];    // shapvg, zero padded: Av[i + LDAV*q]
+    double Af[EK<S>::LDAF * EK<S>::KF];    // shapfg, zero padded: Af[ip + LDAF*q]
+    double sfc[S::NGF * S::NPF];           // face basis values shapfc(kk, q) = shapft[q + NGF*kk]
+    double red[NT / 32];
+    double un[EK<S>::UN];
+    int perm[S::NDF];
+    int inc_n[S::NPV];
+    int inc_f[S::NPV * S::MAXINC];
+    int pos[S::NFE * S::NPV];              // position of element node a on face fc, or -1
+};
+
+template <class S>
+__global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
+    constexpr int ND = S::ND, NPV = S::NPV, NPF = S::NPF, NGV = S::NGV, NGF = S::NGF, NFE = S::NFE;
+    constexpr int NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, ND1 = S::ND1, N = S::N, NB = S::NB;
+    constexpr int NA = S::NA, NQ = S::NQ;
+    using G = EK<S>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ElemSmem<S>& sm = *reinterpret_cast<ElemSmem<S>*>(smem_raw);
+    const Tables& T = A.T;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int gr = lane >> 2, gc = lane & 3;
+
+    double* ws = A.ws + (size_t)blockIdx.x * G::WS;
+    double* wrl = ws;                              // [g + NGV (r + ND1 (j + NCU c))]
+    double* fsl = wrl + G::W_WRL;                  // per face: fhat Jacobian slices
+    double* fslb = fsl + G::W_FSL;                 // per face: boundary-flux Jacobian slices
+    double* fnb = fslb + G::W_FSL;                 // boundary flux [g' + NA j]
+    double* Ys = fnb + G::W_FNB;                   // Y(i,g,j,c) at [g + NGV (c + NC (i + NPV j))]
+
+    // shared union: M^-1 C, M^-1 E, then the phase region
+    double* Cm = sm.un;                            // [b + NPV (a + NPV d)]
+    double* Em = Cm + NPV * NPV * ND;              // [b + NPV (f + NDF d)]
+    double* ph = sm.un + G::CME;
+    double* M = ph;                                // q / flux phase
+    double* ug = M + NPV * NPV;
+    double* ugf = ug + NGV * NC;
+    double* uhg = ugf + NA * NC;
+    double* u = uhg + NA * NCH;
+    double* uhe = u + NPV * NC;
+    double* shu = uhe + NDF * NCH;
+    double* Bs = ph;                               // GEMM phases
+
+    for (int t = tid; t < G::LDAV * G::KV; t += NT) {
+        const int i = t % G::LDAV, q = t / G::LDAV;
+        sm.Av[t] = (i < NPV && q < NQ) ? T.shapvg[i + NPV * q] : 0.0;
+    }
+    for (int t = tid; t < G::LDAF * G::KF; t += NT) {
+        const int i = t % G::LDAF, q = t / G::LDAF;
+        sm.Af[t] = (i < NPF && q < NGF) ? T.shapfg[i + NPF * q] : 0.0;
+    }
+    for (int t = tid; t < NGF * NPF; t += NT) sm.sfc[t] = T.shapft[t];
+    for (int t = tid; t < NDF; t += NT) sm.perm[t] = T.perm[t];
+    __syncthreads();
+    for (int i = tid; i < NPV; i += NT) {
+        int c = 0;
+        for (int f = 0; f < NDF; f++)
+            if (sm.perm[f] == i && c < S::MAXINC) sm.inc_f[i * S::MAXINC + c++] = f;
+        sm.inc_n[i] = c;
+        for (int fc = 0; fc < NFE; fc++) {
+            int p = -1;
+            for (int kk = 0; kk < NPF; kk++)
+                if (sm.perm[fc * NPF + kk] == i) p = kk;
+            sm.pos[fc * NPV + i] = p;
+        }
+    }
+
+    for (int e = A.e_begin + blockIdx.x; e < A.ne; e += gridDim.x) {
+        __syncthreads();
+        const double* xg = A.dgnodes + (size_t)e * NPV * ND;
+        const double* ugl = A.udg + (size_t)e * NPV * NC;
+        const double* shg = A.sh + (size_t)e * NPV * NC;
+        for (int t = tid; t < NPV * ND; t += NT) sm.x[t] = xg[t];
+        for (int t = tid; t < NPV * NC; t += NT) u[t] = ugl[t];
+        for (int t = tid; t < NPV * NCU; t += NT) shu[t] = shg[t];
+        for (int t = tid; t < NDF * NCH; t += NT) {
+            const int fdof = t / NCH, c = t % NCH;
+            uhe[fdof + NDF * c] = A.uh[(size_t)A.elcon[(size_t)e * NDF + fdof] * NCH + c];
+        }
+        __syncthreads();
+        geometry<S>(T, sm.x, sm.jac, sm.Xx, sm.jacf, sm.nl);
+        __syncthreads();
+        qmatrices<S>(T, A.fc_q, sm.jac, sm.Xx, sm.jacf, sm.nl, M, Cm, Em);
+        __syncthreads();
+        const double* P = A.pparam ? A.pparam + 8 * A.eprob[e] : A.param;
+        const int tdep = A.pparam ? (int)P[6] : A.tdep;
+        const double fc_u = A.pparam ? P[7] : A.fc_u;
+        const int* bfe = A.bf ? A.bf + (size_t)e * NFE : nullptr;
+        // warp 0 factors M while the other warps evaluate the states at the points
+        // and the pointwise fluxes, which do not depend on M
+        if (warp == 0) {
+            cholesky_warp<NPV>(M);
+        } else {
+            constexpr int NT1 = NT - 32;
+            const int tid1 = tid - 32;
+            for (int t = tid1; t < NGV * NC; t += NT1) {
+                const int g = t % NGV, c = t / NGV;
+                double s = 0.0;
+                for (int a = 0; a < NPV; a++) s += T.shapvt[g + NGV * a] * u[a + NPV * c];
+                ug[t] = s;
+            }
+            for (int t = tid1; t < NA * (NC + NCH); t += NT1) {
+                const int gg = t % NA, c = t / NA, fc = gg / NGF, q = gg % NGF;
+                double s = 0.0;
+                if (c < NC) {
+                    for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * u[sm.perm[fc * NPF + m] + NPV * c];
+                    ugf[gg + NA * c] = s;
+                } else {
+                    for (int m = 0; m < NPF; m++) s += sm.sfc[q + NGF * m] * uhe[fc * NPF + m + NDF * (c - NC)];
+                    uhg[gg + NA * (c - NC)] = s;
+                }
+            }
+            asm volatile("bar.sync 1, %0;" ::"r"(NT1) : "memory");
+            // pointwise fluxes: one work item per (point, differentiated variable k);
+            // a one-derivative dual pass gives f and df/dw_k at that point.
+            for (int t = tid1; t < (NGV + NA) * NC; t += NT1) {
+                using DD = Dual<1>;
+                const int p = t % (NGV + NA), k = t / (NGV + NA);
+                const bool vol = p < NGV;
+                const int g = vol ? p : p - NGV;
+                DD w[NC], f[ND * NCU];
+#pragma unroll
+                for (int c = 0; c < NC; c++) {
+                    const double val = vol ? ug[g + NGV * c] : ((c < NCU) ? uhg[g + NA * c] : ugf[g + NA * c]);
+                    w[c].v = val;
+                    w[c].d[0] = (c == k) ? 1.0 : 0.0;
+                }
+                ns_flux_dual<ND>(P, w, f, !A.inviscid);
+                if (vol) {
+                    const double jg = sm.jac[g];
+#pragma unroll
+                    for (int j = 0; j < NCU; j++) {
+                        if (k == 0) {
+                            double s = 0.0;
+                            if (tdep) {
+                                double tt = 0.0;
+                                for (int a = 0; a < NPV; a++) tt += T.shapvt[g + NGV * a] * shu[a + NPV * j];
+                                s = tt - ug[g + NGV * j] * fc_u;
+                            }
+                            sm.wrk[g + NGV * (0 + ND1 * j)] = s * jg;
+#pragma unroll
+                            for (int m = 0; m < ND; m++) {
+                                double fx = 0.0;
+#pragma unroll
+                                for (int d = 0; d < ND; d++) fx += f[d * NCU + j].v * sm.Xx[g + NGV * (d + ND * m)];
+                                sm.wrk[g + NGV * ((m + 1) + ND1 * j)] = fx;
+                            }
+                        }
+                        const double su = (tdep && k == j) ? -fc_u : 0.0;
+                        wrl[g + NGV * (0 + ND1 * (j + NCU * k))] = -su * jg;
+#pragma unroll
+                        for (int m = 0; m < ND; m++) {
+                            double tt = 0.0;
+#pragma unroll
+                            for (int d = 0; d < ND; d++) tt += f[d * NCU + j].d[0] * sm.Xx[g + NGV * (d + ND * m)];
+                            wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -tt;
+                        }
+                    }
+                } else {
+                    // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
+                    const double tau = P[5];
+                    const double jf = sm.jacf[g];
+                    const int fc = g / NGF, q = g % NGF;
+                    double* sl = fsl + fc * G::FSL;
+#pragma unroll
+                    for (int j = 0; j < NCU; j++) {
+                        if (k == 0) {
+                            double tt = tau * (ugf[g + NA * j] - uhg[g + NA * j]);
+#pragma unroll
+                            for (int d = 0; d < ND; d++) tt += f[d * NCU + j].v * sm.nl[g + NA * d];
+                            sm.fn[g + NA * j] = tt * jf;
+                        }
+                        double dn = 0.0;
+#pragma unroll
+                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[0] * sm.nl[g + NA * d];
+                        if (k < NCU) {
+                            sl[NGF * NCH * NC + q + NGF * (j + NCH * k)] = (dn - (k == j ? tau : 0.0)) * jf;
+                            sl[q + NGF * (j + NCH * k)] = (k == j ? tau : 0.0) * jf;
+                        } else {
+                            sl[q + NGF * (j + NCH * k)] = dn * jf;
+                        }
+                    }
+                }
+            }
+            // boundary faces: fb and its Jacobians at their points (one item per point and variable)
+            if (bfe) {
+                for (int t = tid1; t < NFE * NGF * (NC + NCH); t += NT1) {
+                    const int fc = t / (NGF * (NC + NCH)), r = t % (NGF * (NC + NCH));
+                    if (bfe[fc] >= 0) continue;
+                    using DD = Dual<1>;
+                    const int q = r % NGF, k = r / NGF, gg = q + NGF * fc;
+                    DD w[NC], uhd[NCH], fb[NCH];
+#pragma unroll
+                    for (int c = 0; c < NC; c++) {
+                        w[c].v = ugf[gg + NA * c];
+                        w[c].d[0] = (c == k) ? 1.0 : 0.0;
+                    }
+#pragma unroll
+                    for (int c = 0; c < NCH; c++) {
+                        uhd[c].v = uhg[gg + NA * c];
+                        uhd[c].d[0] = (NC + c == k) ? 1.0 : 0.0;
+                    }
+                    double nlq[ND];
+#pragma unroll
+                    for (int d = 0; d < ND; d++) nlq[d] = sm.nl[gg + NA * d];
+                    const int ib = -bfe[fc] - 1;
+                    if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb, !A.inviscid)) {
+                        for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
+                    }
+                    const double jf = sm.jacf[gg];
+                    double* sl = fslb + fc * G::FSL;
+#pragma unroll
+                    for (int j = 0; j < NCH; j++) {
+                        if (k == 0) fnb[gg + NA * j] = fb[j].v * jf;
+                        if (k < NC) sl[q + NGF * (j + NCH * k)] = fb[j].d[0] * jf;
+                        else sl[NGF * NCH * NC + q + NGF * (j + NCH * (k - NC))] = fb[j].d[0] * jf;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // M^-1 C and M^-1 E in place, one column per thread
+        for (int t = tid; t < NPV * ND + NDF * ND; t += NT) {
+            double* col = (t < NPV * ND) ? &Cm[NPV * t] : &Em[NPV * (t - NPV * ND)];
+            chol_solve_col_reg<NPV>(M, col);
+        }
+        __syncthreads();
+
+        double* Ke = A.K + (size_t)e * NB * N;
+        double* De = A.D + (size_t)e * N * N;
+        double* Fe = A.F + (size_t)e * N * NB;
+        double* He = A.H + (size_t)e * NB * NB;
+        double* Rhe = A.Rh + (size_t)e * NB;
+        double* Roe = A.Ro + (size_t)e * NB;
+        for (int t = tid; t < NB; t += NT) {
+            const int j = t % NCH, fdof = t / NCH, fc = fdof / NPF, ip = fdof % NPF;
+            double s = 0.0;
+            for (int q = 0; q < NGF; q++) s += sm.Af[ip + G::LDAF * q] * sm.fn[q + NGF * fc + NA * j];
+            sm.rh[t] = -s;
+            Rhe[t] = -s;
+            Roe[t] = -s;
+        }
+        // Y, point index fastest: Ys[g + NGV (c + NC (i + NPV j))], c = NCU d' + k.
+        // One thread per (g, j, c) with g fastest: its wrl words are read once and
+        // the stores of a warp are runs of consecutive words.
+        for (int t = tid; t < NGV * NCU * NC; t += NT) {
+            const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
+            double w[ND1];
+#pragma unroll
+            for (int r = 0; r < ND1; r++) w[r] = wrl[g + NGV * (r + ND1 * (j + NCU * c))];
+#pragma unroll 4
+            for (int i = 0; i < NPV; i++) {
+                double y = 0.0;
+#pragma unroll
+                for (int r = 0; r < ND1; r++) y += sm.Av[i + G::LDAV * (g + NGV * r)] * w[r];
+                Ys[g + NGV * (c + NC * (i + NPV * j))] = y;
+            }
+        }
+        // volume B operands from M^-1 C and M^-1 E: Phi (KV3 x NKP) and Psi (KQ3 x NHP), ld LDBD
+        {
+            double* Phi = Bs;
+            double* Psi = Bs + G::LDBD * G::NKP;
+            for (int t = tid; t < G::KV3 * G::NKP; t += NT) {
+                const int k = t % G::KV3, a = t / G::KV3, g = k % NGV, dp = k / NGV;
+                double x = 0.0;
+                if (a < NPV && k < NGV * ND1) {
+                    if (dp == 0) {
+                        x = T.shapvt[g + NGV * a];
+                    } else {
+                        const double* cm = Cm + NPV * (a + NPV * (dp - 1));
+                        for (int b = 0; b < NPV; b++) x += T.shapvt[g + NGV * b] * cm[b];
+                    }
+                }
+                Phi[k + G::LDBD * a] = x;
+            }
+            for (int t = tid; t < G::KV3 * G::NHP; t += NT) {
+                const int k = t % G::KV3, f2 = t / G::KV3, g = k % NGV, d = k / NGV;
+                double x = 0.0;
+                if (f2 < NDF && k < NGV * ND) {
+                    const double* em = Em + NPV * (f2 + NDF * d);
+                    for (int b = 0; b < NPV; b++) x += T.shapvt[g + NGV * b] * em[b];
+                    x = -x;
+                }
+                Psi[k + G::LDBD * f2] = x;
+            }
+        }
+        __syncthreads();
+        // ---- D_vol = Y' Phi and F_vol = Y'_q Psi (right after Y is written, while it is in L2)
+        {
+            const double* Phi = Bs;
+            const double* Psi = Bs + G::LDBD * G::NKP;
+            constexpr int MTD = (NPV * NCU * NCU + 7) / 8;
+            for (int mt = warp; mt < MTD; mt += NT / 32) {
+                const int r = 8 * mt + gr;
+                const bool rv = r < NPV * NCU * NCU;
+                const int i = r % NPV, j = (r / NPV) % NCU, k = r / (NPV * NCU);
+                const double* yrow = Ys + NGV * (k + NC * (i + NPV * j));
+                double acc[G::NTK][2];
+#pragma unroll
+                for (int b = 0; b < G::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
+                // the m-tile's A values for every k-step are loaded before the first
+                // DMMA, so their latencies overlap
+                double av[G::KV3 / 4];
+#pragma unroll
+                for (int ks = 0; ks < G::KV3 / 4; ks++) {
+                    const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
+                    av[ks] = (rv && kk < NGV * ND1) ? yrow[g + NGV * NCU * dp] : 0.0;
+                }
+#pragma unroll
+                for (int ks = 0; ks < G::KV3 / 4; ks++) {
+                    const int kk = 4 * ks + gc;
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++)
+                        dmma8x8x4(acc[b][0], acc[b][1], av[ks], Phi[kk + G::LDBD * (8 * b + gr)]);
+                }
+                double accf[G::NTH][2];
+#pragma unroll
+                for (int b = 0; b < G::NTH; b++) accf[b][0] = accf[b][1] = 0.0;
+                double aq[G::KQ3 / 4];
+#pragma unroll
+                for (int ks = 0; ks < G::KQ3 / 4; ks++) {
+                    const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
+                    aq[ks] = (rv && kk < NGV * ND) ? yrow[g + NGV * NCU * (d + 1)] : 0.0;
+                }
+#pragma unroll
+                for (int ks = 0; ks < G::KQ3 / 4; ks++) {
+                    const int kk = 4 * ks + gc;
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++)
+                        dmma8x8x4(accf[b][0], accf[b][1], aq[ks], Psi[kk + G::LDBD * (8 * b + gr)]);
+                }
+                if (rv) {
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int a = 8 * b + 2 * gc + h;
+                            if (a < NPV) De[i + NPV * (j + NCU * (a + NPV * k))] = acc[b][h];
+                        }
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int f2 = 8 * b + 2 * gc + h;
+                            if (f2 < NDF) Fe[i + NPV * (j + NCU * (k + NCH * f2))] = accf[b][h];
+                        }
+                }
+            }
+        }
+        // ---- Ru = Ru_vol + P Rh (fhat on every face) and ||Ru||^2
+        double ru2 = 0.0;
+        for (int t = tid; t < N; t += NT) {
+            const int i = t % NPV, j = t / NPV;
+            double s = 0.0;
+            for (int q = 0; q < NQ; q++) s += sm.Av[i + G::LDAV * q] * sm.wrk[q + NQ * j];
+            for (int c2 = 0; c2 < sm.inc_n[i]; c2++) s += sm.rh[j + NCH * sm.inc_f[i * S::MAXINC + c2]];
+            A.Ru[(size_t)e * N + t] = s;
+            ru2 += s * s;
+        }
+        const double tot = block_sum(ru2, sm.red);
+        if (tid == 0) A.ru2[e] = tot;
+
+        // ---- K and H face by face: rows (ip, j, m), k = (q, d'), generated A = shapfg(ip,q) x fhn.
+        // store: the rows are the face's trace equations (K, H); liftD / liftF:
+        // they are added to the element equations of the face's nodes
+        // (D += P K, F += P H) by reductions in L2, face after face
+        auto face_rows = [&](int fc, const double* slices, bool store, bool liftD, bool liftF) {
+            __syncthreads();
+            double* BK = Bs;                              // KFD x NKP  (ld LDBK)
+            double* BH = Bs + G::LDBK * G::NKP;           // KFD x NHP  (ld LDBK)
+            double* sfu = Bs + G::BKH;                    // the face's slices
+            double* sfuh = sfu + NGF * NCH * NC;
+            for (int t = tid; t < G::KFD * G::NKP; t += NT) {
+                const int k = t % G::KFD, a = t / G::KFD, q = k % NGF, dp = k / NGF;
+                double x = 0.0;
+                if (a < NPV && k < NGF * ND1) {
+                    if (dp == 0) {
+                        const int p = sm.pos[fc * NPV + a];
+                        x = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
+                    } else {
+                        const double* cm = Cm + NPV * (a + NPV * (dp - 1));
+                        for (int m = 0; m < NPF; m++) x += sm.sfc[q + NGF * m] * cm[sm.perm[fc * NPF + m]];
+                    }
+                }
+                BK[k + G::LDBK * a] = x;
+            }
+            for (int t = tid; t < G::KFD * G::NHP; t += NT) {
+                const int k = t % G::KFD, f2 = t / G::KFD, q = k % NGF, dp = k / NGF;
+                double x = 0.0;
+                if (f2 < NDF && k < NGF * ND1) {
+                    if (dp == 0) {
+                        x = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
+                    } else {
+                        const double* em = Em + NPV * (f2 + NDF * (dp - 1));
+                        for (int m = 0; m < NPF; m++) x -= sm.sfc[q + NGF * m] * em[sm.perm[fc * NPF + m]];
+                    }
+                }
+                BH[k + G::LDBK * f2] = x;
+            }
+            for (int t = tid; t < G::FSL; t += NT) sfu[t] = slices[t];
+            __syncthreads();
+            constexpr int MTK = (NPF * NCH * NCU + 7) / 8;
+            for (int mt = warp; mt < MTK; mt += NT / 32) {
+                const int r = 8 * mt + gr;
+                const bool rv = r < NPF * NCH * NCU;
+                // j fastest: the 8 rows of a tile are 8 consecutive words of a K/H column
+                const int j = r % NCH, ip = (r / NCH) % NPF, m = r / (NPF * NCH);
+                const int inode = sm.perm[fc * NPF + ip];
+                double aK[G::KFD / 4], aH[G::KFD / 4];
+#pragma unroll
+                for (int ks = 0; ks < G::KFD / 4; ks++) {
+                    const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF;
+                    double vK = 0.0, vH = 0.0;
+                    if (rv && k < NGF * ND1) {
+                        const double sf = sm.Af[ip + G::LDAF * q];
+                        if (dp == 0) {
+                            vK = sf * sfu[q + NGF * (j + NCH * m)];
+                            vH = sf * sfuh[q + NGF * (j + NCH * m)];
+                        } else {
+                            vK = sf * sfu[q + NGF * (j + NCH * (NCU * dp + m))];
+                            vH = vK;
+                        }
+                    }
+                    aK[ks] = vK;
+                    aH[ks] = vH;
+                }
+                double acc[G::NTK][2];
+#pragma unroll
+                for (int b = 0; b < G::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < G::KFD / 4; ks++)
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++)
+                        dmma8x8x4(acc[b][0], acc[b][1], aK[ks], BK[(4 * ks + gc) + G::LDBK * (8 * b + gr)]);
+#pragma unroll
+                for (int b = 0; b < G::NTK; b++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int a = 8 * b + 2 * gc + h;
+                        if (rv && a < NPV) {
+                            if (store) Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = acc[b][h];
+                            if (liftD) atomicAdd(&De[inode + NPV * (j + NCU * (a + NPV * m))], acc[b][h]);
+                        }
+                    }
+                double acch[G::NTH][2];
+#pragma unroll
+                for (int b = 0; b < G::NTH; b++) acch[b][0] = acch[b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < G::KFD / 4; ks++)
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++)
+                        dmma8x8x4(acch[b][0], acch[b][1], aH[ks], BH[(4 * ks + gc) + G::LDBK * (8 * b + gr)]);
+#pragma unroll
+                for (int b = 0; b < G::NTH; b++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int f2 = 8 * b + 2 * gc + h;
+                        if (rv && f2 < NDF) {
+                            if (store) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[b][h];
+                            if (liftF) atomicAdd(&Fe[inode + NPV * (j + NCU * (m + NCH * f2))], acch[b][h]);
+                        }
+                    }
+            }
+        };
+        for (int fc = 0; fc < NFE; fc++) {
+            const bool bnd = bfe && bfe[fc] < 0;
+            // interior faces: the trace rows, lifted into D; boundary faces: fhat
+            // rows lifted into D and F
+            face_rows(fc, fsl + fc * G::FSL, !bnd, true, bnd);
+            if (bnd) {
+                // the boundary face's trace equations take the boundary flux
+                // (faceint 1075-1246)
+                for (int t = tid; t < NPF * NCH; t += NT) {
+                    const int j = t % NCH, ip = t / NCH;
+                    double s = 0.0;
+                    for (int q = 0; q < NGF; q++) s += sm.Af[ip + G::LDAF * q] * fnb[q + NGF * fc + NA * j];
+                    Rhe[j + NCH * (fc * NPF + ip)] = -s;
+                    Roe[j + NCH * (fc * NPF + ip)] = -s;
+                }
+                face_rows(fc, fslb + fc * G::FSL, true, false, false);
+            }
+        }
+    }
+}
+
+}  // namespace hfem

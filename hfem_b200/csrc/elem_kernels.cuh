@@ -1,7 +1,7 @@
 // Shared pieces of the HDG element kernels for sm_100a: element shapes and
 // arguments, geometry and q-equation matrices, the Cholesky helpers, the
 // face-block scatter, the residual norm, q recovery and the solution update.
-// The element assembly itself is element_kernel_v2 (elem_kernel_v2.cuh).
+// The element assembly itself is element_kernel (elem_kernel.cuh).
 //
 // Structure of the element blocks (restating elementassembly.cpp faceint
 // 717-1321): every face contribution to the element equations is the
@@ -52,7 +52,7 @@ struct ElemArgs {
     double fc_u, fc_q;
     int ne;
     double *D, *F, *K, *H, *Ru, *Rh, *Ro, *ru2;
-    double* ws;                 // gridDim.x workspace slots of V2<S>::WS doubles (element_kernel_v2)
+    double* ws;                 // gridDim.x workspace slots of EK<S>::WS doubles (element_kernel)
     // several problems in one mesh (NULL = the uniform values above): element ->
     // problem, and per problem [gamma, eps, Re, Pr, Mach, tau, tdep, fc_u]
     const int* eprob;
@@ -63,7 +63,7 @@ struct ElemArgs {
     const int* bcm;
     const double* bcs;
     int inviscid;               // 1: Euler flux (app.appname 0)
-    int e_begin = 0;            // element range [e_begin, ne) of this launch (element_kernel_v2)
+    int e_begin = 0;            // element range [e_begin, ne) of this launch
 };
 
 constexpr int NT = 256;         // threads per CTA for element kernels

@@ -22,7 +22,8 @@
 #include "krylov_kernels.cuh"
 #include "krylov_seg.cuh"
 #include "schur_kernels.cuh"
-#include "elem_kernel_v2.cuh"
+#include "elem_kernel.cuh"
+#include "lift.cuh"
 #include "schur_tc.cuh"
 #include "bilu0.cuh"
 #include "inverse_blocked.cuh"
@@ -107,13 +108,13 @@ const std::vector<GemmLaunch>& gemm_candidates() {
 
 struct Launch {
     int nd, npv, npf, ngv, ngf;
-    size_t ws2;                 // workspace doubles per CTA slot (element_kernel_v2)
+    size_t ws;                  // workspace doubles per CTA slot (element_kernel)
     size_t q_smem;
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
-    void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
-    void (*element2)(dim3, size_t, cudaStream_t, const ElemArgs&);
-    size_t elem2_smem;
-    const void* elem2_fn;
+    void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*, const LiftArgs&);
+    void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
+    size_t elem_smem;
+    const void* elem_fn;
     int inv_threads;
     size_t inv_smem;
     const void *q_fn, *inv_fn;
@@ -122,18 +123,19 @@ struct Launch {
     size_t tc_smem;
     const void* tc_fn;
     void (*scatter_h)(dim3, cudaStream_t, const ScatterArgs&);
-    void (*schur_fused)(cudaStream_t, int, const double*, const double*, const double*, double*, double*);
+    void (*schur_fused)(cudaStream_t, int, const double*, const double*, const double*, double*, double*,
+                        const LiftArgs&);
     size_t fused_smem;
     const void* fused_fn;
 };
 
 template <int N>
-void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info) {
-    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info);
+void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info, const LiftArgs& L) {
+    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info, L);
 }
 
 template <class S>
-void launch_element2(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel_v2<S><<<g, NT, sm, st>>>(a); }
+void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel<S><<<g, NT, sm, st>>>(a); }
 template <class S>
 void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
 template <class S>
@@ -155,24 +157,24 @@ struct FusedPick {
 };
 template <class S>
 void launch_schur_fused(cudaStream_t st, int ne, const double* Dinv, const double* F, const double* K, double* H,
-                        double* DinvF) {
+                        double* DinvF, const LiftArgs& L) {
     using P = FusedPick<S>;
     schur_fused_kernel<S::N, S::NB, P::BN, P::NW>
-        <<<(unsigned)(ne * P::Cfg::STRIPS), P::Cfg::THREADS, P::Cfg::SMEM, st>>>(ne, Dinv, F, K, H, DinvF);
+        <<<(unsigned)(ne * P::Cfg::STRIPS), P::Cfg::THREADS, P::Cfg::SMEM, st>>>(ne, Dinv, F, K, H, DinvF, L);
 }
 
 template <class S>
 Launch make_launch() {
     Launch L;
     L.nd = S::ND; L.npv = S::NPV; L.npf = S::NPF; L.ngv = S::NGV; L.ngf = S::NGF;
-    L.ws2 = V2<S>::WS;
+    L.ws = EK<S>::WS;
     L.q_smem = sizeof(QSmem<S>);
     L.getq = launch_getq<S>;
     L.q_fn = (const void*)getq_kernel<S>;
     L.inverse = launch_inverse<S::N>;
-    L.element2 = launch_element2<S>;
-    L.elem2_smem = sizeof(ElemSmemV2<S>);
-    L.elem2_fn = (const void*)element_kernel_v2<S>;
+    L.element = launch_element<S>;
+    L.elem_smem = sizeof(ElemSmem<S>);
+    L.elem_fn = (const void*)element_kernel<S>;
     L.inv_threads = InvBlk<S::N>::THREADS;
     L.inv_smem = InvBlk<S::N>::SMEM;
     L.inv_fn = (const void*)inverse_blocked_kernel<S::N>;
@@ -498,7 +500,7 @@ int ensure_assembly_buffers(hfem_ctx* c) {
     if ((rc = dalloc(c, &c->Ro, ne * nb))) return rc;
     if ((rc = dalloc(c, &c->ru2, ne))) return rc;
     if ((rc = dalloc(c, &c->info, ne))) return rc;
-    if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws2))) return rc;
+    if ((rc = dalloc(c, &c->ws, (size_t)c->grid_elem * c->L->ws))) return rc;
     if ((rc = dalloc(c, &c->tc_err, 1))) return rc;
     if ((rc = dalloc(c, &c->rn_part, RNORM_CTAS))) return rc;
     CK(cudaMemsetAsync(c->tc_err, 0, sizeof(int), c->stream));
@@ -540,6 +542,21 @@ ScatterArgs scatter_args(hfem_ctx* c) {
     return s;
 }
 
+// The interior-face lift D += P K (src = K, n columns) or F += P H (src = H,
+// nb columns) applied by the condensation kernels (lift.cuh).
+LiftArgs lift_args(hfem_ctx* c, const double* src, int cols) {
+    LiftArgs L;
+    L.src = src;
+    L.perm = c->perm;
+    L.bf = c->bf;
+    L.npv = c->dims.npv;
+    L.npf = c->dims.npf;
+    L.nfe = c->dims.nfe;
+    L.nch = c->nch;
+    L.cols = cols;
+    return L;
+}
+
 int ready(hfem_ctx* c) {
     if (!c) return HFEM_E_ARG;
     if (!c->have_master || !c->have_mesh || !c->have_phys || !c->have_sol)
@@ -562,12 +579,12 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
                 ElemArgs a = elem_args(c);
                 a.e_begin = c->chunk_lo[k];
                 a.ne = c->chunk_lo[k + 1];
-                c->L->element2(ge, c->L->elem2_smem, c->stream, a);
+                c->L->element(ge, c->L->elem_smem, c->stream, a);
                 if ((rc = check_launch(c, "element"))) return rc;
             }
             c->pending_chunks = 0;
         } else {
-            c->L->element2(ge, c->L->elem2_smem, c->stream, elem_args(c));
+            c->L->element(ge, c->L->elem_smem, c->stream, elem_args(c));
             if ((rc = check_launch(c, "element"))) return rc;
         }
     }
@@ -576,18 +593,23 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
         const int ne = c->dims.ne, n = c->n, nb = c->nb;
         {
             Timed t(c, "inverse");
-            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
+            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info, LiftArgs{});
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
         if (c->precision == 0 && c->g1_sel < 0 && c->g2_sel < 0) {
             // both products in one kernel (tilings chosen by hfem_set_gemm_tiles
             // or hfem_autotune run the two batched GEMMs instead)
             Timed t(c, "schur_fused");
-            c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
+            c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF, lift_args(c, c->H, nb));
             if ((rc = check_launch(c, "schur_fused"))) return rc;
         } else if (c->precision == 0) {
             const GemmLaunch& g1 = c->g1_sel >= 0 ? gemm_candidates()[c->g1_sel] : c->L->g1;
             const GemmLaunch& g2 = c->g2_sel >= 0 ? gemm_candidates()[c->g2_sel] : c->L->g2;
+            {
+                Timed t(c, "lift_F");
+                lift_inplace_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(ne, n, lift_args(c, c->H, nb), c->F);
+                if ((rc = check_launch(c, "lift_F"))) return rc;
+            }
             {
                 Timed t(c, "gemm_DinvF");
                 g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb, 0.0,
@@ -602,7 +624,7 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
             }
         } else {
             Timed t(c, "schur_tc");
-            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err};
+            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err, lift_args(c, c->H, nb)};
             c->L->schur_tc(dim3(c->grid_tc), c->L->tc_smem, c->stream, ta);
             if ((rc = check_launch(c, "schur_tc"))) return rc;
         }
@@ -993,7 +1015,8 @@ int bj_blocked(hfem_ctx* c) {
     const int grid = std::max(1, std::min(nf, sms(c->device) * std::max(occ, 1)));
     // the kernel also solves with a right-hand side: c->w is free here and its
     // result is ignored
-    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->binfo);
+    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->binfo,
+                                                                                     LiftArgs{});
     return check_launch(c, "bj_inverse");
 }
 
@@ -1509,10 +1532,10 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     }
     c->stream = c->own;
     const Launch& L = *c->L;
-    cudaFuncSetAttribute(L.elem2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem2_smem);
+    cudaFuncSetAttribute(L.elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
     cudaFuncSetAttribute(L.q_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.q_smem);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem2_fn, NT, L.elem2_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn, NT, L.elem_smem);
     c->grid_elem = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
@@ -2110,10 +2133,11 @@ int hfem_autotune(hfem_ctx* c, int reps, int* best, double* ms) {
         }
     // the fused kernel does both products: kept when it beats the best pair
     {
-        c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);   // warm-up
+        const LiftArgs lf = lift_args(c, c->H, nb);
+        c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF, lf);   // warm-up
         if ((rc = check_launch(c, "autotune"))) return rc;
         CK(cudaEventRecord(e0, c->stream));
-        for (int r = 0; r < reps; r++) c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
+        for (int r = 0; r < reps; r++) c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF, lf);
         CK(cudaEventRecord(e1, c->stream));
         CK(cudaEventSynchronize(e1));
         float t = 0.f;
@@ -2255,7 +2279,6 @@ int device_buffer(hfem_ctx* c, int what, const double** src, size_t* need) {
         case 8: *src = c->udg; *need = (size_t)d.ne * d.npv * c->nc; break;
         case 9: *src = c->uh; *need = (size_t)d.nf * d.npf * c->nch; break;
         case 10: *src = c->K; *need = (size_t)d.ne * c->nb * c->n; break;
-        case 11: *src = c->F; *need = (size_t)d.ne * c->n * c->nb; break;
         case 12: *src = c->Ro; *need = (size_t)d.ne * c->nb; break;
         case 13: *src = c->D; *need = (size_t)d.ne * c->n * c->n; break;
         case 14: *src = c->ru2; *need = (size_t)d.ne; break;
@@ -2363,7 +2386,7 @@ int hfem_fp64_peak(int device, double* tflops) {
 // RMM allocator, where a raw cudaMalloc synchronises the device and fragments
 // the pool), serving loops that reserve HBM once at admission and may not
 // allocate per request, and host codes that register a fixed set of buffers.
-// It runs the kernels of hfem_assemble (element_kernel_v2, the blocked
+// It runs the kernels of hfem_assemble (element_kernel, the blocked
 // Gauss-Jordan inverse, the fused condensation and Rh - K D^-1 Ru), so its
 // blocks equal that path's; only the element kernel's per-CTA workspace lives
 // in the file-scope array below instead of a context buffer.  The array's size
@@ -2409,7 +2432,7 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
             li = (int)k;
     if (li < 0) return HFEM_E_UNSUPPORTED;
     const Launch* L = &all[li];
-    const size_t slot_bytes = L->ws2 * sizeof(double);
+    const size_t slot_bytes = L->ws * sizeof(double);
     if (slot_bytes > HFEM_NOALLOC_SCRATCH_BYTES) return HFEM_E_ARG;   // one CTA's workspace exceeds the scratch
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HFEM_E_CUDA;
@@ -2427,7 +2450,7 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
         scratch = g_noalloc_ptr[dev];
         NoallocGrids& G = g_noalloc_grids[dev][li];
         if (!G.ready) {
-            if (cudaFuncSetAttribute(L->elem2_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->elem2_smem) !=
+            if (cudaFuncSetAttribute(L->elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->elem_smem) !=
                     cudaSuccess ||
                 cudaFuncSetAttribute(L->inv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->inv_smem) !=
                     cudaSuccess ||
@@ -2435,7 +2458,7 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
                     cudaSuccess)
                 return HFEM_E_CUDA;
             int occ = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->elem2_fn, NT, L->elem2_smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L->elem_fn, NT, L->elem_smem);
             const int slots = (int)(HFEM_NOALLOC_SCRATCH_BYTES / slot_bytes);
             G.elem = std::max(1, std::min(slots, sms(dev) * std::max(occ, 1)));
             occ = 0;
@@ -2471,11 +2494,20 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.bcm = bcm;
     a.bcs = bcs;
     a.inviscid = appname == 0;
-    L->element2(dim3(ge), L->elem2_smem, st, a);
+    L->element(dim3(ge), L->elem_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
-    L->inverse(dim3(gi), st, d.ne, D, DinvRu, info);
+    L->inverse(dim3(gi), st, d.ne, D, DinvRu, info, LiftArgs{});
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
-    L->schur_fused(st, d.ne, D, DinvF, K, H, DinvF);
+    LiftArgs lh;
+    lh.src = H;
+    lh.perm = perm;
+    lh.bf = bf;
+    lh.npv = d.npv;
+    lh.npf = d.npf;
+    lh.nfe = d.nfe;
+    lh.nch = d.nd + 2;
+    lh.cols = nb;
+    L->schur_fused(st, d.ne, D, DinvF, K, H, DinvF, lh);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     batched_dgemv_kernel<<<sms(dev) * 8, 256, 0, st>>>(d.ne, nb, n, -1.0, K, (long long)nb * n, DinvRu, n, Rh, nb);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;

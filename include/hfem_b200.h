@@ -236,8 +236,8 @@ int hfem_gmres_problems(hfem_ctx* ctx, int precond, int restart, double tol, int
  * what = 0 Hg (nblocks*bsz^2), 1 Rg (nf*bsz), 2 Rr = sum of uncondensed Rh
  * (nf*bsz), 3 DinvRu (n*ne), 4 DinvF (n*nb*ne), 5 condensed element H
  * (nb*nb*ne), 6 condensed element Rh (nb*ne), 7 GMRES solution x (nf*bsz),
- * 10 element K (nb*n*ne), 11 element F before condensation (n*nb*ne),
- * 12 element Rh before condensation (nb*ne), 13 element D^-1 after an
+ * 10 element K (nb*n*ne), 12 element Rh before condensation (nb*ne),
+ * 13 element D^-1 after an
  * assembly (n*n*ne; D itself after a residual-only pass), 14 ||Ru_e||^2 before
  * condensation (ne). */
 int hfem_download(hfem_ctx* ctx, int what, double* host, size_t count);

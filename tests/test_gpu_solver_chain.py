@@ -16,7 +16,7 @@ Pins, through the C ABI, what single assemblies do not:
   step against the reference driver (``ns2d_p2_n32_newton1.npz``) at 1e-12 of
   the first residual.
 * the full-size 3D workload (20^3 x 6 = 48,000 tetrahedra, p = 3): 64 seeded
-  elements' blocks (K, F and Rh before condensation, D^-1, the condensed H, Rh,
+  elements' blocks (K and Rh before condensation, D^-1, the condensed H, Rh,
   D^-1 F and D^-1 Ru) against the oracle's element routine, condensed with
   numpy, at 1e-12 relative to each array's largest entry (D^-1 Ru, a residual:
   1e-12 of max(|D^-1 Ru|, 1), as the other residual checks).
@@ -173,7 +173,7 @@ def test_full_size_3d_sampled_elements_match_oracle():
         s.getQ()
         s.assembleLinearSystem()
         udg, uh = s.get_solution()
-        got = {k: s.download_elements(k, elems) for k in ("K", "F", "Ro", "Dinv", "H", "Rh", "DinvF", "DinvRu")}
+        got = {k: s.download_elements(k, elems) for k in ("K", "Ro", "Dinv", "H", "Rh", "DinvF", "DinvRu")}
     finally:
         s.close()
     o = Oracle(prob)
@@ -187,7 +187,6 @@ def test_full_size_3d_sampled_elements_match_oracle():
         Dinv = np.linalg.inv(D)
         DinvF, DinvRu = Dinv @ F, Dinv @ e["Ru"]
         ref["K"].append(e["K"])
-        ref["F"].append(e["F"])
         ref["Ro"].append(e["Rh"])
         ref["Dinv"].append(Dinv.ravel(order="F"))
         ref["DinvF"].append(DinvF.ravel(order="F"))
