@@ -40,33 +40,7 @@ static std::vector<int> g_gmres_iters;
 static std::vector<double> g_newton_rnorm;
 static solstruct* g_sol = nullptr;
 
-void dmdserial(sysstruct& sys, meshstruct& mesh, appstruct& app)
-{
-    const Int nf = mesh.nf, ne = mesh.ne, nfe = mesh.nfemax;
-    std::vector<std::set<Int> > rows(nf);
-    for (Int e = 0; e < ne; e++)
-        for (Int a = 0; a < nfe; a++)
-            for (Int b = 0; b < nfe; b++)
-                rows[mesh.t2f[e * nfe + a]].insert(mesh.t2f[e * nfe + b]);
-    sys.ent2entStart.assign(nf + 1, 0);
-    sys.ent2ent.clear();
-    Int maxrow = 0;
-    for (Int i = 0; i < nf; i++) {
-        sys.ent2ent.push_back(i);
-        for (Int j : rows[i]) if (j != i) sys.ent2ent.push_back(j);
-        sys.ent2entStart[i + 1] = (Int)sys.ent2ent.size();
-        maxrow = std::max(maxrow, sys.ent2entStart[i + 1] - sys.ent2entStart[i]);
-    }
-    sys.numEntities = nf;
-    sys.numBlocks = (Int)sys.ent2ent.size();
-    sys.blkSize = app.nch * mesh.npfmax;
-    sys.maxBlocksPerRow = maxrow;
-    sys.BJ_nrows = nf;
-    sys.nproc = 1;
-    sys.nentrecv = sys.nentsend = sys.nelemrecv = sys.nelemsend = 0;
-    sys.nvecrecv = sys.nvecsend = sys.nmatrecv = sys.nmatsend = 0;
-    sys.nnbsd = 0;
-}
+#include "ref_dmdserial.cpp"
 
 void computeOrdering(sysstruct& sys, Int preconditioner)
 {
