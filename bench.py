@@ -436,33 +436,59 @@ def run_newton_task(args):
 
 
 def run_dirk_task(args):
-    """Config 4: Taylor-Green 16^3 x 6 tets, p = 3, Re 1600, Mach 0.1, DIRK(3,3), dt = 0.01."""
+    """Config 4: Taylor-Green 16^3 x 6 tets, p = 3, Re 1600, Mach 0.1, DIRK(3,3),
+    dt = 0.01, 20 steps, in mixed precision (FP32 preconditioner and TF32
+    condensation GEMMs, FP64 Newton residual, Arnoldi and update) by default.
+    The same steps in FP64 give the mixed run's kinetic-energy error against
+    FP64; the 4^3 x 6 Taylor-Green case, 20 steps in the same precision, is
+    checked against the reference driver's kinetic-energy history
+    (tests/golden/tgv_p3_n4_dirk20.npz)."""
     import torch
     from hfem_b200.core import HDGSolver
     from hfem_b200.diagnostics import kinetic_energy
     from hfem_b200.gen.problem import ns3d_tgv
-    prob = ns3d_tgv(n=args.tgv_n, porder=3, dt=0.01)
-    s = HDGSolver(prob)
-    st = torch.cuda.current_stream()
-    s.set_stream(st.cuda_stream)
-    s.getQ()
-    u, _ = s.get_solution()
-    ke = [kinetic_energy(prob, u)]
-    iters, times = [], []
-    for _ in range(args.dirk_steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        iters.append(s.solveUnsteadyStep(0.01, stages=3, order=3, newton_tol=args.dirk_tol))
-        e1.record(st)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
+
+    def run(n, precision, steps, timed):
+        prob = ns3d_tgv(n=n, porder=3, dt=0.01)
+        s = HDGSolver(prob)
+        st = torch.cuda.current_stream()
+        s.set_stream(st.cuda_stream)
+        s.set_precision(precision)
+        s.getQ()
         u, _ = s.get_solution()
-        ke.append(kinetic_energy(prob, u))
-    s.close()
-    return {"metric": f"DIRK(3,3) time steps/s (3D TGV {args.tgv_n}^3x6 tets = {prob.mesh.ne} elements, p=3)",
-            "value": 1e3 / float(np.mean(times)), "unit": "steps/s", "impl": "hfem", "dtype": "f64",
-            "ms_per_step": float(np.mean(times)), "steps": args.dirk_steps, "newton_iterations": iters,
-            "kinetic_energy": ke, "higher_is_better": True}
+        ke = [kinetic_energy(prob, u)]
+        iters, times = [], []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            iters.append(s.solveUnsteadyStep(0.01, stages=3, order=3, newton_tol=args.dirk_tol))
+            e1.record(st)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            u, _ = s.get_solution()
+            ke.append(kinetic_energy(prob, u))
+        s.close()
+        return prob, np.array(ke), iters, times
+
+    prob, ke, iters, times = run(args.tgv_n, args.dirk_precision, args.dirk_steps, True)
+    out = {"metric": f"DIRK(3,3) time steps/s (3D TGV {args.tgv_n}^3x6 tets = {prob.mesh.ne} elements, p=3)",
+           "value": 1e3 / float(np.mean(times)), "unit": "steps/s", "impl": "hfem",
+           "dtype": "mixed: f32 preconditioner, tf32 condensation GEMMs, f64 Newton/Arnoldi"
+                    if args.dirk_precision == 1 else "f64",
+           "ms_per_step": float(np.mean(times)), "steps": args.dirk_steps, "newton_iterations": iters,
+           "newton_tol": args.dirk_tol, "kinetic_energy": ke.tolist(), "higher_is_better": True}
+    if args.dirk_precision == 1:
+        _, ke64, it64, t64 = run(args.tgv_n, 0, args.dirk_steps, True)
+        out["fp64"] = {"ms_per_step": float(np.mean(t64)), "newton_iterations": it64,
+                       "kinetic_energy_rel_diff": float(np.max(np.abs(ke - ke64) / ke64))}
+    gfile = os.path.join(ROOT, "tests", "golden", "tgv_p3_n4_dirk20.npz")
+    if os.path.exists(gfile):
+        g = dict(np.load(gfile))
+        _, ke4, _, _ = run(int(g["n"][0]), args.dirk_precision, int(g["nsteps"][0]), False)
+        out["reference_check"] = {"case": "TGV 4^3x6 tets, p=3, 20 DIRK(3,3) steps of dt 0.01",
+                                  "kinetic_energy_rel_err_vs_reference_driver": float(np.max(np.abs(ke4 - g["ke"])
+                                                                                              / g["ke"]))}
+    return out
 
 
 def run_serve_task(args):
@@ -583,7 +609,8 @@ def main():
     ap.add_argument("--batched-seed", type=int, default=0)
     ap.add_argument("--tgv-n", type=int, default=16)
     ap.add_argument("--dirk-steps", type=int, default=20)
-    ap.add_argument("--dirk-tol", type=float, default=1e-9)
+    ap.add_argument("--dirk-tol", type=float, default=1e-10)
+    ap.add_argument("--dirk-precision", type=int, default=1, choices=[0, 1])
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[20.0, 50.0, 100.0])
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-seq-requests", type=int, default=200)

@@ -148,14 +148,17 @@ struct BiluSolveArgs {
     const int* u2o;
     const int* rows;
     int nrows;
-    const double* Mg;
+    const void* Mg;         // factors, double or float (FP32 factors in mixed precision)
     const double* x;        // right-hand side (lower solve)
     double* y;              // lower: y = L^-1 x; upper: in y, out v
     double* v;
 };
 
 // Lower solve of one level: y_i = x_i - sum_{k earlier} L_ik y_k (one CTA per row).
+// MT is the factors' type; vectors and sums are FP64.
+template <class MT>
 __global__ void __launch_bounds__(64) bilu0_lower_kernel(BiluSolveArgs A) {
+    const MT* Mg = static_cast<const MT*>(A.Mg);
     const int b = A.bsz;
     const size_t b2 = (size_t)b * b;
     for (int w = blockIdx.x; w < A.nrows; w += gridDim.x) {
@@ -165,10 +168,10 @@ __global__ void __launch_bounds__(64) bilu0_lower_kernel(BiluSolveArgs A) {
             for (int p = A.rowstart[i] + 1; p < A.rowstart[i + 1]; p++) {
                 const int k = A.colidx[p];
                 if (A.u2o[k] >= oi) continue;
-                const double* L = A.Mg + (size_t)p * b2;
+                const MT* L = Mg + (size_t)p * b2;
                 const double* yk = A.y + (size_t)k * b;
                 double s = 0.0;
-                for (int c = 0; c < b; c++) s += L[r + b * c] * yk[c];
+                for (int c = 0; c < b; c++) s += (double)L[r + b * c] * yk[c];
                 t -= s;
             }
             A.y[(size_t)i * b + r] = t;
@@ -177,8 +180,10 @@ __global__ void __launch_bounds__(64) bilu0_lower_kernel(BiluSolveArgs A) {
 }
 
 // Upper solve of one level: v_i = U_ii^-1 (y_i - sum_{k later} U_ik v_k).
+template <class MT>
 __global__ void __launch_bounds__(64) bilu0_upper_kernel(BiluSolveArgs A) {
     __shared__ double t[64];
+    const MT* Mg = static_cast<const MT*>(A.Mg);
     const int b = A.bsz;
     const size_t b2 = (size_t)b * b;
     for (int w = blockIdx.x; w < A.nrows; w += gridDim.x) {
@@ -189,19 +194,19 @@ __global__ void __launch_bounds__(64) bilu0_upper_kernel(BiluSolveArgs A) {
             for (int p = A.rowstart[i] + 1; p < A.rowstart[i + 1]; p++) {
                 const int k = A.colidx[p];
                 if (A.u2o[k] <= oi) continue;
-                const double* U = A.Mg + (size_t)p * b2;
+                const MT* U = Mg + (size_t)p * b2;
                 const double* vk = A.v + (size_t)k * b;
                 double d = 0.0;
-                for (int c = 0; c < b; c++) d += U[r + b * c] * vk[c];
+                for (int c = 0; c < b; c++) d += (double)U[r + b * c] * vk[c];
                 s -= d;
             }
             t[r] = s;
         }
         __syncthreads();
-        const double* Dinv = A.Mg + (size_t)A.rowstart[i] * b2;
+        const MT* Dinv = Mg + (size_t)A.rowstart[i] * b2;
         for (int r = threadIdx.x; r < b; r += blockDim.x) {
             double s = 0.0;
-            for (int c = 0; c < b; c++) s += Dinv[r + b * c] * t[c];
+            for (int c = 0; c < b; c++) s += (double)Dinv[r + b * c] * t[c];
             A.v[(size_t)i * b + r] = s;
         }
     }
@@ -211,11 +216,13 @@ __global__ void __launch_bounds__(64) bilu0_upper_kernel(BiluSolveArgs A) {
 // CTA barrier in between: for orderings whose levels hold few rows (MDF gives
 // long dependency chains) this replaces two launches per level by one launch.
 // Each warp takes one row of the level at a time; lanes own the row's entries.
+template <class MT>
 __global__ void __launch_bounds__(1024) bilu0_apply_cta_kernel(BiluSolveArgs A, const int* __restrict__ lvl_lo,
                                                                int nlo, const int* __restrict__ rows_lo,
                                                                const int* __restrict__ lvl_up, int nup,
                                                                const int* __restrict__ rows_up) {
     __shared__ double t[32][64];
+    const MT* Mg = static_cast<const MT*>(A.Mg);
     const int b = A.bsz;
     const size_t b2 = (size_t)b * b;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -227,10 +234,10 @@ __global__ void __launch_bounds__(1024) bilu0_apply_cta_kernel(BiluSolveArgs A, 
                 for (int p = A.rowstart[i] + 1; p < A.rowstart[i + 1]; p++) {
                     const int k = A.colidx[p];
                     if (A.u2o[k] >= oi) continue;
-                    const double* L = A.Mg + (size_t)p * b2;
+                    const MT* L = Mg + (size_t)p * b2;
                     const double* yk = A.y + (size_t)k * b;
                     double d = 0.0;
-                    for (int c = 0; c < b; c++) d += L[r + b * c] * yk[c];
+                    for (int c = 0; c < b; c++) d += (double)L[r + b * c] * yk[c];
                     s -= d;
                 }
                 A.y[(size_t)i * b + r] = s;
@@ -246,19 +253,19 @@ __global__ void __launch_bounds__(1024) bilu0_apply_cta_kernel(BiluSolveArgs A, 
                 for (int p = A.rowstart[i] + 1; p < A.rowstart[i + 1]; p++) {
                     const int k = A.colidx[p];
                     if (A.u2o[k] <= oi) continue;
-                    const double* U = A.Mg + (size_t)p * b2;
+                    const MT* U = Mg + (size_t)p * b2;
                     const double* vk = A.v + (size_t)k * b;
                     double d = 0.0;
-                    for (int c = 0; c < b; c++) d += U[r + b * c] * vk[c];
+                    for (int c = 0; c < b; c++) d += (double)U[r + b * c] * vk[c];
                     s -= d;
                 }
                 t[w][r] = s;
             }
             __syncwarp();
-            const double* Dinv = A.Mg + (size_t)A.rowstart[i] * b2;
+            const MT* Dinv = Mg + (size_t)A.rowstart[i] * b2;
             for (int r = lane; r < b; r += 32) {
                 double s = 0.0;
-                for (int c = 0; c < b; c++) s += Dinv[r + b * c] * t[w][c];
+                for (int c = 0; c < b; c++) s += (double)Dinv[r + b * c] * t[w][c];
                 A.v[(size_t)i * b + r] = s;
             }
             __syncwarp();

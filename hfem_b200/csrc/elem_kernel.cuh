@@ -50,20 +50,23 @@ struct EK {
     // one face's flux-Jacobian slices: [q + NGF (j + NCH c)], c < NC for fhn_u / fb_u,
     // then NGF NCH NCU entries for fhn_uh / fb_uh
     static constexpr int FSL = S::NGF * S::NCH * (S::NC + S::NCU);
+    static constexpr int FSLP = (FSL + 1) / 2 * 2;                 // per-face stride: 16-byte copies
     // shared-memory union: M^-1 C and M^-1 E, then either the q/flux phase
     // scratch or the B operand of the GEMM being run
     static constexpr int CME = S::NPV * S::NPV * S::ND + S::NPV * S::NDF * S::ND;
     static constexpr int QPH = S::NPV * S::NPV + S::NGV * S::NC + S::NA * (S::NC + S::NCH) + S::NPV * S::NC +
                                S::NDF * S::NCH + S::NPV * S::NCU;
-    static constexpr int GPH = BDF > BKH + FSL ? BDF : BKH + FSL;
+    static constexpr int GPH = BDF > BKH + FSLP ? BDF : BKH + FSLP;
     static constexpr int UN = CME + (QPH > GPH ? QPH : GPH);
     // global workspace per CTA slot (doubles): wrl, the interior and boundary
     // face slices, the boundary flux values, Y
     static constexpr int W_WRL = S::NQ * S::NCU * S::NC;
-    static constexpr int W_FSL = S::NFE * FSL;
+    static constexpr int W_FSL = S::NFE * FSLP;
     static constexpr int W_FNB = S::NA * S::NCH;
     static constexpr int W_Y = S::NPV * S::NGV * S::NCU * S::NC;
     static constexpr int WS = W_WRL + 2 * W_FSL + W_FNB + W_Y;
+    static_assert(CME % 2 == 0 && BKH % 2 == 0 && W_WRL % 2 == 0 && WS % 2 == 0,
+                  "16-byte alignment of the staged face slices");
 };
 
 template <class S>
@@ -78,7 +81,7 @@ struct ElemSmem {
     double Af[EK<S>::LDAF * EK<S>::KF];    // shapfg, zero padded: Af[ip + LDAF*q]
     double sfc[S::NGF * S::NPF];           // face basis values shapfc(kk, q) = shapft[q + NGF*kk]
     double red[NT / 32];
-    double un[EK<S>::UN];
+    alignas(16) double un[EK<S>::UN];
     int perm[S::NDF];
     int inc_n[S::NPV];
     int inc_f[S::NPV * S::MAXINC];
@@ -237,7 +240,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                     const double tau = P[5];
                     const double jf = sm.jacf[g];
                     const int fc = g / NGF, q = g % NGF;
-                    double* sl = fsl + fc * G::FSL;
+                    double* sl = fsl + fc * G::FSLP;
 #pragma unroll
                     for (int j = 0; j < NCU; j++) {
                         if (k == 0) {
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                         for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
                     }
                     const double jf = sm.jacf[gg];
-                    double* sl = fslb + fc * G::FSL;
+                    double* sl = fslb + fc * G::FSLP;
 #pragma unroll
                     for (int j = 0; j < NCH; j++) {
                         if (k == 0) fnb[gg + NA * j] = fb[j].v * jf;
@@ -446,6 +449,9 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             double* BH = Bs + G::LDBK * G::NKP;           // KFD x NHP  (ld LDBK)
             double* sfu = Bs + G::BKH;                    // the face's slices
             double* sfuh = sfu + NGF * NCH * NC;
+            // the slices arrive by 16-byte asynchronous copies while B is built
+            for (int t = tid; t < G::FSLP / 2; t += NT) cp_async16z(sfu + 2 * t, slices + 2 * t, true);
+            cp_async_commit();
             for (int t = tid; t < G::KFD * G::NKP; t += NT) {
                 const int k = t % G::KFD, a = t / G::KFD, q = k % NGF, dp = k / NGF;
                 double x = 0.0;
@@ -473,7 +479,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                 }
                 BH[k + G::LDBK * f2] = x;
             }
-            for (int t = tid; t < G::FSL; t += NT) sfu[t] = slices[t];
+            cp_async_wait<0>();
             __syncthreads();
             constexpr int MTK = (NPF * NCH * NCU + 7) / 8;
             for (int mt = warp; mt < MTK; mt += NT / 32) {
@@ -521,11 +527,16 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                 double acch[G::NTH][2];
 #pragma unroll
                 for (int b = 0; b < G::NTH; b++) acch[b][0] = acch[b][1] = 0.0;
+                // the d' = 0 rows of BH are zero outside the face's own columns
+                // fc NPF .. fc NPF + NPF - 1: those n-tiles are skipped there
+                const int blo = (fc * NPF) / 8, bhi = (fc * NPF + NPF - 1) / 8;
 #pragma unroll
                 for (int ks = 0; ks < G::KFD / 4; ks++)
 #pragma unroll
-                    for (int b = 0; b < G::NTH; b++)
+                    for (int b = 0; b < G::NTH; b++) {
+                        if (4 * ks + 3 < NGF && (b < blo || b > bhi)) continue;
                         dmma8x8x4(acch[b][0], acch[b][1], aH[ks], BH[(4 * ks + gc) + G::LDBK * (8 * b + gr)]);
+                    }
 #pragma unroll
                 for (int b = 0; b < G::NTH; b++)
 #pragma unroll
@@ -542,7 +553,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             const bool bnd = bfe && bfe[fc] < 0;
             // interior faces: the trace rows, lifted into D; boundary faces: fhat
             // rows lifted into D and F
-            face_rows(fc, fsl + fc * G::FSL, !bnd, true, bnd);
+            face_rows(fc, fsl + fc * G::FSLP, !bnd, true, bnd);
             if (bnd) {
                 // the boundary face's trace equations take the boundary flux
                 // (faceint 1075-1246)
@@ -553,7 +564,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                     Rhe[j + NCH * (fc * NPF + ip)] = -s;
                     Roe[j + NCH * (fc * NPF + ip)] = -s;
                 }
-                face_rows(fc, fslb + fc * G::FSL, true, false, false);
+                face_rows(fc, fslb + fc * G::FSLP, true, false, false);
             }
         }
     }

@@ -274,6 +274,7 @@ struct hfem_ctx {
     int *d_lvl_lo = nullptr, *d_lvl_up = nullptr;
     cudaGraphExec_t bilu_exec = nullptr;    // the factorisation's per-level launches, replayed as one graph
     double *Mg = nullptr, *bl_t = nullptr, *bl_y = nullptr;
+    float* Mg32 = nullptr;              // FP32 copy of the BILU0 factors (mixed precision)
     int prec_kind = 2;                  // preconditioner of the current GMRES: 2 BJ, 0 BILU0, -1 none
     KernelTimer timer;
 };
@@ -933,29 +934,44 @@ int bilu0_factor(hfem_ctx* c) {
     CK(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < nf; i++)
         if (bi[i]) return fail(c, HFEM_E_SINGULAR, "BILU0: singular pivot block at face %d", i);
+    if (c->precision == 1) {
+        // mixed precision: the triangular solves read FP32 factors (FP64 vectors and sums)
+        const long long nm = (long long)b2 * c->dims.nblocks;
+        if (!c->Mg32 && (rc = dalloc(c, &c->Mg32, (size_t)nm))) return rc;
+        to_float_kernel<<<sms(c->device) * 4, 256, 0, c->stream>>>(nm, c->Mg, c->Mg32);
+        if ((rc = check_launch(c, "bilu0_factor fp32"))) return rc;
+    }
     return 0;
 }
 
 // v = (L U)^-1 x (applyBILU0.m); v may not alias x.
 int bilu0_apply(hfem_ctx* c, const double* x, double* v) {
     Timed t(c, "bilu0_apply");
-    BiluSolveArgs a{c->bsz, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, c->Mg, x, c->bl_y, v};
+    const bool f32 = c->precision == 1 && c->Mg32;
+    BiluSolveArgs a{c->bsz, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, f32 ? (const void*)c->Mg32 : c->Mg, x,
+                    c->bl_y, v};
     const int nlo = (int)c->lvl_lo.size() - 1, nup = (int)c->lvl_up.size() - 1;
     // few rows per level: one CTA walks all levels (no launch per level)
     if ((long long)c->dims.nf < 64LL * std::max(nlo, nup)) {
-        bilu0_apply_cta_kernel<<<1, 1024, 0, c->stream>>>(a, c->d_lvl_lo, nlo, c->d_rows_lo, c->d_lvl_up, nup,
-                                                          c->d_rows_up);
+        if (f32)
+            bilu0_apply_cta_kernel<float><<<1, 1024, 0, c->stream>>>(a, c->d_lvl_lo, nlo, c->d_rows_lo, c->d_lvl_up,
+                                                                     nup, c->d_rows_up);
+        else
+            bilu0_apply_cta_kernel<double><<<1, 1024, 0, c->stream>>>(a, c->d_lvl_lo, nlo, c->d_rows_lo, c->d_lvl_up,
+                                                                      nup, c->d_rows_up);
         return check_launch(c, "bilu0_apply");
     }
     for (size_t l = 0; l + 1 < c->lvl_lo.size(); l++) {
         a.rows = c->d_rows_lo + c->lvl_lo[l];
         a.nrows = c->lvl_lo[l + 1] - c->lvl_lo[l];
-        bilu0_lower_kernel<<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
+        if (f32) bilu0_lower_kernel<float><<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
+        else bilu0_lower_kernel<double><<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
     }
     for (size_t l = 0; l + 1 < c->lvl_up.size(); l++) {
         a.rows = c->d_rows_up + c->lvl_up[l];
         a.nrows = c->lvl_up[l + 1] - c->lvl_up[l];
-        bilu0_upper_kernel<<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
+        if (f32) bilu0_upper_kernel<float><<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
+        else bilu0_upper_kernel<double><<<std::min(a.nrows, sms(c->device) * 16), 64, 0, c->stream>>>(a);
     }
     return check_launch(c, "bilu0_apply");
 }
@@ -1577,7 +1593,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
                     c->seg_ticket, c->seg_part, c->seg_partk, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
-                    c->d_lvl_lo, c->d_lvl_up};
+                    c->d_lvl_lo, c->d_lvl_up, c->Mg32};
     for (void* p : ptrs)
         if (p) pool_free(p);
     for (auto& p : c->timer.pending) {

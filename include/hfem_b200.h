@@ -157,10 +157,10 @@ int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newto
 /* Arithmetic of the assembly and solve (no counterpart in the reference, which
  * is FP64 throughout).  mode 0: FP64 everywhere (default).  mode 1: the two
  * Schur GEMMs (D^-1 F and H - K D^-1 F) on the tcgen05 tensor cores in TF32
- * with FP32 accumulation, and the block-Jacobi preconditioner applied with FP32
- * inverses; the element LU, the residuals (rnorm), the Arnoldi process and the
- * Newton update stay FP64, so Newton iterations refine the solution to the
- * FP64 residual tolerance. */
+ * with FP32 accumulation, and the preconditioner applied with FP32 factors
+ * (block-Jacobi inverses, BILU0 factors); the element LU, the residuals
+ * (rnorm), the Arnoldi process and the Newton update stay FP64, so Newton
+ * iterations refine the solution to the FP64 residual tolerance. */
 int hfem_set_precision(hfem_ctx* ctx, int mode);
 
 /* The BILU0 ordering in use: ordered2unordered[i] = face pivoted at step i

@@ -73,3 +73,28 @@ def test_mixed_gmres_reaches_tolerance_with_fp32_preconditioner():
     assert c64 == 1 and c32 == 1
     # the mixed system differs from the FP64 one by TF32 rounding, not by the preconditioner
     assert rel(x32, x64) < 1e-2
+
+
+def test_mixed_newton_with_fp32_bilu0_factors():
+    """BILU0 (MDF order) with FP32 factors in mixed mode: Newton still reaches the
+    FP64 residual tolerance, and the GMRES iteration count stays within a few
+    of the FP64-factor run (the preconditioner changes the Krylov path only)."""
+    prob = ns2d_vortex(n=4, porder=2)
+    runs = {}
+    for mode in (0, 1):
+        s = HDGSolver(make_copy(prob))
+        s.set_precision(mode)
+        s.getQ()
+        s.assembleLinearSystem()
+        conv, hist = s.gmres(precond=0, restart=50, tol=1e-10)
+        runs[mode] = (conv, len(hist))
+        conv_n, nh = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=12, precond=0, gmres_tol=1e-10)
+        s.close()
+        assert conv_n == 1 and nh[-1] < 1e-10, nh
+    assert runs[0][0] == 1 and runs[1][0] == 1
+    assert abs(runs[1][1] - runs[0][1]) <= 3, runs
+
+
+def make_copy(prob):
+    import copy
+    return copy.deepcopy(prob)
