@@ -75,6 +75,8 @@ def load_library(path: str = LIB):
     lib.hfem_reset_ordering.argtypes = [C.c_void_p]
     lib.hfem_device_buffer.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t)]
     lib.hfem_kernel_times.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t, _dp, _ip, C.c_int]
+    lib.hfem_matvec.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.hfem_set_step.argtypes = [C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 
@@ -201,6 +203,19 @@ class HDGSolver:
         per = t.numel() // self.prob.mesh.ne
         idx = torch.as_tensor(np.asarray(elems, dtype=np.int64), device=t.device)
         return t.view(-1, per).index_select(0, idx).cpu().numpy()
+
+    def matvec(self, x):
+        """y = Hg x for a float64 CUDA tensor x on the context's device (after an assembly)."""
+        import torch
+        x = x.contiguous()
+        y = torch.empty_like(x)
+        self._chk(self.lib.hfem_matvec(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "matvec")
+        return y
+
+    def set_step(self, duh):
+        """Make duh (float64 CUDA tensor, nf*bsz) the step updateSol applies."""
+        duh = duh.contiguous()
+        self._chk(self.lib.hfem_set_step(self.h, C.c_void_p(duh.data_ptr())), "set_step")
 
     # -- reference surface ---------------------------------------------
     def getQ(self):

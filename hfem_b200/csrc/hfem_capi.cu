@@ -2248,6 +2248,27 @@ int hfem_graph_destroy(hfem_graph* g) {
     return 0;
 }
 
+int hfem_matvec(hfem_ctx* c, const double* x, double* y) {
+    if (!c || !x || !y) return HFEM_E_ARG;
+    if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before a matvec");
+    CK(cudaSetDevice(c->device));
+    int rc = matvec_warp(c, x, y, false, nullptr);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int hfem_set_step(hfem_ctx* c, const double* duh) {
+    if (!c || !duh) return HFEM_E_ARG;
+    if (!c->assembled) return fail(c, HFEM_E_STATE, "assemble before setting a step");
+    CK(cudaSetDevice(c->device));
+    int rc = ensure_krylov(c, 1);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->x, duh, sizeof(double) * nvec(c), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
 int hfem_get_ordering(hfem_ctx* c, int* ordered2unordered) {
     if (!c || !ordered2unordered) return HFEM_E_ARG;
     if (!c->have_order) return fail(c, HFEM_E_STATE, "no ordering yet (run hfem_gmres with precond 0)");

@@ -163,6 +163,16 @@ int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newto
  * iterations refine the solution to the FP64 residual tolerance. */
 int hfem_set_precision(hfem_ctx* ctx, int mode);
 
+/* y = Hg x with device pointers x, y (nf*bsz doubles each, on the context's
+ * device), after an assembly; the matvec of GMRES without a preconditioner.
+ * hfem_set_step makes duh (device, nf*bsz) the step that hfem_update applies,
+ * in place of the last GMRES solution.  For drivers that run their own Krylov
+ * method around the assembled system, e.g. the domain-decomposed GMRES of
+ * several GPUs (matvec of the local rows, then a sum over the part
+ * interfaces; solvers/pDLAK.cpp:322-357 in the reference's MPI path). */
+int hfem_matvec(hfem_ctx* ctx, const double* x, double* y);
+int hfem_set_step(hfem_ctx* ctx, const double* duh);
+
 /* The BILU0 ordering in use: ordered2unordered[i] = face pivoted at step i
  * (sys.ordered2unordered of the reference).  hfem_reset_ordering makes the
  * next BILU0 solve recompute it from the current system. */
