@@ -508,7 +508,7 @@ def run_serve_task(args):
         # warm the kernels, contexts and the device pool once with the same stream
         # (untimed), as the other tasks take warm-up steps
         serve([r for r in make_requests(6, 1e6, seed=999, max_el=512)], hbm_budget=None)
-        warm = make_requests(args.serve_requests, rate, seed=args.serve_seed)
+        warm = make_requests(args.serve_requests, rate, seed=args.serve_seed)[:args.serve_warm_requests]
         for a, b in zip(warm, reqs):
             a.prob = b.prob
         serve(warm, tol=1e-10, gmres_tol=args.serve_gmres_tol, repack_on_device=not args.serve_host_repack)
@@ -612,8 +612,10 @@ def main():
     ap.add_argument("--dirk-tol", type=float, default=1e-10)
     ap.add_argument("--dirk-precision", type=int, default=1, choices=[0, 1])
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[20.0, 50.0, 100.0])
-    ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--serve-seq-requests", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-seq-requests", type=int, default=2000)
+    ap.add_argument("--serve-warm-requests", type=int, default=300,
+                    help="requests of the same stream served once, untimed, before the timed pass")
     ap.add_argument("--serve-seed", type=int, default=0)
     ap.add_argument("--serve-gmres-tol", type=float, default=1e-10)
     ap.add_argument("--serve-host-repack", action="store_true",

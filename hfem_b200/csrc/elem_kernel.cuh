@@ -368,60 +368,97 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
         {
             const double* Phi = Bs;
             const double* Psi = Bs + G::LDBD * G::NKP;
+            // m-tiles in pairs: every B fragment read from shared memory feeds two
+            // DMMAs (shared-memory bandwidth is the busiest unit of this kernel)
             constexpr int MTD = (NPV * NCU * NCU + 7) / 8;
-            for (int mt = warp; mt < MTD; mt += NT / 32) {
-                const int r = 8 * mt + gr;
-                const bool rv = r < NPV * NCU * NCU;
-                const int i = r % NPV, j = (r / NPV) % NCU, k = r / (NPV * NCU);
-                const double* yrow = Ys + NGV * (k + NC * (i + NPV * j));
-                double acc[G::NTK][2];
+            // with NGV a multiple of 4 the F part's A values are the D part's
+            // shifted by NGV/4 k-steps (the q derivatives d' = d + 1)
+            constexpr bool SHIFT = NGV % 4 == 0 && G::KV3 == NGV * ND1;
+            for (int mp = warp; 2 * mp < MTD; mp += NT / 32) {
+                int rr[2];
+                bool rv[2];
+                const double* yrow[2];
 #pragma unroll
-                for (int b = 0; b < G::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
-                // the m-tile's A values for every k-step are loaded before the first
-                // DMMA, so their latencies overlap
-                double av[G::KV3 / 4];
-#pragma unroll
-                for (int ks = 0; ks < G::KV3 / 4; ks++) {
-                    const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
-                    av[ks] = (rv && kk < NGV * ND1) ? yrow[g + NGV * NCU * dp] : 0.0;
+                for (int u = 0; u < 2; u++) {
+                    rr[u] = 8 * (2 * mp + u) + gr;
+                    rv[u] = rr[u] < NPV * NCU * NCU;
+                    const int i = rr[u] % NPV, j = (rr[u] / NPV) % NCU, k = rr[u] / (NPV * NCU);
+                    yrow[u] = Ys + NGV * (k + NC * (i + NPV * j));
                 }
+                // the A values of both m-tiles for every k-step are loaded before the
+                // first DMMA, so their latencies overlap
+                double av[2][G::KV3 / 4];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int ks = 0; ks < G::KV3 / 4; ks++) {
+                        const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
+                        av[u][ks] = (rv[u] && kk < NGV * ND1) ? yrow[u][g + NGV * NCU * dp] : 0.0;
+                    }
+                double acc[2][G::NTK][2];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++) acc[u][b][0] = acc[u][b][1] = 0.0;
 #pragma unroll
                 for (int ks = 0; ks < G::KV3 / 4; ks++) {
                     const int kk = 4 * ks + gc;
 #pragma unroll
-                    for (int b = 0; b < G::NTK; b++)
-                        dmma8x8x4(acc[b][0], acc[b][1], av[ks], Phi[kk + G::LDBD * (8 * b + gr)]);
-                }
-                double accf[G::NTH][2];
-#pragma unroll
-                for (int b = 0; b < G::NTH; b++) accf[b][0] = accf[b][1] = 0.0;
-                double aq[G::KQ3 / 4];
-#pragma unroll
-                for (int ks = 0; ks < G::KQ3 / 4; ks++) {
-                    const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
-                    aq[ks] = (rv && kk < NGV * ND) ? yrow[g + NGV * NCU * (d + 1)] : 0.0;
+                    for (int b = 0; b < G::NTK; b++) {
+                        const double bv = Phi[kk + G::LDBD * (8 * b + gr)];
+                        dmma8x8x4(acc[0][b][0], acc[0][b][1], av[0][ks], bv);
+                        dmma8x8x4(acc[1][b][0], acc[1][b][1], av[1][ks], bv);
+                    }
                 }
 #pragma unroll
-                for (int ks = 0; ks < G::KQ3 / 4; ks++) {
-                    const int kk = 4 * ks + gc;
-#pragma unroll
-                    for (int b = 0; b < G::NTH; b++)
-                        dmma8x8x4(accf[b][0], accf[b][1], aq[ks], Psi[kk + G::LDBD * (8 * b + gr)]);
-                }
-                if (rv) {
+                for (int u = 0; u < 2; u++) {
+                    if (!rv[u]) continue;
+                    const int i = rr[u] % NPV, j = (rr[u] / NPV) % NCU, k = rr[u] / (NPV * NCU);
 #pragma unroll
                     for (int b = 0; b < G::NTK; b++)
 #pragma unroll
                         for (int h = 0; h < 2; h++) {
                             const int a = 8 * b + 2 * gc + h;
-                            if (a < NPV) De[i + NPV * (j + NCU * (a + NPV * k))] = acc[b][h];
+                            if (a < NPV) De[i + NPV * (j + NCU * (a + NPV * k))] = acc[u][b][h];
                         }
+                }
+                double aq[2][G::KQ3 / 4];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int ks = 0; ks < G::KQ3 / 4; ks++) {
+                        if constexpr (SHIFT) {
+                            aq[u][ks] = av[u][ks + NGV / 4];
+                        } else {
+                            const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
+                            aq[u][ks] = (rv[u] && kk < NGV * ND) ? yrow[u][g + NGV * NCU * (d + 1)] : 0.0;
+                        }
+                    }
+                double accf[2][G::NTH][2];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++) accf[u][b][0] = accf[u][b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < G::KQ3 / 4; ks++) {
+                    const int kk = 4 * ks + gc;
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++) {
+                        const double bv = Psi[kk + G::LDBD * (8 * b + gr)];
+                        dmma8x8x4(accf[0][b][0], accf[0][b][1], aq[0][ks], bv);
+                        dmma8x8x4(accf[1][b][0], accf[1][b][1], aq[1][ks], bv);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    if (!rv[u]) continue;
+                    const int i = rr[u] % NPV, j = (rr[u] / NPV) % NCU, k = rr[u] / (NPV * NCU);
 #pragma unroll
                     for (int b = 0; b < G::NTH; b++)
 #pragma unroll
                         for (int h = 0; h < 2; h++) {
                             const int f2 = 8 * b + 2 * gc + h;
-                            if (f2 < NDF) Fe[i + NPV * (j + NCU * (k + NCH * f2))] = accf[b][h];
+                            if (f2 < NDF) Fe[i + NPV * (j + NCU * (k + NCH * f2))] = accf[u][b][h];
                         }
                 }
             }
@@ -482,71 +519,93 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             cp_async_wait<0>();
             __syncthreads();
             constexpr int MTK = (NPF * NCH * NCU + 7) / 8;
-            for (int mt = warp; mt < MTK; mt += NT / 32) {
-                const int r = 8 * mt + gr;
-                const bool rv = r < NPF * NCH * NCU;
-                // j fastest: the 8 rows of a tile are 8 consecutive words of a K/H column
-                const int j = r % NCH, ip = (r / NCH) % NPF, m = r / (NPF * NCH);
-                const int inode = sm.perm[fc * NPF + ip];
-                double aK[G::KFD / 4], aH[G::KFD / 4];
+            constexpr int KH0 = (NGF + 3) / 4;            // k-steps holding d' = 0 rows
+            // the d' = 0 rows of BH are zero outside the face's own columns
+            // fc NPF .. fc NPF + NPF - 1: those n-tiles are skipped there
+            const int blo = (fc * NPF) / 8, bhi = (fc * NPF + NPF - 1) / 8;
+            // m-tiles in pairs, as in the volume GEMM: one B fragment, two DMMAs
+            for (int mp = warp; 2 * mp < MTK; mp += NT / 32) {
+                int jj[2], ipp[2], mm[2], inode[2];
+                bool rv[2];
+                double aK[2][G::KFD / 4], aH0[2][KH0];
 #pragma unroll
-                for (int ks = 0; ks < G::KFD / 4; ks++) {
-                    const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF;
-                    double vK = 0.0, vH = 0.0;
-                    if (rv && k < NGF * ND1) {
-                        const double sf = sm.Af[ip + G::LDAF * q];
-                        if (dp == 0) {
-                            vK = sf * sfu[q + NGF * (j + NCH * m)];
-                            vH = sf * sfuh[q + NGF * (j + NCH * m)];
-                        } else {
-                            vK = sf * sfu[q + NGF * (j + NCH * (NCU * dp + m))];
-                            vH = vK;
+                for (int u = 0; u < 2; u++) {
+                    const int r = 8 * (2 * mp + u) + gr;
+                    rv[u] = r < NPF * NCH * NCU;
+                    // j fastest: the 8 rows of a tile are 8 consecutive words of a K/H column
+                    jj[u] = r % NCH, ipp[u] = (r / NCH) % NPF, mm[u] = r / (NPF * NCH);
+                    inode[u] = sm.perm[fc * NPF + ipp[u]];
+#pragma unroll
+                    for (int ks = 0; ks < G::KFD / 4; ks++) {
+                        const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF;
+                        double vK = 0.0, vH = 0.0;
+                        if (rv[u] && k < NGF * ND1) {
+                            const double sf = sm.Af[ipp[u] + G::LDAF * q];
+                            if (dp == 0) {
+                                vK = sf * sfu[q + NGF * (jj[u] + NCH * mm[u])];
+                                vH = sf * sfuh[q + NGF * (jj[u] + NCH * mm[u])];
+                            } else {
+                                vK = sf * sfu[q + NGF * (jj[u] + NCH * (NCU * dp + mm[u]))];
+                                vH = vK;
+                            }
                         }
+                        aK[u][ks] = vK;
+                        if (ks < KH0) aH0[u][ks] = vH;
                     }
-                    aK[ks] = vK;
-                    aH[ks] = vH;
                 }
-                double acc[G::NTK][2];
+                double acc[2][G::NTK][2];
 #pragma unroll
-                for (int b = 0; b < G::NTK; b++) acc[b][0] = acc[b][1] = 0.0;
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++) acc[u][b][0] = acc[u][b][1] = 0.0;
 #pragma unroll
                 for (int ks = 0; ks < G::KFD / 4; ks++)
 #pragma unroll
-                    for (int b = 0; b < G::NTK; b++)
-                        dmma8x8x4(acc[b][0], acc[b][1], aK[ks], BK[(4 * ks + gc) + G::LDBK * (8 * b + gr)]);
-#pragma unroll
-                for (int b = 0; b < G::NTK; b++)
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int a = 8 * b + 2 * gc + h;
-                        if (rv && a < NPV) {
-                            if (store) Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = acc[b][h];
-                            if (liftD) atomicAdd(&De[inode + NPV * (j + NCU * (a + NPV * m))], acc[b][h]);
-                        }
+                    for (int b = 0; b < G::NTK; b++) {
+                        const double bv = BK[(4 * ks + gc) + G::LDBK * (8 * b + gr)];
+                        dmma8x8x4(acc[0][b][0], acc[0][b][1], aK[0][ks], bv);
+                        dmma8x8x4(acc[1][b][0], acc[1][b][1], aK[1][ks], bv);
                     }
-                double acch[G::NTH][2];
 #pragma unroll
-                for (int b = 0; b < G::NTH; b++) acch[b][0] = acch[b][1] = 0.0;
-                // the d' = 0 rows of BH are zero outside the face's own columns
-                // fc NPF .. fc NPF + NPF - 1: those n-tiles are skipped there
-                const int blo = (fc * NPF) / 8, bhi = (fc * NPF + NPF - 1) / 8;
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int a = 8 * b + 2 * gc + h;
+                            if (rv[u] && a < NPV) {
+                                const int j = jj[u], ip = ipp[u], m = mm[u];
+                                if (store) Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = acc[u][b][h];
+                                if (liftD) atomicAdd(&De[inode[u] + NPV * (j + NCU * (a + NPV * m))], acc[u][b][h]);
+                            }
+                        }
+                double acch[2][G::NTH][2];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++) acch[u][b][0] = acch[u][b][1] = 0.0;
 #pragma unroll
                 for (int ks = 0; ks < G::KFD / 4; ks++)
 #pragma unroll
                     for (int b = 0; b < G::NTH; b++) {
                         if (4 * ks + 3 < NGF && (b < blo || b > bhi)) continue;
-                        dmma8x8x4(acch[b][0], acch[b][1], aH[ks], BH[(4 * ks + gc) + G::LDBK * (8 * b + gr)]);
+                        const double bv = BH[(4 * ks + gc) + G::LDBK * (8 * b + gr)];
+                        dmma8x8x4(acch[0][b][0], acch[0][b][1], ks < KH0 ? aH0[0][ks < KH0 ? ks : 0] : aK[0][ks], bv);
+                        dmma8x8x4(acch[1][b][0], acch[1][b][1], ks < KH0 ? aH0[1][ks < KH0 ? ks : 0] : aK[1][ks], bv);
                     }
 #pragma unroll
-                for (int b = 0; b < G::NTH; b++)
+                for (int u = 0; u < 2; u++)
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int f2 = 8 * b + 2 * gc + h;
-                        if (rv && f2 < NDF) {
-                            if (store) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[b][h];
-                            if (liftF) atomicAdd(&Fe[inode + NPV * (j + NCU * (m + NCH * f2))], acch[b][h]);
+                    for (int b = 0; b < G::NTH; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int f2 = 8 * b + 2 * gc + h;
+                            if (rv[u] && f2 < NDF) {
+                                const int j = jj[u], ip = ipp[u], m = mm[u];
+                                if (store) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[u][b][h];
+                                if (liftF) atomicAdd(&Fe[inode[u] + NPV * (j + NCU * (m + NCH * f2))], acch[u][b][h]);
+                            }
                         }
-                    }
             }
         };
         for (int fc = 0; fc < NFE; fc++) {

@@ -624,8 +624,15 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
                 if ((rc = check_launch(c, "gemm_schur"))) return rc;
             }
         } else {
+            {
+                // F += P H by a coalesced pass over F (the tensor-core kernel stages
+                // F column by column, where the gather of H would not coalesce)
+                Timed t(c, "lift_F");
+                lift_inplace_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(ne, n, lift_args(c, c->H, nb), c->F);
+                if ((rc = check_launch(c, "lift_F"))) return rc;
+            }
             Timed t(c, "schur_tc");
-            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err, lift_args(c, c->H, nb)};
+            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err, LiftArgs{}};
             c->L->schur_tc(dim3(c->grid_tc), c->L->tc_smem, c->stream, ta);
             if ((rc = check_launch(c, "schur_tc"))) return rc;
         }

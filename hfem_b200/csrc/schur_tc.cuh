@@ -16,8 +16,8 @@
 //     update is applied to H in FP64.
 // Every mbarrier wait is bounded; on expiry the kernel records an error,
 // waits (bounded) for its MMAs, frees its tensor memory and returns.
-// F arrives as F_vol: the interior-face trace rows of H are added while it is
-// staged (lift.cuh).
+// When a lift is given, F arrives as F_vol and the interior-face trace rows of
+// H are added while it is staged (lift.cuh).
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
@@ -33,7 +33,7 @@ struct SchurTcArgs {
     double* H;            // ne x (nb x nb), H -= K D^-1 F in place
     double* DinvF;        // ne x (n x nb), written
     int* err;             // set to 1 when an MMA completion wait expires
-    LiftArgs lift;        // F += P H (interior faces) as F is staged
+    LiftArgs lift;        // F += P H (interior faces) as F is staged; src NULL: F is complete
 };
 
 template <int N, int NB>
