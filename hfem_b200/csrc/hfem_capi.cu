@@ -111,7 +111,7 @@ struct Launch {
     size_t ws;                  // workspace doubles per CTA slot (element_kernel)
     size_t q_smem;
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
-    void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*, const LiftArgs&);
+    void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
     void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
     size_t elem_smem;
     const void* elem_fn;
@@ -123,15 +123,14 @@ struct Launch {
     size_t tc_smem;
     const void* tc_fn;
     void (*scatter_h)(dim3, cudaStream_t, const ScatterArgs&);
-    void (*schur_fused)(cudaStream_t, int, const double*, const double*, const double*, double*, double*,
-                        const LiftArgs&);
+    void (*schur_fused)(cudaStream_t, int, const double*, const double*, const double*, double*, double*);
     size_t fused_smem;
     const void* fused_fn;
 };
 
 template <int N>
-void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info, const LiftArgs& L) {
-    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info, L);
+void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info) {
+    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info);
 }
 
 template <class S>
@@ -157,10 +156,11 @@ struct FusedPick {
 };
 template <class S>
 void launch_schur_fused(cudaStream_t st, int ne, const double* Dinv, const double* F, const double* K, double* H,
-                        double* DinvF, const LiftArgs& L) {
+                        double* DinvF) {
+    static_assert(S::NB <= LIFT_MAXNB, "the lift stages one column of H per warp");
     using P = FusedPick<S>;
     schur_fused_kernel<S::N, S::NB, P::BN, P::NW>
-        <<<(unsigned)(ne * P::Cfg::STRIPS), P::Cfg::THREADS, P::Cfg::SMEM, st>>>(ne, Dinv, F, K, H, DinvF, L);
+        <<<(unsigned)(ne * P::Cfg::STRIPS), P::Cfg::THREADS, P::Cfg::SMEM, st>>>(ne, Dinv, F, K, H, DinvF);
 }
 
 template <class S>
@@ -558,6 +558,15 @@ LiftArgs lift_args(hfem_ctx* c, const double* src, int cols) {
     return L;
 }
 
+// F += P H (interior faces) in place, ahead of the condensation kernels.
+int lift_F(hfem_ctx* c) {
+    Timed t(c, "lift_F");
+    const long long cols = (long long)c->dims.ne * c->nb;
+    const int grid = (int)std::max(1LL, std::min(cols / LIFT_WARPS, (long long)sms(c->device) * 8));
+    lift_inplace_kernel<<<grid, 32 * LIFT_WARPS, 0, c->stream>>>(c->dims.ne, c->n, lift_args(c, c->H, c->nb), c->F);
+    return check_launch(c, "lift_F");
+}
+
 int ready(hfem_ctx* c) {
     if (!c) return HFEM_E_ARG;
     if (!c->have_master || !c->have_mesh || !c->have_phys || !c->have_sol)
@@ -594,23 +603,20 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
         const int ne = c->dims.ne, n = c->n, nb = c->nb;
         {
             Timed t(c, "inverse");
-            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info, LiftArgs{});
+            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
         if (c->precision == 0 && c->g1_sel < 0 && c->g2_sel < 0) {
             // both products in one kernel (tilings chosen by hfem_set_gemm_tiles
             // or hfem_autotune run the two batched GEMMs instead)
+            if ((rc = lift_F(c))) return rc;
             Timed t(c, "schur_fused");
-            c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF, lift_args(c, c->H, nb));
+            c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
             if ((rc = check_launch(c, "schur_fused"))) return rc;
         } else if (c->precision == 0) {
             const GemmLaunch& g1 = c->g1_sel >= 0 ? gemm_candidates()[c->g1_sel] : c->L->g1;
             const GemmLaunch& g2 = c->g2_sel >= 0 ? gemm_candidates()[c->g2_sel] : c->L->g2;
-            {
-                Timed t(c, "lift_F");
-                lift_inplace_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(ne, n, lift_args(c, c->H, nb), c->F);
-                if ((rc = check_launch(c, "lift_F"))) return rc;
-            }
+            if ((rc = lift_F(c))) return rc;
             {
                 Timed t(c, "gemm_DinvF");
                 g1.run(c->stream, ne, n, nb, n, 1.0, c->D, n, (long long)n * n, c->F, n, (long long)n * nb, 0.0,
@@ -624,15 +630,9 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
                 if ((rc = check_launch(c, "gemm_schur"))) return rc;
             }
         } else {
-            {
-                // F += P H by a coalesced pass over F (the tensor-core kernel stages
-                // F column by column, where the gather of H would not coalesce)
-                Timed t(c, "lift_F");
-                lift_inplace_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(ne, n, lift_args(c, c->H, nb), c->F);
-                if ((rc = check_launch(c, "lift_F"))) return rc;
-            }
+            if ((rc = lift_F(c))) return rc;
             Timed t(c, "schur_tc");
-            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err, LiftArgs{}};
+            SchurTcArgs ta{ne, c->D, c->F, c->K, c->H, c->DinvF, c->tc_err};
             c->L->schur_tc(dim3(c->grid_tc), c->L->tc_smem, c->stream, ta);
             if ((rc = check_launch(c, "schur_tc"))) return rc;
         }
@@ -1038,8 +1038,7 @@ int bj_blocked(hfem_ctx* c) {
     const int grid = std::max(1, std::min(nf, sms(c->device) * std::max(occ, 1)));
     // the kernel also solves with a right-hand side: c->w is free here and its
     // result is ignored
-    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->binfo,
-                                                                                     LiftArgs{});
+    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->binfo);
     return check_launch(c, "bj_inverse");
 }
 
@@ -2156,11 +2155,10 @@ int hfem_autotune(hfem_ctx* c, int reps, int* best, double* ms) {
         }
     // the fused kernel does both products: kept when it beats the best pair
     {
-        const LiftArgs lf = lift_args(c, c->H, nb);
-        c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF, lf);   // warm-up
+        c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);   // warm-up
         if ((rc = check_launch(c, "autotune"))) return rc;
         CK(cudaEventRecord(e0, c->stream));
-        for (int r = 0; r < reps; r++) c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF, lf);
+        for (int r = 0; r < reps; r++) c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
         CK(cudaEventRecord(e1, c->stream));
         CK(cudaEventSynchronize(e1));
         float t = 0.f;
@@ -2540,7 +2538,7 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.inviscid = appname == 0;
     L->element(dim3(ge), L->elem_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
-    L->inverse(dim3(gi), st, d.ne, D, DinvRu, info, LiftArgs{});
+    L->inverse(dim3(gi), st, d.ne, D, DinvRu, info);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     LiftArgs lh;
     lh.src = H;
@@ -2551,7 +2549,10 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     lh.nfe = d.nfe;
     lh.nch = d.nd + 2;
     lh.cols = nb;
-    L->schur_fused(st, d.ne, D, DinvF, K, H, DinvF, lh);
+    // F (formed in the DinvF buffer) += P H, then the condensation in place
+    lift_inplace_kernel<<<sms(dev) * 8, 32 * LIFT_WARPS, 0, st>>>(d.ne, n, lh, DinvF);
+    if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
+    L->schur_fused(st, d.ne, D, DinvF, K, H, DinvF);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     batched_dgemv_kernel<<<sms(dev) * 8, 256, 0, st>>>(d.ne, nb, n, -1.0, K, (long long)nb * n, DinvRu, n, Rh, nb);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;

@@ -17,11 +17,8 @@
 // No rows are swapped.  After the last panel the in-place result X satisfies
 // D^-1(k, p_m) = X(p_k, m) and (D^-1 Ru)(k) = X(p_k, Ru column), p_k the row
 // pivoted at step k.  A zero pivot reports 1 + step in info[e].
-// When a lift is given (the element's D from the element kernel is D_vol), the
-// interior-face trace rows of K are added to D as it arrives (lift.cuh).
 #pragma once
 #include <cuda_runtime.h>
-#include "lift.cuh"
 #include "schur_kernels.cuh"
 
 namespace hfem {
@@ -147,8 +144,7 @@ __device__ __forceinline__ void inv_tile(double* __restrict__ A, const double* _
 
 template <int N>
 __global__ void __launch_bounds__(InvBlk<N>::THREADS, 2)
-    inverse_blocked_kernel(int ne, double* __restrict__ D, double* __restrict__ Ru, int* __restrict__ info,
-                           LiftArgs L) {
+    inverse_blocked_kernel(int ne, double* __restrict__ D, double* __restrict__ Ru, int* __restrict__ info) {
     using C = InvBlk<N>;
     constexpr int NP = C::NP, LDA = C::LDA, LDB = C::LDB, NW = C::THREADS / 32;
     extern __shared__ __align__(16) unsigned char inv_raw[];
@@ -156,10 +152,8 @@ __global__ void __launch_bounds__(InvBlk<N>::THREADS, 2)
     double* B = A + (size_t)LDA * C::NCP;             // LDB x NCP
     __shared__ int piv[NP];
     __shared__ int s_bad;
-    __shared__ LiftTable lift;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int gr = lane >> 2, gc = lane & 3;
-    lift_table(L, lift);
     for (int e = blockIdx.x; e < ne; e += gridDim.x) {
         double* De = D + (size_t)e * N * N;
         // D by 16-byte asynchronous copies, all in flight at once (N is even, so
@@ -178,13 +172,6 @@ __global__ void __launch_bounds__(InvBlk<N>::THREADS, 2)
         unsigned used = 0;   // warp 0: bit r set once row lane + 32 r has pivoted
         cp_async_wait<0>();
         __syncthreads();
-        if (L.src) {
-            for (int t = tid; t < N * N; t += C::THREADS) {
-                const int k = t % N, j = t / N;
-                A[k + LDA * j] = lift_add(L, lift, e, k, j, A[k + LDA * j]);
-            }
-            __syncthreads();
-        }
         if (warp == 0) {
             const int bad = inv_panel<N>(A, piv, 0, used, lane);
             if (lane == 0 && bad) s_bad = bad;

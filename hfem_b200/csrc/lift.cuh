@@ -5,11 +5,11 @@
 // to the element node that carries the face dof, so
 //   D = D_vol + P K,   F = F_vol + P H,
 // with P the node <- face-dof incidence given by perm.  The element kernel
-// writes D_vol, F_vol and the trace rows K, H; the condensation kernels, which
-// read K and H anyway, add P K and P H while they load D and F, so the element
-// kernel needs no read-modify-write of D and F.  Boundary faces are lifted by
-// the element kernel itself (their trace rows take the boundary flux while
-// their element rows keep fhat), so the lift here skips them.
+// writes D (lifted), F_vol and the trace rows K, H; lift_inplace_kernel adds
+// P H to F between the element kernel and the condensation, one coalesced pass
+// instead of reductions in L2 from the element kernel.  Boundary faces are
+// lifted by the element kernel itself (their trace rows take the boundary flux
+// while their element rows keep fhat), so the lift here skips them.
 //
 // Row r = i + npv j of D (or F) with column c receives, for every interior face
 // dof fdof of node i in increasing order (the order of the reference's face
@@ -45,8 +45,8 @@ __device__ __forceinline__ void lift_table(const LiftArgs& L, LiftTable& t) {
     }
 }
 
-// v plus the lifted trace entries of row `row`, column `col` of element e;
-// hs (optional) is column `col` of the element's src already in shared memory.
+// v plus the lifted trace entries of row `row` of element e, one column; hs is
+// that column of the element's src (K or H), already in shared memory.
 __device__ __forceinline__ double lift_add_col(const LiftArgs& L, const LiftTable& t, int e, int row,
                                               const double* hs, double v) {
     const int i = row % L.npv, j = row / L.npv;
@@ -59,33 +59,30 @@ __device__ __forceinline__ double lift_add_col(const LiftArgs& L, const LiftTabl
     return v;
 }
 
-// v plus the lifted trace entries of row `row`, column `col` of element e.
-__device__ __forceinline__ double lift_add(const LiftArgs& L, const LiftTable& t, int e, int row, int col, double v) {
-    const int i = row % L.npv, j = row / L.npv;
-    const int nb = L.nch * L.npf * L.nfe;
-    const double* s = L.src + (size_t)e * nb * L.cols + (size_t)nb * col + j;
-    const int cnt = t.n[i];
-    for (int q = 0; q < cnt; q++) {
-        const int fdof = t.f[i * LIFT_MAXINC + q];
-        if (L.bf && L.bf[(size_t)e * L.nfe + fdof / L.npf] < 0) continue;
-        v += s[L.nch * fdof];
-    }
-    return v;
-}
-
 // T += P src in place for every element (rows x cols per element, column-major):
-// the lift on its own, for the condensation paths that read F from global
-// memory with a library-style batched GEMM.
-__global__ void __launch_bounds__(256) lift_inplace_kernel(int ne, int rows, LiftArgs L, double* __restrict__ T) {
+// the lift on its own, ahead of a condensation kernel that reads T whole.  One
+// warp per column: the column of src (nb values) is read coalesced into shared
+// memory, then the warp's lanes update the column of T from it.
+constexpr int LIFT_WARPS = 8;
+constexpr int LIFT_MAXNB = 200;                  // trace dofs per element (tetrahedron p = 3)
+
+__global__ void __launch_bounds__(32 * LIFT_WARPS) lift_inplace_kernel(int ne, int rows, LiftArgs L,
+                                                                       double* __restrict__ T) {
     __shared__ LiftTable tab;
+    __shared__ double hs[LIFT_WARPS][LIFT_MAXNB];
     lift_table(L, tab);
     __syncthreads();
-    const long long per = (long long)rows * L.cols, tot = per * ne;
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < tot; x += (long long)gridDim.x * blockDim.x) {
-        const int e = (int)(x / per);
-        const long long r = x - (long long)e * per;
-        const int row = (int)(r % rows), col = (int)(r / rows);
-        T[x] = lift_add(L, tab, e, row, col, T[x]);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nb = L.nch * L.npf * L.nfe;
+    const long long ncol = (long long)ne * L.cols;
+    for (long long col = (long long)blockIdx.x * LIFT_WARPS + w; col < ncol; col += (long long)gridDim.x * LIFT_WARPS) {
+        const int e = (int)(col / L.cols), c = (int)(col - (long long)e * L.cols);
+        const double* src = L.src + (size_t)e * nb * L.cols + (size_t)nb * c;
+        for (int r = lane; r < nb; r += 32) hs[w][r] = src[r];
+        __syncwarp();
+        double* t = T + (size_t)e * rows * L.cols + (size_t)rows * c;
+        for (int r = lane; r < rows; r += 32) t[r] = lift_add_col(L, tab, e, r, hs[w], t[r]);
+        __syncwarp();
     }
 }
 

@@ -7,14 +7,9 @@
 // then the X strip) sits in shared memory whole.  Warp w owns m-tiles w, w+NW,
 // ... of every job and all BN/8 n-tiles.  H's accumulators start from H.
 // DinvF may be F itself: a CTA has its whole F strip in shared memory before it
-// writes the X strip over it, and strips are disjoint.  When a lift is given
-// (F from the element kernel is F_vol), the interior-face trace rows of H are
-// added to the F strip after it arrives (lift.cuh); they are the strip's own
-// columns of H, read before this CTA overwrites them.
+// writes the X strip over it, and strips are disjoint.
 #pragma once
 #include <cuda_runtime.h>
-#include "inverse_blocked.cuh"
-#include "lift.cuh"
 #include "schur_kernels.cuh"
 
 namespace hfem {
@@ -41,17 +36,15 @@ template <int N, int NB, int BN, int NW>
 __global__ void __launch_bounds__(32 * NW) schur_fused_kernel(int ne, const double* __restrict__ Dinv,
                                                               const double* F,
                                                               const double* __restrict__ K, double* __restrict__ H,
-                                                              double* DinvF, LiftArgs L) {
+                                                              double* DinvF) {
     using C = FusedCfg<N, NB, BN, NW>;
     extern __shared__ __align__(16) double fsm[];
     double* Bs = fsm;                                  // LDB x BN: the F strip, then the X strip
     double* As = fsm + (size_t)C::LDB * BN;            // 2 stages of LDA x BK
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int gr = lane >> 2, gc = lane & 3;
-    __shared__ LiftTable lift;
     const int e = blockIdx.x / C::STRIPS, c0 = (blockIdx.x % C::STRIPS) * BN;
     if (e >= ne) return;
-    lift_table(L, lift);
     const double* De = Dinv + (size_t)e * N * N;
     const double* Fe = F + (size_t)e * N * NB;
     const double* Ke = K + (size_t)e * NB * N;
@@ -65,28 +58,6 @@ __global__ void __launch_bounds__(32 * NW) schur_fused_kernel(int ne, const doub
         cp_async16z(&Bs[k + C::LDB * col], Fe + (ok ? k + (size_t)N * (c0 + col) : 0), ok);
     }
     cp_async_commit();
-    if (L.src) {
-        // the strip's columns of H (NB rows each) through the A ring's space,
-        // HC columns per round by 16-byte copies, then F strip += P H strip
-        constexpr int HC = (2 * C::LDA * C::BK) / NB < BN ? (2 * C::LDA * C::BK) / NB : BN;
-        static_assert(HC >= 1, "the A ring holds at least one column of H");
-        const double* He0 = H + (size_t)e * NB * NB;
-        for (int r0 = 0; r0 < BN && c0 + r0 < NB; r0 += HC) {
-            const int nc = min(HC, min(BN - r0, NB - c0 - r0));
-            for (int t = tid; t < (NB / 2) * nc; t += C::THREADS) {
-                const int k2 = t % (NB / 2), col = t / (NB / 2);
-                cp_async16(&As[2 * k2 + NB * col], He0 + 2 * k2 + (size_t)NB * (c0 + r0 + col));
-            }
-            cp_async_commit();
-            cp_async_wait<0>();
-            __syncthreads();
-            for (int t = tid; t < N * nc; t += C::THREADS) {
-                const int k = t % N, col = t / N;
-                Bs[k + C::LDB * (r0 + col)] = lift_add_col(L, lift, e, k, As + NB * col, Bs[k + C::LDB * (r0 + col)]);
-            }
-            __syncthreads();
-        }
-    }
 
     // A tile loader: rows [m0, m0 + BM) of A (lda rows, m_end valid), k columns [k0, k0 + BK)
     auto load_a = [&](int st, const double* A, int lda, int m0, int m_end, int k0) {

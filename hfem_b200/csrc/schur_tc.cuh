@@ -16,12 +16,9 @@
 //     update is applied to H in FP64.
 // Every mbarrier wait is bounded; on expiry the kernel records an error,
 // waits (bounded) for its MMAs, frees its tensor memory and returns.
-// When a lift is given, F arrives as F_vol and the interior-face trace rows of
-// H are added while it is staged (lift.cuh).
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
-#include "lift.cuh"
 
 namespace hfem {
 
@@ -33,7 +30,6 @@ struct SchurTcArgs {
     double* H;            // ne x (nb x nb), H -= K D^-1 F in place
     double* DinvF;        // ne x (n x nb), written
     int* err;             // set to 1 when an MMA completion wait expires
-    LiftArgs lift;        // F += P H (interior faces) as F is staged; src NULL: F is complete
 };
 
 template <int N, int NB>
@@ -150,8 +146,7 @@ __device__ __forceinline__ void stage_rows(float4* dst, const double* __restrict
 // B operand (NBP rows x KP) = transpose of a column-major FP64 KDIM x NCOL
 // matrix: tile row nn is column nn, read as 16-byte pairs along k.
 template <int KDIM, int NCOL, int NBP>
-__device__ __forceinline__ void stage_cols(float4* dst, const double* __restrict__ src, int tid, const LiftArgs& L,
-                                           const LiftTable& tab, int e) {
+__device__ __forceinline__ void stage_cols(float4* dst, const double* __restrict__ src, int tid) {
     constexpr int KC = (KDIM + 7) / 8 * 2;
     constexpr int TOT = KC * NBP;
     constexpr int U = 4;
@@ -165,12 +160,6 @@ __device__ __forceinline__ void stage_cols(float4* dst, const double* __restrict
             const double2* col = reinterpret_cast<const double2*>(src + (size_t)KDIM * nn + k0);
             v[u][0] = (ok && k0 < KDIM) ? col[0] : make_double2(0.0, 0.0);
             v[u][1] = (ok && k0 + 2 < KDIM) ? col[1] : make_double2(0.0, 0.0);
-            if (L.src && ok) {
-                if (k0 < KDIM) v[u][0].x = lift_add(L, tab, e, k0, nn, v[u][0].x);
-                if (k0 + 1 < KDIM) v[u][0].y = lift_add(L, tab, e, k0 + 1, nn, v[u][0].y);
-                if (k0 + 2 < KDIM) v[u][1].x = lift_add(L, tab, e, k0 + 2, nn, v[u][1].x);
-                if (k0 + 3 < KDIM) v[u][1].y = lift_add(L, tab, e, k0 + 3, nn, v[u][1].y);
-            }
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -192,9 +181,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tslot;
     __shared__ int s_bad;
-    __shared__ LiftTable lift;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    lift_table(A.lift, lift);
     const int wq = warp & 3, grp = warp >> 2;
     const int row = 32 * wq + lane;                               // accumulator row = TMEM lane
     if (warp == 0) {
@@ -226,7 +213,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
         double* DFe = A.DinvF + (size_t)e * N * NB;
         // ---- stage A = D^-1 (row m, k) and B = F^T (row nn, k) as FP32
         stage_rows<N, 128>(sA, Di, N, 0, N, tid);
-        stage_cols<N, NB, C::NBP>(sB, Fe, tid, A.lift, lift, e);
+        stage_cols<N, NB, C::NBP>(sB, Fe, tid);
         proxy_fence();
         __syncthreads();
         // ---- GEMM 1: TMEM[:, 0:NBP) = D^-1 F
