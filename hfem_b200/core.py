@@ -274,7 +274,8 @@ class HDGSolver:
         return o2u
 
     def set_precision(self, mode):
-        """0: FP64 throughout; 1: TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)."""
+        """0: FP64 throughout; 1: TF32 tensor-core Schur GEMMs and FP32 preconditioner (FP64 LU,
+        residuals, Arnoldi); 2: FP32 preconditioner only."""
         self._chk(self.lib.hfem_set_precision(self.h, int(mode)), "set_precision")
 
     def set_timing(self, on=True):

@@ -219,7 +219,7 @@ struct hfem_ctx {
     double* seg_partk = nullptr;            // CGS2 partial dots, npieces x (restart + 1)
     size_t seg_partk_n = 0;
     int seg_hP = 0;
-    int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs (FP64 LU, residuals, Arnoldi)
+    int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs + FP32 preconditioner; 2 FP32 preconditioner only
     int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
     // boundary faces (mesh.bf, app.bcm, app.bcs); bf == NULL: no boundary faces
     int *bf = nullptr, *bcm = nullptr;
@@ -606,14 +606,14 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
             c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
-        if (c->precision == 0 && c->g1_sel < 0 && c->g2_sel < 0) {
+        if (c->precision != 1 && c->g1_sel < 0 && c->g2_sel < 0) {
             // both products in one kernel (tilings chosen by hfem_set_gemm_tiles
             // or hfem_autotune run the two batched GEMMs instead)
             if ((rc = lift_F(c))) return rc;
             Timed t(c, "schur_fused");
             c->L->schur_fused(c->stream, ne, c->D, c->F, c->K, c->H, c->DinvF);
             if ((rc = check_launch(c, "schur_fused"))) return rc;
-        } else if (c->precision == 0) {
+        } else if (c->precision != 1) {
             const GemmLaunch& g1 = c->g1_sel >= 0 ? gemm_candidates()[c->g1_sel] : c->L->g1;
             const GemmLaunch& g2 = c->g2_sel >= 0 ? gemm_candidates()[c->g2_sel] : c->L->g2;
             if ((rc = lift_F(c))) return rc;
@@ -670,7 +670,7 @@ int finish_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
         CK(cudaStreamSynchronize(c->stream));
         for (int e = 0; e < c->dims.ne; e++)
             if (info[e]) return fail(c, HFEM_E_SINGULAR, "element %d: singular local matrix (pivot %d)", e, info[e]);
-        if (c->precision) {
+        if (c->precision == 1) {
             int terr = 0;
             CK(cudaMemcpyAsync(&terr, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
             CK(cudaStreamSynchronize(c->stream));
@@ -941,7 +941,7 @@ int bilu0_factor(hfem_ctx* c) {
     CK(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < nf; i++)
         if (bi[i]) return fail(c, HFEM_E_SINGULAR, "BILU0: singular pivot block at face %d", i);
-    if (c->precision == 1) {
+    if (c->precision >= 1) {
         // mixed precision: the triangular solves read FP32 factors (FP64 vectors and sums)
         const long long nm = (long long)b2 * c->dims.nblocks;
         if (!c->Mg32 && (rc = dalloc(c, &c->Mg32, (size_t)nm))) return rc;
@@ -954,7 +954,7 @@ int bilu0_factor(hfem_ctx* c) {
 // v = (L U)^-1 x (applyBILU0.m); v may not alias x.
 int bilu0_apply(hfem_ctx* c, const double* x, double* v) {
     Timed t(c, "bilu0_apply");
-    const bool f32 = c->precision == 1 && c->Mg32;
+    const bool f32 = c->precision >= 1 && c->Mg32;
     BiluSolveArgs a{c->bsz, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, f32 ? (const void*)c->Mg32 : c->Mg, x,
                     c->bl_y, v};
     const int nlo = (int)c->lvl_lo.size() - 1, nup = (int)c->lvl_up.size() - 1;
@@ -992,7 +992,7 @@ int matvec_prec(hfem_ctx* c, const double* x, double* z, bool prec) {
         if (rc) return rc;
         return bilu0_apply(c, c->bl_t, z);
     }
-    if (prec && c->precision == 1)
+    if (prec && c->precision >= 1)
         bsr_matvec_bj_kernel<float><<<std::min(c->dims.nf, sms(c->device) * 16), 64, sizeof(double) * 64, c->stream>>>(
             c->dims.nf, c->bsz, c->rowstart, c->colidx, c->Hg, c->Minv32, x, z);
     else
@@ -1091,7 +1091,7 @@ int gmres_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit, int
         CK(cudaStreamSynchronize(c->stream));
         for (int i = 0; i < c->dims.nf; i++)
             if (bi[i]) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d is singular", i);
-        if (c->precision == 1) {
+        if (c->precision >= 1) {
             const long long nm = (long long)c->dims.nf * c->bsz * c->bsz;
             if (!c->Minv32 && (rc = dalloc(c, &c->Minv32, (size_t)nm))) return rc;
             to_float_kernel<<<g, 256, 0, c->stream>>>(nm, c->Minv, c->Minv32);
@@ -1192,7 +1192,7 @@ int matvec_warp(hfem_ctx* c, const double* x, double* z, bool prec, const unsign
     switch (c->bsz) {
 #define HFEM_MV(B)                                                                                                \
     case B:                                                                                                       \
-        if (prec && c->precision == 1)                                                                            \
+        if (prec && c->precision >= 1)                                                                            \
             bsr_matvec_warp_kernel<B, float><<<grid, 256, 0, c->stream>>>(c->dims.nf, c->rowstart, c->colidx,      \
                                                                             c->Hg, c->Minv32, x, z, rseg, act);   \
         else                                                                                                      \
@@ -1283,7 +1283,7 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
         CK(cudaStreamSynchronize(c->stream));
         for (int i = 0; i < c->dims.nf; i++)
             if (bi[i]) return fail(c, HFEM_E_SINGULAR, "diagonal block of face %d is singular", i);
-        if (c->precision == 1) {
+        if (c->precision >= 1) {
             const long long nm = (long long)c->dims.nf * c->bsz * c->bsz;
             if (!c->Minv32 && (rc = dalloc(c, &c->Minv32, (size_t)nm))) return rc;
             to_float_kernel<<<g, 256, 0, c->stream>>>(nm, c->Minv, c->Minv32);
@@ -2296,7 +2296,9 @@ long long hfem_pool_cached_bytes(void) {
 
 int hfem_set_precision(hfem_ctx* c, int mode) {
     if (!c) return HFEM_E_ARG;
-    if (mode != 0 && mode != 1) return fail(c, HFEM_E_ARG, "precision mode must be 0 (FP64) or 1 (TF32 Schur)");
+    if (mode < 0 || mode > 2)
+        return fail(c, HFEM_E_ARG, "precision mode must be 0 (FP64), 1 (TF32 Schur, FP32 preconditioner) or 2 "
+                                   "(FP32 preconditioner)");
     c->precision = mode;
     c->assembled = false;
     return 0;

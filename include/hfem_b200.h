@@ -160,7 +160,9 @@ int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newto
  * with FP32 accumulation, and the preconditioner applied with FP32 factors
  * (block-Jacobi inverses, BILU0 factors); the element LU, the residuals
  * (rnorm), the Arnoldi process and the Newton update stay FP64, so Newton
- * iterations refine the solution to the FP64 residual tolerance. */
+ * iterations refine the solution to the FP64 residual tolerance.  mode 2: only
+ * the preconditioner in FP32 (the Jacobian FP64, so Newton converges as in
+ * mode 0 while GMRES applies FP32 factors). */
 int hfem_set_precision(hfem_ctx* ctx, int mode);
 
 /* y = Hg x with device pointers x, y (nf*bsz doubles each, on the context's
