@@ -141,13 +141,19 @@ def _run_ref_timing(prefix, nelem, reps):
     return json.loads(out.strip().splitlines()[-1])
 
 
+# Reference runs time a 4^3 x 6 = 384-element mesh of the workload's element
+# type per process: large enough that its assembled system (107 MB for p = 3)
+# and element arrays leave the host caches, as the full workload's would.
+REF_SAMPLE_N = 4
+
+
 def reference_cpu(workload, seconds_per_proc=10.0, procs=None, reps=None):
     """Reference C++ assembleLinearSystem on the host cores: P independent processes
     (the reference's MPI driver cannot be built here; its OpenMP is disabled)."""
     if not os.path.exists(REF_BIN):
         return None
     w = WORKLOADS[workload]
-    sample_n = 3
+    sample_n = REF_SAMPLE_N
     procs = procs or max(1, os.cpu_count() or 1)
     with tempfile.TemporaryDirectory() as tmp:
         prefix, ne = _write_ref_inputs(tmp, w["kind"], w["porder"], sample_n)
@@ -352,7 +358,7 @@ def run_reference(args, rank):
     w = WORKLOADS[args.workload]
     procs = max(1, os.cpu_count() or 1)
     with tempfile.TemporaryDirectory() as tmp:
-        prefix, ne = _write_ref_inputs(tmp, w["kind"], w["porder"], 3)
+        prefix, ne = _write_ref_inputs(tmp, w["kind"], w["porder"], REF_SAMPLE_N)
         for _ in range(args.warmup):
             _run_ref_timing(prefix, ne, 1)
         results = [None] * procs
@@ -368,7 +374,7 @@ def run_reference(args, rank):
             t.join()
         wall = time.time() - t0
     value = sum(r["elems_per_s"] for r in results)
-    sample = (f"{w['kind']} p={w['porder']} on a 3^3x6={ne}-element periodic mesh, {args.steps} "
+    sample = (f"{w['kind']} p={w['porder']} on a {REF_SAMPLE_N}^3x6={ne}-element periodic mesh, {args.steps} "
               f"assembleLinearSystem passes per process, {procs} processes")
     return {"metric": "assembly+Schur elements/s (FP64)", "value": value, "unit": "elements/s", "impl": "reference",
             "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps,
