@@ -13,7 +13,9 @@
 //   D_vol[(i,j,k), a]  = sum_{g,d'} Y(i,g,j,(d',k)) Phi[(g,d'), a],  Phi = [phi_a(g); (phi M^-1 C_d)(g;a)]
 //   F_vol[(i,j,k), f2] = sum_{g,d} Y(i,g,j,(d+1,k)) (-phi M^-1 E_d)(g; f2)
 // The B operands are formed in shared memory from M^-1 C and M^-1 E, which
-// stay in shared memory after the local Cholesky solves.  Of the lifted trace
+// stay in shared memory after the local Cholesky solves: their rows d' > 0 are
+// the products shapvt (M^-1 C | M^-1 E) and, per face, shapfc (M^-1 C | M^-1 E)
+// at the face's nodes, small GEMMs on the same FP64 tensor cores.  Of the lifted trace
 // terms, D += P K is added here by reductions in L2 (face after face, so each
 // sum has a fixed order), and F += P H of interior faces by the condensation
 // kernels when they load F (lift.cuh), where H is read anyway; boundary faces,
@@ -69,6 +71,74 @@ struct EK {
                   "16-byte alignment of the staged face slices");
 };
 
+// Cholesky solves L L' x = b for one column held in registers, in the axpy
+// (column) form: after x_j is final every later entry takes its update, so each
+// step has up to npv - 1 independent FMAs; rdg holds 1 / L(j, j).
+template <int NPV>
+__device__ __forceinline__ void chol_solve_col_axpy(const double* lm, const double* rdg, double* col) {
+    const volatile double* l = lm;
+    double x[NPV];
+#pragma unroll
+    for (int i = 0; i < NPV; i++) x[i] = col[i];
+#pragma unroll
+    for (int j = 0; j < NPV; j++) {
+        x[j] *= rdg[j];
+#pragma unroll
+        for (int i = j + 1; i < NPV; i++) x[i] = fma(-l[i + NPV * j], x[j], x[i]);
+    }
+#pragma unroll
+    for (int j = NPV - 1; j >= 0; j--) {
+        x[j] *= rdg[j];
+#pragma unroll
+        for (int i = 0; i < j; i++) x[i] = fma(-l[j + NPV * i], x[j], x[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NPV; i++) col[i] = x[i];
+}
+
+// Basis-by-(M^-1 C | M^-1 E) products on the FP64 tensor cores, one n-tile per
+// warp at a time:
+//   OUT(r, n) = sum_kk A(r, kk) CE(row(kk), n),  r < MR, kk < KD, n < NPV ND + NDF ND
+// with A(r, kk) = a[r + lda kk], CE the column-major npv x (npv nd + ndf nd)
+// block [M^-1 C | M^-1 E] and row(kk) = rmap[kk] (a face's nodes) or kk.
+// st(r, n, v) receives every valid entry.
+template <int MR, int KD, int NPV, int NCOL, int NW, class Store>
+__device__ __forceinline__ void basis_ce_gemm(const double* a, int lda, const int* rmap, const double* CE, Store st) {
+    constexpr int MT = (MR + 7) / 8, KS = (KD + 3) / 4, NNT = (NCOL + 7) / 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gr = lane >> 2, gc = lane & 3;
+    double af[MT][KS];
+    int brow[KS];
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++) {
+        const int kk = 4 * ks + gc;
+        brow[ks] = kk < KD ? (rmap ? rmap[kk] : kk) : -1;
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) {
+            const int r = 8 * mt + gr;
+            af[mt][ks] = (r < MR && kk < KD) ? a[r + lda * kk] : 0.0;
+        }
+    }
+    for (int nt = warp; nt < NNT; nt += NW) {
+        const int n = 8 * nt + gr;
+        double acc[MT][2];
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++) acc[mt][0] = acc[mt][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ks++) {
+            const double bv = (brow[ks] >= 0 && n < NCOL) ? CE[brow[ks] + NPV * n] : 0.0;
+#pragma unroll
+            for (int mt = 0; mt < MT; mt++) dmma8x8x4(acc[mt][0], acc[mt][1], af[mt][ks], bv);
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int r = 8 * mt + gr, nn = 8 * nt + 2 * gc + h;
+                if (r < MR && nn < NCOL) st(r, nn, acc[mt][h]);
+            }
+    }
+}
+
 template <class S>
 struct ElemSmem {
     double x[S::NPV * S::ND];
@@ -81,6 +151,7 @@ struct ElemSmem {
     double Af[EK<S>::LDAF * EK<S>::KF];    // shapfg, zero padded: Af[ip + LDAF*q]
     double sfc[S::NGF * S::NPF];           // face basis values shapfc(kk, q) = shapft[q + NGF*kk]
     double red[NT / 32];
+    double rdg[S::NPV];                    // 1 / L(j, j) of the Cholesky factor of M
     alignas(16) double un[EK<S>::UN];
     int perm[S::NDF];
     int inc_n[S::NPV];
@@ -168,7 +239,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
         // warp 0 factors M while the other warps evaluate the states at the points
         // and the pointwise fluxes, which do not depend on M
         if (warp == 0) {
-            cholesky_warp<NPV>(M);
+            cholesky_warp<NPV>(M, sm.rdg);
         } else {
             constexpr int NT1 = NT - 32;
             const int tid1 = tid - 32;
@@ -299,10 +370,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
         }
         __syncthreads();
         // M^-1 C and M^-1 E in place, one column per thread
-        for (int t = tid; t < NPV * ND + NDF * ND; t += NT) {
-            double* col = (t < NPV * ND) ? &Cm[NPV * t] : &Em[NPV * (t - NPV * ND)];
-            chol_solve_col_reg<NPV>(M, col);
-        }
+        for (int t = tid; t < NPV * ND + NDF * ND; t += NT) chol_solve_col_axpy<NPV>(M, sm.rdg, &Cm[NPV * t]);
         __syncthreads();
 
         double* Ke = A.K + (size_t)e * NB * N;
@@ -322,46 +390,57 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
         // Y, point index fastest: Ys[g + NGV (c + NC (i + NPV j))], c = NCU d' + k.
         // One thread per (g, j, c) with g fastest: its wrl words are read once and
         // the stores of a warp are runs of consecutive words.
-        for (int t = tid; t < NGV * NCU * NC; t += NT) {
-            const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
-            double w[ND1];
+        // The next item's wrl words are requested before this item's products, so
+        // their latency overlaps them.
+        {
+            constexpr int NY = NGV * NCU * NC;
+            auto wload = [&](int t, double* w) {
+                const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
 #pragma unroll
-            for (int r = 0; r < ND1; r++) w[r] = wrl[g + NGV * (r + ND1 * (j + NCU * c))];
+                for (int r = 0; r < ND1; r++) w[r] = t < NY ? wrl[g + NGV * (r + ND1 * (j + NCU * c))] : 0.0;
+            };
+            double w[ND1], wn[ND1];
+            wload(tid, w);
+            for (int t = tid; t < NY; t += NT) {
+                wload(t + NT, wn);
+                const int g = t % NGV, j = (t / NGV) % NCU, c = t / (NGV * NCU);
 #pragma unroll 4
-            for (int i = 0; i < NPV; i++) {
-                double y = 0.0;
+                for (int i = 0; i < NPV; i++) {
+                    double y = 0.0;
 #pragma unroll
-                for (int r = 0; r < ND1; r++) y += sm.Av[i + G::LDAV * (g + NGV * r)] * w[r];
-                Ys[g + NGV * (c + NC * (i + NPV * j))] = y;
+                    for (int r = 0; r < ND1; r++) y += sm.Av[i + G::LDAV * (g + NGV * r)] * w[r];
+                    Ys[g + NGV * (c + NC * (i + NPV * j))] = y;
+                }
+#pragma unroll
+                for (int r = 0; r < ND1; r++) w[r] = wn[r];
             }
         }
-        // volume B operands from M^-1 C and M^-1 E: Phi (KV3 x NKP) and Psi (KQ3 x NHP), ld LDBD
+        // volume B operands: Phi (KV3 x NKP) and Psi (KQ3 x NHP), ld LDBD.  The
+        // rows d' > 0 are shapvt (M^-1 C | M^-1 E) on the tensor cores; the d' = 0
+        // rows of Phi (the basis values) and the zero padding are written directly.
         {
             double* Phi = Bs;
             double* Psi = Bs + G::LDBD * G::NKP;
             for (int t = tid; t < G::KV3 * G::NKP; t += NT) {
-                const int k = t % G::KV3, a = t / G::KV3, g = k % NGV, dp = k / NGV;
-                double x = 0.0;
-                if (a < NPV && k < NGV * ND1) {
-                    if (dp == 0) {
-                        x = T.shapvt[g + NGV * a];
-                    } else {
-                        const double* cm = Cm + NPV * (a + NPV * (dp - 1));
-                        for (int b = 0; b < NPV; b++) x += T.shapvt[g + NGV * b] * cm[b];
-                    }
-                }
-                Phi[k + G::LDBD * a] = x;
+                const int k = t % G::KV3, a = t / G::KV3;
+                if (a < NPV && k >= NGV && k < NGV * ND1) continue;
+                Phi[k + G::LDBD * a] = (a < NPV && k < NGV) ? T.shapvt[k + NGV * a] : 0.0;
             }
             for (int t = tid; t < G::KV3 * G::NHP; t += NT) {
-                const int k = t % G::KV3, f2 = t / G::KV3, g = k % NGV, d = k / NGV;
-                double x = 0.0;
-                if (f2 < NDF && k < NGV * ND) {
-                    const double* em = Em + NPV * (f2 + NDF * d);
-                    for (int b = 0; b < NPV; b++) x += T.shapvt[g + NGV * b] * em[b];
-                    x = -x;
-                }
-                Psi[k + G::LDBD * f2] = x;
+                const int k = t % G::KV3, f2 = t / G::KV3;
+                if (f2 < NDF && k < NGV * ND) continue;
+                Psi[k + G::LDBD * f2] = 0.0;
             }
+            basis_ce_gemm<NGV, NPV, NPV, NPV * ND + NDF * ND, NT / 32>(
+                T.shapvt, NGV, nullptr, Cm, [&](int g, int n, double v) {
+                    if (n < NPV * ND) {
+                        const int a = n % NPV, d = n / NPV;
+                        Phi[(g + NGV * (d + 1)) + G::LDBD * a] = v;
+                    } else {
+                        const int f2 = (n - NPV * ND) % NDF, d = (n - NPV * ND) / NDF;
+                        Psi[(g + NGV * d) + G::LDBD * f2] = -v;
+                    }
+                });
         }
         __syncthreads();
         // ---- D_vol = Y' Phi and F_vol = Y'_q Psi (right after Y is written, while it is in L2)
@@ -489,33 +568,36 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             // the slices arrive by 16-byte asynchronous copies while B is built
             for (int t = tid; t < G::FSLP / 2; t += NT) cp_async16z(sfu + 2 * t, slices + 2 * t, true);
             cp_async_commit();
+            // d' = 0 rows (the face basis at the face's nodes) and zero padding
+            // directly; rows d' > 0 = shapfc (M^-1 C | M^-1 E)(face nodes) on the
+            // tensor cores
             for (int t = tid; t < G::KFD * G::NKP; t += NT) {
-                const int k = t % G::KFD, a = t / G::KFD, q = k % NGF, dp = k / NGF;
+                const int k = t % G::KFD, a = t / G::KFD, q = k % NGF;
+                if (a < NPV && k >= NGF && k < NGF * ND1) continue;
                 double x = 0.0;
-                if (a < NPV && k < NGF * ND1) {
-                    if (dp == 0) {
-                        const int p = sm.pos[fc * NPV + a];
-                        x = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
-                    } else {
-                        const double* cm = Cm + NPV * (a + NPV * (dp - 1));
-                        for (int m = 0; m < NPF; m++) x += sm.sfc[q + NGF * m] * cm[sm.perm[fc * NPF + m]];
-                    }
+                if (a < NPV && k < NGF) {
+                    const int p = sm.pos[fc * NPV + a];
+                    x = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
                 }
                 BK[k + G::LDBK * a] = x;
             }
             for (int t = tid; t < G::KFD * G::NHP; t += NT) {
-                const int k = t % G::KFD, f2 = t / G::KFD, q = k % NGF, dp = k / NGF;
+                const int k = t % G::KFD, f2 = t / G::KFD, q = k % NGF;
+                if (f2 < NDF && k >= NGF && k < NGF * ND1) continue;
                 double x = 0.0;
-                if (f2 < NDF && k < NGF * ND1) {
-                    if (dp == 0) {
-                        x = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
-                    } else {
-                        const double* em = Em + NPV * (f2 + NDF * (dp - 1));
-                        for (int m = 0; m < NPF; m++) x -= sm.sfc[q + NGF * m] * em[sm.perm[fc * NPF + m]];
-                    }
-                }
+                if (f2 < NDF && k < NGF) x = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
                 BH[k + G::LDBK * f2] = x;
             }
+            basis_ce_gemm<NGF, NPF, NPV, NPV * ND + NDF * ND, NT / 32>(
+                sm.sfc, NGF, sm.perm + fc * NPF, Cm, [&](int q, int n, double v) {
+                    if (n < NPV * ND) {
+                        const int a = n % NPV, d = n / NPV;
+                        BK[(q + NGF * (d + 1)) + G::LDBK * a] = v;
+                    } else {
+                        const int f2 = (n - NPV * ND) % NDF, d = (n - NPV * ND) / NDF;
+                        BH[(q + NGF * (d + 1)) + G::LDBK * f2] = -v;
+                    }
+                });
             cp_async_wait<0>();
             __syncthreads();
             constexpr int MTK = (NPF * NCH * NCU + 7) / 8;

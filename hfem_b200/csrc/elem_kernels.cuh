@@ -181,9 +181,10 @@ __device__ void qmatrices(const Tables& T, double fc_q, const double* jac, const
     }
 }
 
-// Lower Cholesky of M (npv x npv) in place, one warp.
+// Lower Cholesky of M (npv x npv) in place, one warp; rdg (if given) receives
+// the reciprocals of the diagonal.
 template <int NPV>
-__device__ void cholesky_warp(double* a) {
+__device__ void cholesky_warp(double* a, double* rdg = nullptr) {
     if (threadIdx.x >= 32) return;
     const int lane = threadIdx.x;
     for (int j = 0; j < NPV; j++) {
@@ -191,6 +192,7 @@ __device__ void cholesky_warp(double* a) {
             double s = a[j + NPV * j];
             for (int k = 0; k < j; k++) s -= a[j + NPV * k] * a[j + NPV * k];
             a[j + NPV * j] = sqrt(s);
+            if (rdg) rdg[j] = 1.0 / a[j + NPV * j];
         }
         __syncwarp();
         const double djj = a[j + NPV * j];
@@ -215,36 +217,6 @@ __device__ __forceinline__ void chol_solve_col(const double* l, double* x) {
         for (int k = i + 1; k < NPV; k++) t -= l[k + NPV * i] * x[k];
         x[i] = t / l[i + NPV * i];
     }
-}
-
-// The same two triangular solves with the column held in registers: the
-// column's shared-memory words are read once and written once (threads own
-// columns NPV doubles apart, so every shared access of a column is bank
-// conflicted), and the dependent chains run on registers.
-template <int NPV>
-__device__ __forceinline__ void chol_solve_col_reg(const double* lm, double* col) {
-    // factor entries are read where they are used (not hoisted), which keeps
-    // the register footprint to the column itself
-    const volatile double* l = lm;
-    double x[NPV];
-#pragma unroll
-    for (int i = 0; i < NPV; i++) x[i] = col[i];
-#pragma unroll
-    for (int i = 0; i < NPV; i++) {
-        double t = x[i];
-#pragma unroll
-        for (int k = 0; k < i; k++) t -= l[i + NPV * k] * x[k];
-        x[i] = t / l[i + NPV * i];
-    }
-#pragma unroll
-    for (int i = NPV - 1; i >= 0; i--) {
-        double t = x[i];
-#pragma unroll
-        for (int k = i + 1; k < NPV; k++) t -= l[k + NPV * i] * x[k];
-        x[i] = t / l[i + NPV * i];
-    }
-#pragma unroll
-    for (int i = 0; i < NPV; i++) col[i] = x[i];
 }
 
 // --------------------------------------------------------------- scatter
