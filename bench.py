@@ -249,14 +249,15 @@ def run_gpu(args, rank, world, local_rank):
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
-    # mixed precision leg: the same step with the Schur GEMMs on the tcgen05 tensor cores (TF32)
-    mixed_ms, mixed_k, mixed_err = 0.0, {}, {}
-    if not args.no_mixed:
+    # mixed precision legs: the same step in precision mode 1 (3xTF32 element
+    # contractions, TF32 tcgen05 Schur GEMMs) and mode 3 (3xTF32 element
+    # contractions, FP64 Schur); errors against this run's FP64 blocks
+    def mixed_leg(mode):
+        solver.set_precision(0)
         solver.set_solution(udg_q, uh0, prob.sh)
-        solver.assembleLinearSystem()
-        ref = {k: solver.device_tensor(k).clone() for k in ("Hg", "DinvF")}
         r64 = solver.assembleLinearSystem()
-        solver.set_precision(1)
+        ref = {k: solver.device_tensor(k).clone() for k in ("K", "Hg", "DinvF")}
+        solver.set_precision(mode)
         for _ in range(max(3, args.warmup)):
             solver.assembleLinearSystem()
         solver.set_timing(True)
@@ -269,20 +270,28 @@ def run_gpu(args, rank, world, local_rank):
         m1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        mixed_ms = m0.elapsed_time(m1)
-        mixed_k = solver.kernel_times()
+        leg_ms = m0.elapsed_time(m1)
+        leg_k = solver.kernel_times()
         solver.set_timing(False)
+        err = {}
         for k, v in ref.items():
             cur = solver.device_tensor(k)
-            mixed_err[k] = float((cur - v).abs().max() / v.abs().max())
-        mixed_err["rnorm"] = abs(r32 - r64) / r64
+            err[k] = float((cur - v).abs().max() / v.abs().max())
+        err["rnorm"] = abs(r32 - r64) / r64
         del ref
         solver.set_precision(0)
+        return leg_ms, leg_k, err
+
+    mixed_ms, mixed_k, mixed_err = 0.0, {}, {}
+    split_ms, split_k, split_err = 0.0, {}, {}
+    if not args.no_mixed:
+        mixed_ms, mixed_k, mixed_err = mixed_leg(1)
+        split_ms, split_k, split_err = mixed_leg(3)
 
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms, mixed_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        t = torch.tensor([ms, e2e_ms, mixed_ms, split_ms], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms, mixed_ms = float(t[0]), float(t[1]), float(t[2])
+        ms, e2e_ms, mixed_ms, split_ms = float(t[0]), float(t[1]), float(t[2]), float(t[3])
     solver.close()
     if rank != 0:
         return None
@@ -338,13 +347,21 @@ def run_gpu(args, rank, world, local_rank):
     if not args.no_mixed:
         tc_ms = mixed_k.get("schur_tc", (0.0, 1))
         line["mixed"] = {
-            "metric": "assembly+Schur elements/s (TF32 tensor-core Schur GEMMs, FP64 LU/residual)",
+            "metric": "assembly+Schur elements/s (precision mode 1: 3xTF32 element contractions, TF32 tensor-core "
+                      "Schur GEMMs, FP64 LU/residual)",
             "value": world * ne * args.steps / (mixed_ms * 1e-3), "unit": "elements/s",
             "ms_per_step": mixed_ms / args.steps, "speedup_vs_fp64": ms / mixed_ms,
             "error_vs_fp64": mixed_err,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in mixed_k.items()},
             "schur_tc_tflops": (2.0 * prob.n_local * prob.n_trace * (prob.n_local + prob.n_trace)) * ne
                                / (tc_ms[0] / tc_ms[1] * 1e-3) / 1e12 if tc_ms[0] > 0 else None}
+        line["mixed_split"] = {
+            "metric": "assembly+Schur elements/s (precision mode 3: 3xTF32 element contractions, FP64 LU, Schur "
+                      "and residual)",
+            "value": world * ne * args.steps / (split_ms * 1e-3), "unit": "elements/s",
+            "ms_per_step": split_ms / args.steps, "speedup_vs_fp64": ms / split_ms,
+            "error_vs_fp64": split_err,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in split_k.items()}}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_cpu(args.workload, seconds_per_proc=args.cpu_seconds)
     return line
@@ -479,8 +496,12 @@ def run_dirk_task(args):
     prob, ke, iters, times = run(args.tgv_n, args.dirk_precision, args.dirk_steps, True)
     out = {"metric": f"DIRK(3,3) time steps/s (3D TGV {args.tgv_n}^3x6 tets = {prob.mesh.ne} elements, p=3)",
            "value": 1e3 / float(np.mean(times)), "unit": "steps/s", "impl": "hfem",
-           "dtype": {0: "f64", 1: "mixed: f32 preconditioner, tf32 condensation GEMMs, f64 Newton/Arnoldi",
-                     2: "mixed: f32 preconditioner, f64 Jacobian, Newton and Arnoldi"}[args.dirk_precision],
+           "dtype": {0: "f64",
+                     1: "mixed: f32 preconditioner, 3xtf32 element contractions, tf32 condensation GEMMs, "
+                        "f64 Newton/Arnoldi",
+                     2: "mixed: f32 preconditioner, f64 Jacobian, Newton and Arnoldi",
+                     3: "mixed: f32 preconditioner, 3xtf32 element contractions, f64 condensation, Newton and "
+                        "Arnoldi"}[args.dirk_precision],
            "ms_per_step": float(np.mean(times)), "steps": args.dirk_steps, "newton_iterations": iters,
            "newton_tol": args.dirk_tol, "kinetic_energy": ke.tolist(), "higher_is_better": True}
     if args.dirk_precision != 0:
@@ -606,7 +627,7 @@ def main():
     ap.add_argument("--workload", default="ns3d_p3_48k", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (TF32 Schur) leg")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision legs (precision modes 1 and 3)")
     ap.add_argument("--e2e-chunks", type=int, default=8, help="pieces of the element-wise state copied ahead of the element kernel in the e2e leg")
     ap.add_argument("--task", default="assembly", choices=["assembly", "newton", "dirk", "serve", "batched"])
     ap.add_argument("--batched-meshes", type=int, default=64)
@@ -616,8 +637,9 @@ def main():
     ap.add_argument("--tgv-n", type=int, default=16)
     ap.add_argument("--dirk-steps", type=int, default=20)
     ap.add_argument("--dirk-tol", type=float, default=1e-10)
-    ap.add_argument("--dirk-precision", type=int, default=2, choices=[0, 1, 2],
-                    help="0 FP64; 1 TF32 Schur + FP32 preconditioner; 2 FP32 preconditioner (config 4)")
+    ap.add_argument("--dirk-precision", type=int, default=2, choices=[0, 1, 2, 3],
+                    help="0 FP64; 1 3xTF32 element + TF32 Schur + FP32 preconditioner; 2 FP32 preconditioner "
+                         "(config 4); 3 3xTF32 element + FP32 preconditioner")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[20.0, 50.0, 100.0])
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-seq-requests", type=int, default=2000)

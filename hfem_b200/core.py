@@ -274,8 +274,9 @@ class HDGSolver:
         return o2u
 
     def set_precision(self, mode):
-        """0: FP64 throughout; 1: TF32 tensor-core Schur GEMMs and FP32 preconditioner (FP64 LU,
-        residuals, Arnoldi); 2: FP32 preconditioner only."""
+        """0: FP64 throughout; 1: 3xTF32 element contractions, TF32 tensor-core Schur GEMMs and FP32
+        preconditioner; 2: FP32 preconditioner only; 3: 3xTF32 element contractions and FP32
+        preconditioner with FP64 Schur (FP64 LU, residuals and Arnoldi in every mode)."""
         self._chk(self.lib.hfem_set_precision(self.h, int(mode)), "set_precision")
 
     def set_timing(self, on=True):

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include "elem_kernels.cuh"
 #include "schur_kernels.cuh"
+#include "tf32x3.cuh"
 
 namespace hfem {
 
@@ -159,7 +160,7 @@ struct ElemSmem {
     int pos[S::NFE * S::NPV];              // position of element node a on face fc, or -1
 };
 
-template <class S>
+template <class S, bool TF = false>
 __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
     constexpr int ND = S::ND, NPV = S::NPV, NPF = S::NPF, NGV = S::NGV, NGF = S::NGF, NFE = S::NFE;
     constexpr int NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, ND1 = S::ND1, N = S::N, NB = S::NB;
@@ -409,7 +410,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                     double y = 0.0;
 #pragma unroll
                     for (int r = 0; r < ND1; r++) y += sm.Av[i + G::LDAV * (g + NGV * r)] * w[r];
-                    Ys[g + NGV * (c + NC * (i + NPV * j))] = y;
+                    bput<TF>(&Ys[g + NGV * (c + NC * (i + NPV * j))], y);
                 }
 #pragma unroll
                 for (int r = 0; r < ND1; r++) w[r] = wn[r];
@@ -424,21 +425,21 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             for (int t = tid; t < G::KV3 * G::NKP; t += NT) {
                 const int k = t % G::KV3, a = t / G::KV3;
                 if (a < NPV && k >= NGV && k < NGV * ND1) continue;
-                Phi[k + G::LDBD * a] = (a < NPV && k < NGV) ? T.shapvt[k + NGV * a] : 0.0;
+                bput<TF>(&Phi[k + G::LDBD * a], (a < NPV && k < NGV) ? T.shapvt[k + NGV * a] : 0.0);
             }
             for (int t = tid; t < G::KV3 * G::NHP; t += NT) {
                 const int k = t % G::KV3, f2 = t / G::KV3;
                 if (f2 < NDF && k < NGV * ND) continue;
-                Psi[k + G::LDBD * f2] = 0.0;
+                bput<TF>(&Psi[k + G::LDBD * f2], 0.0);
             }
             basis_ce_gemm<NGV, NPV, NPV, NPV * ND + NDF * ND, NT / 32>(
                 T.shapvt, NGV, nullptr, Cm, [&](int g, int n, double v) {
                     if (n < NPV * ND) {
                         const int a = n % NPV, d = n / NPV;
-                        Phi[(g + NGV * (d + 1)) + G::LDBD * a] = v;
+                        bput<TF>(&Phi[(g + NGV * (d + 1)) + G::LDBD * a], v);
                     } else {
                         const int f2 = (n - NPV * ND) % NDF, d = (n - NPV * ND) / NDF;
-                        Psi[(g + NGV * d) + G::LDBD * f2] = -v;
+                        bput<TF>(&Psi[(g + NGV * d) + G::LDBD * f2], -v);
                     }
                 });
         }
@@ -453,6 +454,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             // with NGV a multiple of 4 the F part's A values are the D part's
             // shifted by NGV/4 k-steps (the q derivatives d' = d + 1)
             constexpr bool SHIFT = NGV % 4 == 0 && G::KV3 == NGV * ND1;
+            if constexpr (!TF) {
             for (int mp = warp; 2 * mp < MTD; mp += NT / 32) {
                 int rr[2];
                 bool rv[2];
@@ -541,6 +543,110 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                         }
                 }
             }
+            } else {
+            // 3xTF32: the same m-tile pairs as one m16 tile, k-steps of 8
+            const uint2* Phi2 = reinterpret_cast<const uint2*>(Phi);
+            const uint2* Psi2 = reinterpret_cast<const uint2*>(Psi);
+            constexpr int KS = G::KV3 / 4, KSQ = G::KQ3 / 4;
+            for (int mp = warp; 2 * mp < MTD; mp += NT / 32) {
+                int rr[2];
+                bool rv[2];
+                const uint2* yrow[2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    rr[u] = 8 * (2 * mp + u) + gr;
+                    rv[u] = rr[u] < NPV * NCU * NCU;
+                    const int i = rr[u] % NPV, j = (rr[u] / NPV) % NCU, k = rr[u] / (NPV * NCU);
+                    yrow[u] = reinterpret_cast<const uint2*>(Ys) + NGV * (k + NC * (i + NPV * j));
+                }
+                uint32_t ah[2][KS], al[2][KS];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int ks = 0; ks < KS; ks++) {
+                        const int kk = 4 * ks + gc, g = kk % NGV, dp = kk / NGV;
+                        const uint2 y = (rv[u] && kk < NGV * ND1) ? yrow[u][g + NGV * NCU * dp] : make_uint2(0u, 0u);
+                        ah[u][ks] = y.x;
+                        al[u][ks] = y.y;
+                    }
+                {
+                    float acc[G::NTK][4];
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++) acc[b][0] = acc[b][1] = acc[b][2] = acc[b][3] = 0.f;
+#pragma unroll
+                    for (int s8 = 0; s8 < (KS + 1) / 2; s8++) {
+                        const int k0 = 2 * s8, k1 = 2 * s8 + 1;
+                        const uint32_t fh[4] = {ah[0][k0], ah[1][k0], k1 < KS ? ah[0][k1 < KS ? k1 : 0] : 0u,
+                                                k1 < KS ? ah[1][k1 < KS ? k1 : 0] : 0u};
+                        const uint32_t fl[4] = {al[0][k0], al[1][k0], k1 < KS ? al[0][k1 < KS ? k1 : 0] : 0u,
+                                                k1 < KS ? al[1][k1 < KS ? k1 : 0] : 0u};
+#pragma unroll
+                        for (int b = 0; b < G::NTK; b++) {
+                            const uint2 b0 = Phi2[(8 * s8 + gc) + G::LDBD * (8 * b + gr)];
+                            const uint2 b1 = k1 < KS ? Phi2[(8 * s8 + 4 + gc) + G::LDBD * (8 * b + gr)] : make_uint2(0u, 0u);
+                            mma_3xtf32(acc[b], fh, fl, b0, b1);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; u++) {
+                        if (!rv[u]) continue;
+                        const int i = rr[u] % NPV, j = (rr[u] / NPV) % NCU, k = rr[u] / (NPV * NCU);
+#pragma unroll
+                        for (int b = 0; b < G::NTK; b++)
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                const int a = 8 * b + 2 * gc + h;
+                                if (a < NPV) De[i + NPV * (j + NCU * (a + NPV * k))] = (double)acc[b][2 * u + h];
+                            }
+                    }
+                }
+                uint32_t qh[2][KSQ], ql[2][KSQ];
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int ks = 0; ks < KSQ; ks++) {
+                        if constexpr (SHIFT) {
+                            qh[u][ks] = ah[u][ks + NGV / 4];
+                            ql[u][ks] = al[u][ks + NGV / 4];
+                        } else {
+                            const int kk = 4 * ks + gc, g = kk % NGV, d = kk / NGV;
+                            const uint2 y =
+                                (rv[u] && kk < NGV * ND) ? yrow[u][g + NGV * NCU * (d + 1)] : make_uint2(0u, 0u);
+                            qh[u][ks] = y.x;
+                            ql[u][ks] = y.y;
+                        }
+                    }
+                float accf[G::NTH][4];
+#pragma unroll
+                for (int b = 0; b < G::NTH; b++) accf[b][0] = accf[b][1] = accf[b][2] = accf[b][3] = 0.f;
+#pragma unroll
+                for (int s8 = 0; s8 < (KSQ + 1) / 2; s8++) {
+                    const int k0 = 2 * s8, k1 = 2 * s8 + 1;
+                    const uint32_t fh[4] = {qh[0][k0], qh[1][k0], k1 < KSQ ? qh[0][k1 < KSQ ? k1 : 0] : 0u,
+                                            k1 < KSQ ? qh[1][k1 < KSQ ? k1 : 0] : 0u};
+                    const uint32_t fl[4] = {ql[0][k0], ql[1][k0], k1 < KSQ ? ql[0][k1 < KSQ ? k1 : 0] : 0u,
+                                            k1 < KSQ ? ql[1][k1 < KSQ ? k1 : 0] : 0u};
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++) {
+                        const uint2 b0 = Psi2[(8 * s8 + gc) + G::LDBD * (8 * b + gr)];
+                        const uint2 b1 = k1 < KSQ ? Psi2[(8 * s8 + 4 + gc) + G::LDBD * (8 * b + gr)] : make_uint2(0u, 0u);
+                        mma_3xtf32(accf[b], fh, fl, b0, b1);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    if (!rv[u]) continue;
+                    const int i = rr[u] % NPV, j = (rr[u] / NPV) % NCU, k = rr[u] / (NPV * NCU);
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int f2 = 8 * b + 2 * gc + h;
+                            if (f2 < NDF) Fe[i + NPV * (j + NCU * (k + NCH * f2))] = (double)accf[b][2 * u + h];
+                        }
+                }
+            }
+            }
         }
         // ---- Ru = Ru_vol + P Rh (fhat on every face) and ||Ru||^2
         double ru2 = 0.0;
@@ -579,23 +685,23 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                     const int p = sm.pos[fc * NPV + a];
                     x = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
                 }
-                BK[k + G::LDBK * a] = x;
+                bput<TF>(&BK[k + G::LDBK * a], x);
             }
             for (int t = tid; t < G::KFD * G::NHP; t += NT) {
                 const int k = t % G::KFD, f2 = t / G::KFD, q = k % NGF;
                 if (f2 < NDF && k >= NGF && k < NGF * ND1) continue;
                 double x = 0.0;
                 if (f2 < NDF && k < NGF) x = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
-                BH[k + G::LDBK * f2] = x;
+                bput<TF>(&BH[k + G::LDBK * f2], x);
             }
             basis_ce_gemm<NGF, NPF, NPV, NPV * ND + NDF * ND, NT / 32>(
                 sm.sfc, NGF, sm.perm + fc * NPF, Cm, [&](int q, int n, double v) {
                     if (n < NPV * ND) {
                         const int a = n % NPV, d = n / NPV;
-                        BK[(q + NGF * (d + 1)) + G::LDBK * a] = v;
+                        bput<TF>(&BK[(q + NGF * (d + 1)) + G::LDBK * a], v);
                     } else {
                         const int f2 = (n - NPV * ND) % NDF, d = (n - NPV * ND) / NDF;
-                        BH[(q + NGF * (d + 1)) + G::LDBK * f2] = -v;
+                        bput<TF>(&BH[(q + NGF * (d + 1)) + G::LDBK * f2], -v);
                     }
                 });
             cp_async_wait<0>();
@@ -605,6 +711,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             // the d' = 0 rows of BH are zero outside the face's own columns
             // fc NPF .. fc NPF + NPF - 1: those n-tiles are skipped there
             const int blo = (fc * NPF) / 8, bhi = (fc * NPF + NPF - 1) / 8;
+            if constexpr (!TF) {
             // m-tiles in pairs, as in the volume GEMM: one B fragment, two DMMAs
             for (int mp = warp; 2 * mp < MTK; mp += NT / 32) {
                 int jj[2], ipp[2], mm[2], inode[2];
@@ -688,6 +795,111 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                                 if (liftF) atomicAdd(&Fe[inode[u] + NPV * (j + NCU * (m + NCH * f2))], acch[u][b][h]);
                             }
                         }
+            }
+            } else {
+            // 3xTF32: the m-tile pair as one m16 tile, k-steps of 8
+            const uint2* BK2 = reinterpret_cast<const uint2*>(BK);
+            const uint2* BH2 = reinterpret_cast<const uint2*>(BH);
+            constexpr int KS = G::KFD / 4;
+            for (int mp = warp; 2 * mp < MTK; mp += NT / 32) {
+                int jj[2], ipp[2], mm[2], inode[2];
+                bool rv[2];
+                uint32_t kh[2][KS], kl[2][KS], hh[2][KH0], hl[2][KH0];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int r = 8 * (2 * mp + u) + gr;
+                    rv[u] = r < NPF * NCH * NCU;
+                    jj[u] = r % NCH, ipp[u] = (r / NCH) % NPF, mm[u] = r / (NPF * NCH);
+                    inode[u] = sm.perm[fc * NPF + ipp[u]];
+#pragma unroll
+                    for (int ks = 0; ks < KS; ks++) {
+                        const int k = 4 * ks + gc, q = k % NGF, dp = k / NGF;
+                        double vK = 0.0, vH = 0.0;
+                        if (rv[u] && k < NGF * ND1) {
+                            const double sf = sm.Af[ipp[u] + G::LDAF * q];
+                            if (dp == 0) {
+                                vK = sf * sfu[q + NGF * (jj[u] + NCH * mm[u])];
+                                vH = sf * sfuh[q + NGF * (jj[u] + NCH * mm[u])];
+                            } else {
+                                vK = sf * sfu[q + NGF * (jj[u] + NCH * (NCU * dp + mm[u]))];
+                                vH = vK;
+                            }
+                        }
+                        const uint2 sk = tf32_split(vK);
+                        kh[u][ks] = sk.x;
+                        kl[u][ks] = sk.y;
+                        if (ks < KH0) {
+                            const uint2 sh = tf32_split(vH);
+                            hh[u][ks < KH0 ? ks : 0] = sh.x;
+                            hl[u][ks < KH0 ? ks : 0] = sh.y;
+                        }
+                    }
+                }
+                {
+                    float acc[G::NTK][4];
+#pragma unroll
+                    for (int b = 0; b < G::NTK; b++) acc[b][0] = acc[b][1] = acc[b][2] = acc[b][3] = 0.f;
+#pragma unroll
+                    for (int s8 = 0; s8 < (KS + 1) / 2; s8++) {
+                        const int k0 = 2 * s8, k1 = 2 * s8 + 1, k1c = k1 < KS ? k1 : 0;
+                        const uint32_t fh[4] = {kh[0][k0], kh[1][k0], k1 < KS ? kh[0][k1c] : 0u, k1 < KS ? kh[1][k1c] : 0u};
+                        const uint32_t fl[4] = {kl[0][k0], kl[1][k0], k1 < KS ? kl[0][k1c] : 0u, k1 < KS ? kl[1][k1c] : 0u};
+#pragma unroll
+                        for (int b = 0; b < G::NTK; b++) {
+                            const uint2 b0 = BK2[(8 * s8 + gc) + G::LDBK * (8 * b + gr)];
+                            const uint2 b1 = k1 < KS ? BK2[(8 * s8 + 4 + gc) + G::LDBK * (8 * b + gr)] : make_uint2(0u, 0u);
+                            mma_3xtf32(acc[b], fh, fl, b0, b1);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; u++)
+#pragma unroll
+                        for (int b = 0; b < G::NTK; b++)
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                const int a = 8 * b + 2 * gc + h;
+                                if (rv[u] && a < NPV) {
+                                    const int j = jj[u], ip = ipp[u], m = mm[u];
+                                    const double v = (double)acc[b][2 * u + h];
+                                    if (store) Ke[j + NCH * (fc * NPF + ip) + (size_t)NB * (a + NPV * m)] = v;
+                                    if (liftD) atomicAdd(&De[inode[u] + NPV * (j + NCU * (a + NPV * m))], v);
+                                }
+                            }
+                }
+                float acch[G::NTH][4];
+#pragma unroll
+                for (int b = 0; b < G::NTH; b++) acch[b][0] = acch[b][1] = acch[b][2] = acch[b][3] = 0.f;
+#pragma unroll
+                for (int s8 = 0; s8 < (KS + 1) / 2; s8++) {
+                    const int k0 = 2 * s8, k1 = 2 * s8 + 1, k1c = k1 < KS ? k1 : 0;
+                    // entries of k4-step ks: the d' = 0 values for ks < KH0, else K's
+                    auto eh = [&](int u, int ks) { return ks < KH0 ? hh[u][ks < KH0 ? ks : 0] : kh[u][ks]; };
+                    auto el = [&](int u, int ks) { return ks < KH0 ? hl[u][ks < KH0 ? ks : 0] : kl[u][ks]; };
+                    const uint32_t fh[4] = {eh(0, k0), eh(1, k0), k1 < KS ? eh(0, k1c) : 0u, k1 < KS ? eh(1, k1c) : 0u};
+                    const uint32_t fl[4] = {el(0, k0), el(1, k0), k1 < KS ? el(0, k1c) : 0u, k1 < KS ? el(1, k1c) : 0u};
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++) {
+                        if (4 * k1 + 3 < NGF && (b < blo || b > bhi)) continue;
+                        const uint2 b0 = BH2[(8 * s8 + gc) + G::LDBK * (8 * b + gr)];
+                        const uint2 b1 = k1 < KS ? BH2[(8 * s8 + 4 + gc) + G::LDBK * (8 * b + gr)] : make_uint2(0u, 0u);
+                        mma_3xtf32(acch[b], fh, fl, b0, b1);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int b = 0; b < G::NTH; b++)
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            const int f2 = 8 * b + 2 * gc + h;
+                            if (rv[u] && f2 < NDF) {
+                                const int j = jj[u], ip = ipp[u], m = mm[u];
+                                const double v = (double)acch[b][2 * u + h];
+                                if (store) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = v;
+                                if (liftF) atomicAdd(&Fe[inode[u] + NPV * (j + NCU * (m + NCH * f2))], v);
+                            }
+                        }
+            }
             }
         };
         for (int fc = 0; fc < NFE; fc++) {

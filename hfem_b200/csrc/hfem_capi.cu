@@ -113,8 +113,10 @@ struct Launch {
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
     void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
     void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
+    void (*element_tf)(dim3, size_t, cudaStream_t, const ElemArgs&);   // 3xTF32 contractions
     size_t elem_smem;
     const void* elem_fn;
+    const void* elem_fn_tf;
     int inv_threads;
     size_t inv_smem;
     const void *q_fn, *inv_fn;
@@ -133,8 +135,10 @@ void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int*
     inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info);
 }
 
-template <class S>
-void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) { element_kernel<S><<<g, NT, sm, st>>>(a); }
+template <class S, bool TF>
+void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) {
+    element_kernel<S, TF><<<g, NT, sm, st>>>(a);
+}
 template <class S>
 void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
 template <class S>
@@ -172,9 +176,11 @@ Launch make_launch() {
     L.getq = launch_getq<S>;
     L.q_fn = (const void*)getq_kernel<S>;
     L.inverse = launch_inverse<S::N>;
-    L.element = launch_element<S>;
+    L.element = launch_element<S, false>;
+    L.element_tf = launch_element<S, true>;
     L.elem_smem = sizeof(ElemSmem<S>);
-    L.elem_fn = (const void*)element_kernel<S>;
+    L.elem_fn = (const void*)element_kernel<S, false>;
+    L.elem_fn_tf = (const void*)element_kernel<S, true>;
     L.inv_threads = InvBlk<S::N>::THREADS;
     L.inv_smem = InvBlk<S::N>::SMEM;
     L.inv_fn = (const void*)inverse_blocked_kernel<S::N>;
@@ -209,7 +215,7 @@ struct hfem_ctx {
     cudaStream_t own = nullptr, stream = nullptr;
     std::string err;
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
-    int grid_elem = 0, grid_inv = 0, grid_tc = 0;
+    int grid_elem = 0, grid_elem_tf = 0, grid_inv = 0, grid_tc = 0;
     // element-wise state arriving in pieces (hfem_assemble_host): the element
     // kernel of piece k waits for chunk_ev[k]
     cudaStream_t copy_stream = nullptr;
@@ -219,7 +225,10 @@ struct hfem_ctx {
     double* seg_partk = nullptr;            // CGS2 partial dots, npieces x (restart + 1)
     size_t seg_partk_n = 0;
     int seg_hP = 0;
-    int precision = 0;          // 0 FP64; 1 TF32 tensor-core Schur GEMMs + FP32 preconditioner; 2 FP32 preconditioner only
+    // 0 FP64; 1 3xTF32 element contractions, TF32 tensor-core Schur GEMMs, FP32
+    // preconditioner; 2 FP32 preconditioner only; 3 3xTF32 element contractions,
+    // FP64 Schur, FP32 preconditioner
+    int precision = 0;
     int g1_sel = -1, g2_sel = -1;   // autotuned batched-GEMM tilings (-1: the shape's default)
     // boundary faces (mesh.bf, app.bcm, app.bcs); bf == NULL: no boundary faces
     int *bf = nullptr, *bcm = nullptr;
@@ -579,7 +588,9 @@ int ready(hfem_ctx* c) {
 // sequence can be captured into a CUDA graph).  Buffers must exist.
 int enqueue_assembly(hfem_ctx* c, bool matrix) {
     int rc;
-    const dim3 ge(c->grid_elem);
+    const bool tf = c->precision == 1 || c->precision == 3;
+    const dim3 ge(tf ? c->grid_elem_tf : c->grid_elem);
+    auto element = tf ? c->L->element_tf : c->L->element;
     {
         Timed t(c, "element");
         if (c->pending_chunks > 0) {
@@ -589,12 +600,12 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
                 ElemArgs a = elem_args(c);
                 a.e_begin = c->chunk_lo[k];
                 a.ne = c->chunk_lo[k + 1];
-                c->L->element(ge, c->L->elem_smem, c->stream, a);
+                element(ge, c->L->elem_smem, c->stream, a);
                 if ((rc = check_launch(c, "element"))) return rc;
             }
             c->pending_chunks = 0;
         } else {
-            c->L->element(ge, c->L->elem_smem, c->stream, elem_args(c));
+            element(ge, c->L->elem_smem, c->stream, elem_args(c));
             if ((rc = check_launch(c, "element"))) return rc;
         }
     }
@@ -1555,10 +1566,15 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     c->stream = c->own;
     const Launch& L = *c->L;
     cudaFuncSetAttribute(L.elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
+    cudaFuncSetAttribute(L.elem_fn_tf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
     cudaFuncSetAttribute(L.q_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.q_smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn, NT, L.elem_smem);
     c->grid_elem = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
+    occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn_tf, NT, L.elem_smem);
+    // the workspace has grid_elem slots
+    c->grid_elem_tf = std::max(1, std::min(c->grid_elem, sms(device) * std::max(occ, 1)));
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
     cudaFuncSetAttribute(L.tc_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.tc_smem);
@@ -2296,9 +2312,10 @@ long long hfem_pool_cached_bytes(void) {
 
 int hfem_set_precision(hfem_ctx* c, int mode) {
     if (!c) return HFEM_E_ARG;
-    if (mode < 0 || mode > 2)
-        return fail(c, HFEM_E_ARG, "precision mode must be 0 (FP64), 1 (TF32 Schur, FP32 preconditioner) or 2 "
-                                   "(FP32 preconditioner)");
+    if (mode < 0 || mode > 3)
+        return fail(c, HFEM_E_ARG, "precision mode must be 0 (FP64), 1 (3xTF32 element contractions, TF32 Schur, "
+                                   "FP32 preconditioner), 2 (FP32 preconditioner) or 3 (3xTF32 element "
+                                   "contractions, FP32 preconditioner)");
     c->precision = mode;
     c->assembled = false;
     return 0;

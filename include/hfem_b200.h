@@ -155,14 +155,19 @@ int hfem_dirk_step(hfem_ctx* ctx, double dt, int stages, int order, double newto
                    int precond, int restart, double gmres_tol, int gmres_maxit, int* newton_iters);
 
 /* Arithmetic of the assembly and solve (no counterpart in the reference, which
- * is FP64 throughout).  mode 0: FP64 everywhere (default).  mode 1: the two
- * Schur GEMMs (D^-1 F and H - K D^-1 F) on the tcgen05 tensor cores in TF32
- * with FP32 accumulation, and the preconditioner applied with FP32 factors
- * (block-Jacobi inverses, BILU0 factors); the element LU, the residuals
- * (rnorm), the Arnoldi process and the Newton update stay FP64, so Newton
- * iterations refine the solution to the FP64 residual tolerance.  mode 2: only
- * the preconditioner in FP32 (the Jacobian FP64, so Newton converges as in
- * mode 0 while GMRES applies FP32 factors). */
+ * is FP64 throughout).  mode 0: FP64 everywhere (default).  mode 1: the
+ * element contractions (volume D = Y'Phi, F = Y'Psi and the face K, H rows)
+ * in 3xTF32 split precision on the tensor cores with FP32 accumulation, the
+ * two Schur GEMMs (D^-1 F and H - K D^-1 F) on the tcgen05 tensor cores in
+ * TF32 with FP32 accumulation, and the preconditioner applied with FP32 factors
+ * (block-Jacobi inverses, BILU0 factors).  mode 2: only the preconditioner in
+ * FP32 (the Jacobian FP64, so Newton converges as in mode 0 while GMRES
+ * applies FP32 factors).  mode 3: the 3xTF32 element contractions and the FP32
+ * preconditioner, the Schur GEMMs in FP64 (Jacobian blocks good to about 1e-6
+ * relative, so Newton keeps its FP64 iteration count).  In every mode the
+ * element LU, the residuals (rnorm), the Arnoldi process and the Newton update
+ * stay FP64, so Newton iterations refine the solution to the FP64 residual
+ * tolerance. */
 int hfem_set_precision(hfem_ctx* ctx, int mode);
 
 /* y = Hg x with device pointers x, y (nf*bsz doubles each, on the context's

@@ -47,16 +47,17 @@ def test_dirk33_tgv_matches_oracle():
     assert ke[-1] < ke[0]            # viscous decay
 
 
-@pytest.mark.parametrize("precision", [0, 1, 2], ids=["fp64", "mixed", "fp32_preconditioner"])
+@pytest.mark.parametrize("precision", [0, 1, 2, 3], ids=["fp64", "mixed", "fp32_preconditioner", "split_tf32"])
 def test_dirk33_tgv_p3_20_steps_match_reference_driver(precision):
     """The Taylor-Green DIRK workload at the size the reference finishes in
     minutes: 4^3 x 6 tetrahedra, p = 3, DIRK(3,3), 20 steps of dt = 0.01, each
     stage solved by Newton to 1e-10.  The fixture holds the kinetic-energy
     history of the reference's own driver (solveUnsteadyProblem, made by
     tests/golden/make_golden.py).  Mixed precision: FP32 block-Jacobi inverses
-    and the TF32 condensation GEMMs (mode 1) or the FP32 inverses alone with the
-    FP64 Jacobian (mode 2, the precision of the Taylor-Green workload), with
-    FP64 residuals, Arnoldi and Newton updates in both.  Bar: kinetic energy within 1e-9 relative at every step;
+    with the 3xTF32 element contractions and the TF32 condensation GEMMs (mode
+    1), the FP32 inverses alone with the FP64 Jacobian (mode 2, the precision of
+    the Taylor-Green workload), or the FP32 inverses with the 3xTF32 element
+    contractions (mode 3), with FP64 residuals, Arnoldi and Newton updates in all.  Bar: kinetic energy within 1e-9 relative at every step;
     final state within 1e-8 of the reference's (both converged to 1e-10)."""
     import os
     g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tgv_p3_n4_dirk20.npz")))
