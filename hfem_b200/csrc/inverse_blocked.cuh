@@ -206,11 +206,41 @@ __global__ void __launch_bounds__(InvBlk<N>::THREADS, 2)
                     if (lane == 0 && bad) s_bad = bad;
                 }
             } else {
-#pragma unroll 2
-                for (int t = warp - 1; t < C::MT * C::NTL; t += NW - 1) {
-                    const int mt = t % C::MT, nt = t / C::MT;
+                // the other warps: pairs of row tiles x column tiles, each warp a
+                // contiguous run of them, so the panel fragments of its row pair
+                // stay in registers across the run and every B fragment feeds
+                // both row tiles
+                constexpr int PR = (C::MT + 1) / 2, ITEMS = PR * C::NTL, UW = NW - 1;
+                constexpr int RUN = (ITEMS + UW - 1) / UW;
+                const int t0 = (warp - 1) * RUN, t1 = min(ITEMS, t0 + RUN);
+                int cur = -1;
+                double w[2][2];
+                for (int t = t0; t < t1; t++) {
+                    const int pr = t / C::NTL, nt = t % C::NTL;
+                    if (pr != cur) {
+                        cur = pr;
+#pragma unroll
+                        for (int u = 0; u < 2; u++) {
+                            const int mt = 2 * pr + u;
+                            const double* wp = A + 8 * mt + gr + LDA * (kb + gc);
+                            w[u][0] = mt < C::MT ? wp[0] : 0.0;
+                            w[u][1] = (mt < C::MT && bn > 4) ? wp[4 * LDA] : 0.0;
+                        }
+                    }
                     if (nt == ptile || nt == ntile) continue;
-                    inv_tile<N>(A, B, mt, nt, kb, bn, gr, gc);
+                    const double* bp = B + gc + LDB * (8 * nt + gr);
+                    const double b0 = bp[0], b1 = bp[4];
+#pragma unroll
+                    for (int u = 0; u < 2; u++) {
+                        const int mt = 2 * pr + u;
+                        if (mt >= C::MT) continue;
+                        double* cp = A + 8 * mt + gr + LDA * (8 * nt + 2 * gc);
+                        double c0 = cp[0], c1 = cp[LDA];
+                        dmma8x8x4(c0, c1, w[u][0], b0);
+                        if (bn > 4) dmma8x8x4(c0, c1, w[u][1], b1);
+                        cp[0] = c0;
+                        cp[LDA] = c1;
+                    }
                 }
             }
             __syncthreads();
