@@ -14,7 +14,8 @@ column-major ``npv x nc x ne`` etc.).  The named workloads are:
 Physics parameters are ``param = [gamma, eps, Re, Pr, Mach, tau]``
 (``application/FM/nsNew/flux_ns2dNEW.c:7-12``, ``runns.m:31``), constant
 stabilisation ``tau = 2`` (``convStabMethod = 0``) and constant viscosity
-(``viscosityModel = 0``).  Every problem here carries the time term of one
+(``viscosityModel = 0``) unless :func:`with_models` selects the Lax-Friedrichs
+or Roe stabilisation tensor or Sutherland's law.  Every problem here carries the time term of one
 implicit stage: ``s += SH - fc_u * u`` with ``SH = fc_u * UDG_n``
 (``elementassembly.cpp:293-304``), which is how both the DIRK driver and a
 pseudo-transient Newton step call the assembly.
@@ -48,6 +49,8 @@ class Problem:
     bcm: np.ndarray = None       # boundary condition type per boundary index (app.bcm); None: periodic
     bcs: np.ndarray = None       # (nbnd, nch) boundary states (app.bcs)
     appname: int = 1             # app.appname: 1 compressible Navier-Stokes, 0 Euler (inviscid, no q equation)
+    conv_stab: int = 0           # app.convStabMethod: 0 constant tau, 1 Lax-Friedrichs, 2 Roe
+    viscosity_model: int = 0     # app.viscosityModel: 0 constant viscosity, 1 Sutherland's law
 
     @property
     def nd(self):
@@ -179,6 +182,18 @@ def as_euler(prob: Problem) -> Problem:
     sh[:, prob.ncu:, :] = 0.0
     meta = dict(prob.meta, physics="euler")
     return replace(prob, name=prob.name + "_euler", udg=udg, sh=sh, appname=0, meta=meta)
+
+
+def with_models(prob: Problem, conv_stab: int = 0, viscosity_model: int = 0) -> Problem:
+    """The same problem with another convective stabilisation tensor
+    (app.convStabMethod: 0 constant tau = param[5], 1 Lax-Friedrichs, 2 Roe;
+    application/FM/stabilizationTensor.cpp) and viscosity model
+    (app.viscosityModel: 0 constant, 1 Sutherland's law; application/FM/getViscosity.c)."""
+    from dataclasses import replace
+    tag = {0: "", 1: "_lf", 2: "_roe"}[conv_stab] + {0: "", 1: "_suth"}[viscosity_model]
+    meta = dict(prob.meta, conv_stab=conv_stab, viscosity_model=viscosity_model)
+    return replace(prob, name=prob.name + tag, conv_stab=int(conv_stab), viscosity_model=int(viscosity_model),
+                   meta=meta)
 
 
 def make_problem(kind: str, **kw) -> Problem:

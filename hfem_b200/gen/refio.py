@@ -38,8 +38,8 @@ def app_arrays(prob: Problem, preconditioner=0, newton_tol=1e-10, gmres_tol=1e-1
     problem[1] = prob.appname        # app.appname: 1 compressible Navier-Stokes, 0 Euler
     problem[3] = dirk_order
     problem[4] = dirk_stage
-    problem[5] = 0                   # constant tau
-    problem[8] = 0                   # constant viscosity
+    problem[5] = getattr(prob, "conv_stab", 0)           # app.convStabMethod: 0 constant tau, 1 LF, 2 Roe
+    problem[8] = getattr(prob, "viscosity_model", 0)     # app.viscosityModel: 0 constant, 1 Sutherland
     problem[12] = 1                  # GMRES
     problem[13] = newton_maxiter
     dt = np.array(dt_list if dt_list is not None else [prob.dt if prob.dt > 0 else 1.0])

@@ -44,6 +44,8 @@ struct oracle_problem {
     const int *bcm;                                    // boundary condition type per ib (app.bcm)
     const double *bcs;                                 // nch per ib (app.bcs)
     int appname;                                       // 1 Navier-Stokes, 0 Euler (inviscid flux)
+    int conv_stab;                                     // app.convStabMethod: 0 constant, 1 Lax-Friedrichs, 2 Roe
+    int visc_model;                                    // app.viscosityModel: 0 constant, 1 Sutherland
 };
 
 }  // extern "C"
@@ -71,8 +73,40 @@ static Dual operator/(const Dual& a, const Dual& b) {
     return r;
 }
 
+static Dual datan(const Dual& a) {
+    Dual r; r.n = a.n; r.v = std::atan(a.v);
+    const double h = 1.0 / (1.0 + a.v * a.v);
+    for (int i = 0; i < a.n; i++) r.d[i] = a.d[i] * h;
+    return r;
+}
+static Dual dpow15(const Dual& a) {              // a^(3/2)
+    Dual r; r.n = a.n; r.v = std::pow(a.v, 1.5);
+    const double h = 1.5 * std::sqrt(a.v);
+    for (int i = 0; i < a.n; i++) r.d[i] = a.d[i] * h;
+    return r;
+}
+
+static int g_visc_model = 0, g_conv_stab = 0;
+
+// Dynamic viscosity (application/FM/getViscosity.c): 0 constant mu = 1
+// (constantDynamicViscosity, 6-22); 1 Sutherland's law regularised at zero
+// (sutherlandLaw2d 25-146, sutherlandLaw3d 275-...): with the temperature
+// T = (rE - |m|^2 / (2 rho)) / (rho gamma (gamma - 1) Mach^2) and a = (S + T0)
+// T^(3/2) / (S + T0 T), S = 111, T0 = 300,
+//   mu = c + a (atan(b a) / pi + 1/2),  b = 100, c = 1/2 - atan(b) / pi.
+static Dual viscosity(int nd, const double* param, const Dual* w) {
+    const int n = w[0].n;
+    if (g_visc_model == 0) return dconst(1.0, n);
+    const double gam = param[0], mach = param[4], S = 111.0, T0 = 300.0, b = 100.0, pi = 3.141592653589793;
+    Dual ke = dconst(0.0, n);
+    for (int i = 0; i < nd; i++) ke = ke + w[1 + i] * w[1 + i];
+    const Dual T = (w[nd + 1] - 0.5 * (ke / w[0])) / ((gam * (gam - 1.0) * mach * mach) * w[0]);
+    const Dual a = (S + T0) * (dpow15(T) / (dconst(S, n) + T0 * T));
+    return dconst(0.5 - std::atan(b) / pi, n) + a * ((1.0 / pi) * datan(b * a) + dconst(0.5, n));
+}
+
 // Compressible Navier-Stokes flux F(u, q) (application/FM/nsNew/flux_ns2dNEW.c:22-74
-// and flux_ns3dNEW.c), constant viscosity mu = 1 (FM/getViscosity.c:5-12):
+// and flux_ns3dNEW.c), viscosity mu(u) from viscosity() (FM/getViscosity.c):
 //   f_rho^d = m_d
 //   f_mi^d  = m_i v_d + p delta_id + tau_id
 //   f_E^d   = (E + p) v_d + sum_i tau_id v_i + mu gamma/(Re Pr) (q_E^d/rho - E q_rho^d/rho^2 - sum_i v_i dv_i/dx_d)
@@ -97,11 +131,12 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
     Dual div = dconst(0.0, n);
     for (int i = 0; i < nd; i++) div = div + dv[i][i];
     Dual tau[3][3];
+    const Dual mu = g_inviscid ? dconst(1.0, n) : viscosity(nd, param, w);
     for (int i = 0; i < nd; i++)
         for (int j = 0; j < nd; j++) {
             Dual t = dv[i][j] + dv[j][i];
             if (i == j) t = t - (2.0 / 3.0) * div;
-            tau[i][j] = (1.0 / Re) * t;
+            tau[i][j] = (1.0 / Re) * (mu * t);
         }
     const double kappa = gam / (Re * Pr);
     if (g_inviscid)
@@ -119,7 +154,7 @@ static void ns_flux(int nd, const double* param, const Dual* w, Dual* f /* [d*nc
         Dual vdv = dconst(0.0, n);
         for (int i = 0; i < nd; i++) { fe = fe + tau[i][d] * v[i]; vdv = vdv + v[i] * dv[i][d]; }
         Dual heat = q[nd + 1] / rho - E * q[0] / (rho * rho) - vdv;
-        f[d * ncu + nd + 1] = g_inviscid ? fe : fe + kappa * heat;
+        f[d * ncu + nd + 1] = g_inviscid ? fe : fe + kappa * (mu * heat);
     }
 }
 
@@ -171,12 +206,88 @@ static void normal_jacobian(int absflag, int nd, const double* param, const Dual
     }
 }
 
+// out = tau(uh) v, the convective stabilization tensor of fhatDriver
+// (application/FM/stabilizationTensor.cpp, getConvectiveStabilizationTensor 3439-3456):
+//   0 constant: param[5] v (getConstantStabilizationTensor, 9-29);
+//   1 Lax-Friedrichs: lam v, lam = |un| + c at uh (3D, 221-425); the 2D routine
+//     (31-218) evaluates lam at the fixed state (rho, rho u, rho v, rho E) =
+//     (1, 0.9994, 0.0349, 1.7858e4) and returns a zero Jacobian, restated as is;
+//   2 Roe (440-1716): |A_n(uh)| v with the eigenvalues un + c, un - c, un taken
+//     through the smooth absolute value r(x) = 2 (x (atan(b x)/pi + 1/2) -
+//     atan(b)/pi + 1/2) - x, b = 10, and, with eps = param[1] > 0, r < eps c
+//     replaced by (r^2 / (eps c) + eps c) / 2; columns as in normal_jacobian.
+static void stab_apply(int nd, const double* param, const double* nl, const Dual* U, const Dual* V, Dual* out) {
+    const int ncu = nd + 2, n = U[0].n;
+    if (g_conv_stab == 0) {
+        for (int j = 0; j < ncu; j++) out[j] = param[5] * V[j];
+        return;
+    }
+    const double gam = param[0], g1 = gam - 1.0, eps = param[1];
+    if (g_conv_stab == 1) {
+        Dual lam;
+        if (nd == 2) {
+            const double r = 1.0, ru = 0.9994, rv = 0.0349, rE = 1.7858e+04;
+            const double uv = ru / r, vv = rv / r, af = 0.5 * (uv * uv + vv * vv), p = g1 * (rE - r * af);
+            const double c = std::sqrt(gam * p / r), un = uv * nl[0] + vv * nl[1];
+            lam = dconst(un >= 0 ? un + c : -un + c, n);
+        } else {
+            const Dual r = U[0];
+            Dual af = dconst(0.0, n), un = dconst(0.0, n);
+            for (int i = 0; i < nd; i++) {
+                const Dual vi = U[1 + i] / r;
+                af = af + 0.5 * (vi * vi);
+                un = un + nl[i] * vi;
+            }
+            const Dual p = g1 * (U[nd + 1] - r * af);
+            const Dual c = dsqrt(gam * (p / r));
+            lam = un.v >= 0 ? un + c : c - un;
+        }
+        for (int j = 0; j < ncu; j++) out[j] = lam * V[j];
+        return;
+    }
+    const double b = 10.0, pi = 3.141592653589793;
+    const Dual r = U[0];
+    Dual uv[3], af = dconst(0.0, n), un = dconst(0.0, n);
+    for (int i = 0; i < nd; i++) {
+        uv[i] = U[1 + i] / r;
+        af = af + 0.5 * (uv[i] * uv[i]);
+        un = un + nl[i] * uv[i];
+    }
+    const Dual E = U[nd + 1] / r;
+    const Dual p = g1 * (U[nd + 1] - r * af);
+    const Dual h = E + p / r;
+    const Dual c2 = gam * (p / r);
+    const Dual c = dsqrt(c2);
+    auto sabs = [&](const Dual& x) {
+        return 2.0 * (x * ((1.0 / pi) * datan(b * x) + dconst(0.5, n)) + dconst(0.5 - std::atan(b) / pi, n)) - x;
+    };
+    Dual rl[3] = {sabs(un + c), sabs(un - c), sabs(un)};
+    if (eps > 0)
+        for (int m = 0; m < 3; m++)
+            if (rl[m].v < eps * c.v) rl[m] = 0.5 * (rl[m] * rl[m] / (eps * c) + eps * c);
+    const Dual s1 = 0.5 * (rl[0] + rl[1]), s2 = 0.5 * (rl[0] - rl[1]), l3 = rl[2];
+    for (int j = 0; j < ncu; j++) out[j] = dconst(0.0, n);
+    for (int k = 0; k < ncu; k++) {
+        const Dual a = (k == 0) ? af : (k == nd + 1 ? dconst(1.0, n) : dconst(0.0, n) - uv[k - 1]);
+        const Dual bb = (k == 0) ? dconst(0.0, n) - un : (k == nd + 1 ? dconst(0.0, n) : dconst(nl[k - 1], n));
+        const Dual cc1 = g1 * ((s1 - l3) * a / c2) + s2 * bb / c;
+        const Dual cc2 = g1 * (s2 * a / c) + (s1 - l3) * bb;
+        for (int j = 0; j < ncu; j++) {
+            const Dual v1 = (j == 0) ? dconst(1.0, n) : (j == nd + 1 ? h : uv[j - 1]);
+            const Dual v2 = (j == 0) ? dconst(0.0, n) : (j == nd + 1 ? un : dconst(nl[j - 1], n));
+            Dual m = cc1 * v1 + cc2 * v2;
+            if (j == k) m = m + l3;
+            out[j] = out[j] + m * V[k];
+        }
+    }
+}
+
 // Boundary flux fb(u, q, uh) of the NS boundary conditions (application/FM/fbou.cpp)
 // at one point, with its Jacobians fb_u[j + nch*k] (k over u and q) and
 // fb_uh[j + nch*k], by forward differentiation over (u, q, uh):
 //   2 no-slip adiabatic wall (fbou.cpp:219-277, fixed mesh): rho - rho_hat,
 //     -m_hat (wall velocity 0), energy row = the interior trace flux
-//     F(uh, q).n + tau (u - uh) of fhatDriver;
+//     F(uh, q).n + tau(uh) (u - uh) of fhatDriver (stab_apply);
 //   5 Dirichlet (fbou.cpp:569-583): tau (ui - uh);
 //   6 extrapolation (fbou.cpp:584-600): u - uh;
 //   7 slip wall (fbou.cpp:601-652, fixed mesh): rho - rho_hat,
@@ -209,7 +320,10 @@ static int fbou_point(int bn, int nd, const double* param, const double* ui, con
         for (int k = 0; k < ncu; k++) wf[k] = U[k];
         for (int k = ncu; k < nc; k++) wf[k] = W[k];
         ns_flux(nd, param, wf.data(), fl.data());
-        Dual t = tau * (W[nd + 1] - U[nd + 1]);
+        std::vector<Dual> du(ncu), st(ncu);
+        for (int k = 0; k < ncu; k++) du[k] = W[k] - U[k];
+        stab_apply(nd, param, nl, U.data(), du.data(), st.data());
+        Dual t = st[nd + 1];
         for (int d = 0; d < nd; d++) t = t + nl[d] * fl[d * ncu + nd + 1];
         F[nd + 1] = t;
     } else if (bn == 5) {
@@ -419,6 +533,8 @@ struct ElemOut {
 static void element(const oracle_problem& P, const Dims& D, const double* udg_all, const double* uh_all,
                     const double* sh_all, int ie, ElemOut& O) {
     g_inviscid = (P.appname == 0);
+    g_conv_stab = P.conv_stab;
+    g_visc_model = P.visc_model;
     const int nd = D.nd, npv = D.npv, ngv = D.ngv, ngf = D.ngf, nfe = D.nfe, npf = D.npf;
     const int ncu = D.ncu, nc = D.nc, nch = D.nch, ndf = D.ndf, nd1 = D.nd1, n = D.n, nb = D.nb;
     const double* udg = udg_all + (size_t)ie * npv * nc;
@@ -558,26 +674,43 @@ static void element(const oracle_problem& P, const Dims& D, const double* udg_al
         for (int c = ncu; c < nc; c++) waux[g + na * c] = ugf[g + na * c];
     }
     flux_points(nd, P.param, na, waux.data(), fh.data(), fhu.data());
-    const double tau = P.param[5];
-    // fhn (na x nch), fhn_u (na x nch x nc), fhn_uh (na x nch x nch), all times jacf
+    // fhn (na x nch), fhn_u (na x nch x nc), fhn_uh (na x nch x nch), all times jacf;
+    // the stabilization term S = tau(uh) (u - uh) and its uh-derivative by
+    // forward differentiation over uh, the columns of tau (the u-derivative) by
+    // applying tau to the unit vectors
     std::vector<double> fn_(na * nch), fn_u(na * nch * nc, 0.0), fn_uh(na * nch * nch, 0.0);
+    std::vector<Dual> Ud(ncu), Vd(ncu), Sd(ncu), U0(ncu), Ek(ncu), Ck(ncu);
+    std::vector<double> nlq(nd), tauM(ncu * ncu);
     for (int g = 0; g < na; g++) {
         const double jf = G.jacf[g];
+        for (int d = 0; d < nd; d++) nlq[d] = G.nl[g + na * d];
+        for (int k = 0; k < ncu; k++) {
+            Ud[k] = dvar(uhg[g + na * k], ncu, k);
+            Vd[k] = dconst(ugf[g + na * k], ncu) - Ud[k];
+            U0[k] = dconst(uhg[g + na * k], 1);
+        }
+        stab_apply(nd, P.param, nlq.data(), Ud.data(), Vd.data(), Sd.data());
+        for (int k = 0; k < ncu; k++) {
+            for (int m = 0; m < ncu; m++) Ek[m] = dconst(m == k ? 1.0 : 0.0, 1);
+            stab_apply(nd, P.param, nlq.data(), U0.data(), Ek.data(), Ck.data());
+            for (int j = 0; j < ncu; j++) tauM[j + ncu * k] = Ck[j].v;
+        }
         for (int j = 0; j < ncu; j++) {
-            double t = tau * (ugf[g + na * j] - uhg[g + na * j]);
+            double t = Sd[j].v;
             for (int d = 0; d < nd; d++) t += fh[g + na * (j + ncu * d)] * G.nl[g + na * d];
             fn_[g + na * j] = t * jf;
             for (int k = 0; k < nc; k++) {
                 double v = 0;
                 if (k >= ncu)
                     for (int d = 0; d < nd; d++) v += fhu[g + na * (j + ncu * (d + nd * k))] * G.nl[g + na * d];
-                if (k == j) v += tau;
+                else
+                    v = tauM[j + ncu * k];
                 fn_u[g + na * (j + nch * k)] = v * jf;
             }
             for (int k = 0; k < nch; k++) {
                 double v = 0;
                 for (int d = 0; d < nd; d++) v += fhu[g + na * (j + ncu * (d + nd * k))] * G.nl[g + na * d];
-                if (k == j) v -= tau;
+                v += Sd[j].d[k];
                 fn_uh[g + na * (j + nch * k)] = v * jf;
             }
         }

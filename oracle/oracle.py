@@ -33,6 +33,7 @@ class OracleProblem(C.Structure):
         ("param", C.c_double * 6), ("tdep", C.c_int),
         ("fc_u", C.c_double), ("fc_q", C.c_double), ("time", C.c_double),
         ("bf", _ip), ("bcm", _ip), ("bcs", _dp), ("appname", C.c_int),
+        ("conv_stab", C.c_int), ("visc_model", C.c_int),
     ]
 
 # boundary condition types restated in hfem_oracle.cpp (fbou_point)
@@ -98,6 +99,8 @@ class Oracle:
             p.param[i] = float(prob.param[i])
         p.tdep, p.fc_u, p.fc_q, p.time = prob.tdep, prob.fc_u, prob.fc_q, prob.time
         p.appname = int(getattr(prob, "appname", 1))
+        p.conv_stab = int(getattr(prob, "conv_stab", 0))
+        p.visc_model = int(getattr(prob, "viscosity_model", 0))
         if getattr(prob, "bcm", None) is not None:
             if any(int(b) not in BC_TYPES for b in prob.bcm):
                 raise ValueError(f"boundary condition types {list(prob.bcm)} not all in {BC_TYPES}")

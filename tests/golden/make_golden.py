@@ -29,7 +29,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from hfem_b200.diagnostics import kinetic_energy  # noqa: E402
-from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier, ns3d_tgv  # noqa: E402
+from hfem_b200.gen.problem import (as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier,  # noqa: E402
+                                   ns3d_tgv, with_models)
 from oracle import run_reference  # noqa: E402
 
 CASES = {
@@ -43,6 +44,16 @@ CASES = {
     "ns3d_box_p1_n2": lambda: ns3d_box(n=2, porder=1),
     "ns2d_farfield_p2_n3": lambda: ns2d_channel(n=3, porder=2, bcm=(1, 1, 1, 1)),
     "euler2d_channel_p2_n3": lambda: as_euler(ns2d_channel(n=3, porder=2, bcm=(1, 6, 7, 2))),
+    # stabilization tensors (app.convStabMethod 1 Lax-Friedrichs, 2 Roe) and
+    # Sutherland's law (app.viscosityModel 1)
+    "ns2d_lf_p2_n3": lambda: with_models(ns2d_vortex(n=3, porder=2), 1, 0),
+    "ns2d_roe_p2_n3": lambda: with_models(ns2d_vortex(n=3, porder=2), 2, 0),
+    "ns2d_suth_p2_n3": lambda: with_models(ns2d_vortex(n=3, porder=2), 0, 1),
+    "ns3d_lf_p2_n3": lambda: with_models(ns3d_fourier(n=3, porder=2), 1, 0),
+    "ns3d_roe_p2_n3": lambda: with_models(ns3d_fourier(n=3, porder=2), 2, 0),
+    "ns3d_suth_p2_n3": lambda: with_models(ns3d_fourier(n=3, porder=2), 0, 1),
+    "ns2d_channel_roe_suth_p2_n3": lambda: with_models(ns2d_channel(n=3, porder=2), 2, 1),
+    "euler2d_channel_lf_p2_n3": lambda: with_models(as_euler(ns2d_channel(n=3, porder=2, bcm=(1, 6, 7, 2))), 1, 0),
 }
 FULL_LIMIT = 400_000          # store arrays up to this many entries in full
 

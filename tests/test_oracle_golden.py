@@ -12,7 +12,7 @@ import os
 import numpy as np
 import pytest
 
-from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier
+from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier, with_models
 from oracle import Oracle
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -27,6 +27,16 @@ CASES = {
     "ns2d_farfield_p2_n3": lambda: ns2d_channel(n=3, porder=2, bcm=(1, 1, 1, 1)),
     # Euler (app.appname 0, flag_q 0): the reference stores no q
     "euler2d_channel_p2_n3": lambda: as_euler(ns2d_channel(n=3, porder=2, bcm=(1, 6, 7, 2))),
+    # stabilization tensors (app.convStabMethod 1 Lax-Friedrichs, 2 Roe) and
+    # Sutherland's law (app.viscosityModel 1)
+    "ns2d_lf_p2_n3": lambda: with_models(ns2d_vortex(n=3, porder=2), 1, 0),
+    "ns2d_roe_p2_n3": lambda: with_models(ns2d_vortex(n=3, porder=2), 2, 0),
+    "ns2d_suth_p2_n3": lambda: with_models(ns2d_vortex(n=3, porder=2), 0, 1),
+    "ns3d_lf_p2_n3": lambda: with_models(ns3d_fourier(n=3, porder=2), 1, 0),
+    "ns3d_roe_p2_n3": lambda: with_models(ns3d_fourier(n=3, porder=2), 2, 0),
+    "ns3d_suth_p2_n3": lambda: with_models(ns3d_fourier(n=3, porder=2), 0, 1),
+    "ns2d_channel_roe_suth_p2_n3": lambda: with_models(ns2d_channel(n=3, porder=2), 2, 1),
+    "euler2d_channel_lf_p2_n3": lambda: with_models(as_euler(ns2d_channel(n=3, porder=2, bcm=(1, 6, 7, 2))), 1, 0),
 }
 
 
