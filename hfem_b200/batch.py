@@ -35,6 +35,9 @@ def union_problem(probs: list) -> tuple:
             raise ValueError("all problems in a union must share the master element")
         if getattr(p, "appname", 1) != getattr(probs[0], "appname", 1):
             raise ValueError("all problems in a union must solve the same equations")
+        if (getattr(p, "conv_stab", 0), getattr(p, "viscosity_model", 0)) != \
+                (getattr(probs[0], "conv_stab", 0), getattr(probs[0], "viscosity_model", 0)):
+            raise ValueError("all problems in a union must share the stabilization tensor and viscosity model")
     npf = m.npf
     eoff = np.cumsum([0] + [p.mesh.ne for p in probs])
     foff = np.cumsum([0] + [p.mesh.nf for p in probs])

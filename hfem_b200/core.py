@@ -54,6 +54,7 @@ def load_library(path: str = LIB):
     lib.hfem_set_mesh.argtypes = [C.c_void_p, _dp, _ip, _ip, _ip, _ip]
     lib.hfem_set_boundary.argtypes = [C.c_void_p, _ip, C.c_int, _ip, _dp]
     lib.hfem_set_app.argtypes = [C.c_void_p, C.c_int]
+    lib.hfem_set_models.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.hfem_set_physics.argtypes = [C.c_void_p, _dp, C.c_int, C.c_double, C.c_double, C.c_double]
     lib.hfem_set_solution.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.hfem_set_solution_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -110,6 +111,8 @@ class HDGSolver:
         self._chk(self.lib.hfem_set_master(self.h, *[_d(k) for k in keep], _i(perm)), "set_master")
         self.set_mesh(me)
         self._chk(self.lib.hfem_set_app(self.h, int(getattr(prob, "appname", 1))), "set_app")
+        self._chk(self.lib.hfem_set_models(self.h, int(getattr(prob, "conv_stab", 0)),
+                                           int(getattr(prob, "viscosity_model", 0))), "set_models")
         if getattr(prob, "bcm", None) is not None:
             self.set_boundary(me.bf, prob.bcm, prob.bcs)
         self.set_physics(prob.param, prob.tdep, prob.fc_u, prob.fc_q, prob.time)

@@ -235,6 +235,8 @@ struct hfem_ctx {
     double* bcs = nullptr;
     int nbnd = 0;
     int appname = 1;            // app.appname: 1 Navier-Stokes, 0 Euler
+    int conv_stab = 0;          // app.convStabMethod: 0 constant tau, 1 Lax-Friedrichs, 2 Roe
+    int visc_model = 0;         // app.viscosityModel: 0 constant, 1 Sutherland's law
     int* tc_err = nullptr;
     double* rn_part = nullptr;
     // master tables
@@ -520,6 +522,8 @@ int ensure_assembly_buffers(hfem_ctx* c) {
 ElemArgs elem_args(hfem_ctx* c) {
     ElemArgs a;
     a.inviscid = c->appname == 0;
+    a.conv_stab = c->conv_stab;
+    a.visc_model = c->visc_model;
     a.bf = c->bf;
     a.bcm = c->bcm;
     a.bcs = c->bcs;
@@ -1770,6 +1774,19 @@ int hfem_set_app(hfem_ctx* c, int appname) {
     if (appname != 0 && appname != 1)
         return fail(c, HFEM_E_UNSUPPORTED, "appname %d (supported: 0 Euler, 1 Navier-Stokes)", appname);
     c->appname = appname;
+    c->assembled = false;
+    return 0;
+}
+
+int hfem_set_models(hfem_ctx* c, int conv_stab, int viscosity_model) {
+    if (!c) return HFEM_E_ARG;
+    if (conv_stab < 0 || conv_stab > 2)
+        return fail(c, HFEM_E_UNSUPPORTED, "convStabMethod %d (supported: 0 constant, 1 Lax-Friedrichs, 2 Roe)",
+                    conv_stab);
+    if (viscosity_model < 0 || viscosity_model > 1)
+        return fail(c, HFEM_E_UNSUPPORTED, "viscosityModel %d (supported: 0 constant, 1 Sutherland)", viscosity_model);
+    c->conv_stab = conv_stab;
+    c->visc_model = viscosity_model;
     c->assembled = false;
     return 0;
 }

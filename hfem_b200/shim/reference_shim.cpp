@@ -79,6 +79,7 @@ inline hfem_ctx* context(sysstruct& sys, meshstruct& mesh, masterstruct& master,
         check(hfem_set_boundary(g_ctx, bf.data(), (int)bcm.size(), bcm.data(), &app.bcs[0]), "hfem_set_boundary");
     }
     check(hfem_set_app(g_ctx, (int)app.appname), "hfem_set_app");
+    check(hfem_set_models(g_ctx, (int)app.convStabMethod, (int)app.viscosityModel), "hfem_set_models");
     return g_ctx;
 }
 

@@ -84,9 +84,20 @@ int hfem_set_boundary(hfem_ctx* ctx, const int* bf, int nbnd, const int* bcm, co
  * the reference's q-free Euler discretisation (flag_q 0, nc = ncu). */
 int hfem_set_app(hfem_ctx* ctx, int appname);
 
+/* The trace-flux stabilization tensor and the viscosity model (app.convStabMethod
+ * and app.viscosityModel, initializestructs.cpp:131,134; digasopre.h:84,88).
+ * conv_stab: 0 constant tau = physicsparam[5] (default), 1 Lax-Friedrichs,
+ * 2 Roe (application/FM/stabilizationTensor.cpp); viscosity_model: 0 constant
+ * (default), 1 Sutherland's law (application/FM/getViscosity.c).  The
+ * no-slip wall's energy row takes the same tensor (its fhat), the Dirichlet
+ * condition keeps physicsparam[5] as the reference's fbou does.  Other values:
+ * HFEM_E_UNSUPPORTED. */
+int hfem_set_models(hfem_ctx* ctx, int conv_stab, int viscosity_model);
+
 /* Physics: physicsparam = [gamma, eps, Re, Pr, Mach, tau] (compressible
- * Navier-Stokes, constant tau, constant viscosity), tdep/fc_u/fc_q/time as
- * appstruct (digasopre.h:7-91); the equations are chosen by hfem_set_app. */
+ * Navier-Stokes), tdep/fc_u/fc_q/time as appstruct (digasopre.h:7-91); the
+ * equations are chosen by hfem_set_app, the stabilization and viscosity by
+ * hfem_set_models. */
 int hfem_set_physics(hfem_ctx* ctx, const double* physicsparam, int tdep, double fc_u, double fc_q, double time);
 
 /* Solution state sol.UDG (npv x nc x ne), sol.UH (nch x nf*npf) and the time
