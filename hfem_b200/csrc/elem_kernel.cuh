@@ -160,7 +160,10 @@ struct ElemSmem {
     int pos[S::NFE * S::NPV];              // position of element node a on face fc, or -1
 };
 
-template <class S, bool TF = false>
+// TF: the contractions in 3xTF32 (precision modes 1, 3); GEN: the Lax-Friedrichs
+// / Roe stabilization tensors and Sutherland's law compiled in (the default
+// instantiation holds the constant-tau, constant-viscosity physics only).
+template <class S, bool TF = false, bool GEN = false>
 __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
     constexpr int ND = S::ND, NPV = S::NPV, NPF = S::NPF, NGV = S::NGV, NGF = S::NGF, NFE = S::NFE;
     constexpr int NCU = S::NCU, NC = S::NC, NCH = S::NCH, NDF = S::NDF, ND1 = S::ND1, N = S::N, NB = S::NB;
@@ -276,7 +279,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                     w[c].v = val;
                     w[c].d[0] = (c == k) ? 1.0 : 0.0;
                 }
-                ns_flux_dual<ND>(P, w, f, !A.inviscid, A.visc_model);
+                ns_flux_dual<ND, 1, GEN>(P, w, f, !A.inviscid, A.visc_model);
                 if (vol) {
                     const double jg = sm.jac[g];
 #pragma unroll
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                             wrl[g + NGV * ((m + 1) + ND1 * (j + NCU * k))] = -tt;
                         }
                     }
-                } else if (A.conv_stab == 0) {
+                } else if (!GEN || A.conv_stab == 0) {
                     // fhat = F(uh, q).n + tau (u - uh)   (fhatDriver.cpp:54-236), times jacf
                     const double tau = P[5];
                     const double jf = sm.jacf[g];
@@ -333,44 +336,33 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                     }
                 } else {
                     // fhat = F(uh, q).n + tau(uh) (u - uh) with the Lax-Friedrichs or
-                    // Roe tensor: the uh-derivative of the stabilization term from the
-                    // same dual pass, its u-derivative (column k of tau) by applying
-                    // tau to e_k
+                    // Roe tensor (ns_stab_point): the uh-derivative of the
+                    // stabilization term along this item's variable and column k of tau
                     const double jf = sm.jacf[g];
                     const int fc = g / NGF, q = g % NGF;
                     double* sl = fsl + fc * G::FSLP;
-                    double nlq[ND];
+                    double nlq[ND], uhv[NCU], uv[NCU], sv[NCU], sd[NCU], tcol[NCU];
 #pragma unroll
                     for (int d = 0; d < ND; d++) nlq[d] = sm.nl[g + NA * d];
-                    DD dv[NCU], st[NCU];
 #pragma unroll
-                    for (int m = 0; m < NCU; m++) dv[m] = dc<1>(ugf[g + NA * m]) - w[m];
-                    ns_stab_apply<ND, 1>(A.conv_stab, P, nlq, w, dv, st);
-                    double tcol[NCU];
-                    if (k < NCU) {
-                        DD u0[NCU], ek[NCU], ck[NCU];
-#pragma unroll
-                        for (int m = 0; m < NCU; m++) {
-                            u0[m] = dc<1>(w[m].v);
-                            ek[m] = dc<1>(m == k ? 1.0 : 0.0);
-                        }
-                        ns_stab_apply<ND, 1>(A.conv_stab, P, nlq, u0, ek, ck);
-#pragma unroll
-                        for (int j = 0; j < NCU; j++) tcol[j] = ck[j].v;
+                    for (int m = 0; m < NCU; m++) {
+                        uhv[m] = w[m].v;
+                        uv[m] = ugf[g + NA * m];
                     }
+                    ns_stab_point<ND>(A.conv_stab, P, nlq, uhv, uv, k, sv, sd, tcol);
 #pragma unroll
                     for (int j = 0; j < NCU; j++) {
                         if (k == 0) {
-                            double tt = st[j].v;
+                            double tt = sv[j];
 #pragma unroll
-                            for (int d = 0; d < ND; d++) tt += f[d * NCU + j].v * nlq[d];
+                            for (int d = 0; d < ND; d++) tt += f[d * NCU + j].v * sm.nl[g + NA * d];
                             sm.fn[g + NA * j] = tt * jf;
                         }
                         double dn = 0.0;
 #pragma unroll
-                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[0] * nlq[d];
+                        for (int d = 0; d < ND; d++) dn += f[d * NCU + j].d[0] * sm.nl[g + NA * d];
                         if (k < NCU) {
-                            sl[NGF * NCH * NC + q + NGF * (j + NCH * k)] = (dn + st[j].d[0]) * jf;
+                            sl[NGF * NCH * NC + q + NGF * (j + NCH * k)] = (dn + sd[j]) * jf;
                             sl[q + NGF * (j + NCH * k)] = tcol[j] * jf;
                         } else {
                             sl[q + NGF * (j + NCH * k)] = dn * jf;
@@ -400,8 +392,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
 #pragma unroll
                     for (int d = 0; d < ND; d++) nlq[d] = sm.nl[gg + NA * d];
                     const int ib = -bfe[fc] - 1;
-                    if (!ns_fbou_dual<ND, 1>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb, !A.inviscid,
-                                             A.conv_stab, A.visc_model)) {
+                    if (!ns_fbou_dual<ND, 1, GEN>(A.bcm[ib], P, A.bcs + (size_t)ib * NCH, nlq, w, uhd, fb,
+                                                  !A.inviscid, A.conv_stab, A.visc_model)) {
                         for (int j = 0; j < NCH; j++) fb[j] = dc<1>(0.0);
                     }
                     const double jf = sm.jacf[gg];

@@ -113,10 +113,11 @@ struct Launch {
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
     void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
     void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
-    void (*element_tf)(dim3, size_t, cudaStream_t, const ElemArgs&);   // 3xTF32 contractions
+    // [tf][gen]: 3xTF32 contractions; Lax-Friedrichs / Roe tensor or Sutherland's law compiled in
+    void (*element_v[2][2])(dim3, size_t, cudaStream_t, const ElemArgs&);
     size_t elem_smem;
     const void* elem_fn;
-    const void* elem_fn_tf;
+    const void* elem_fn_v[2][2];
     int inv_threads;
     size_t inv_smem;
     const void *q_fn, *inv_fn;
@@ -135,9 +136,9 @@ void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int*
     inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info);
 }
 
-template <class S, bool TF>
+template <class S, bool TF, bool GEN>
 void launch_element(dim3 g, size_t sm, cudaStream_t st, const ElemArgs& a) {
-    element_kernel<S, TF><<<g, NT, sm, st>>>(a);
+    element_kernel<S, TF, GEN><<<g, NT, sm, st>>>(a);
 }
 template <class S>
 void launch_getq(dim3 g, size_t sm, cudaStream_t st, const QArgs& a) { getq_kernel<S><<<g, NT, sm, st>>>(a); }
@@ -176,11 +177,17 @@ Launch make_launch() {
     L.getq = launch_getq<S>;
     L.q_fn = (const void*)getq_kernel<S>;
     L.inverse = launch_inverse<S::N>;
-    L.element = launch_element<S, false>;
-    L.element_tf = launch_element<S, true>;
+    L.element = launch_element<S, false, false>;
+    L.element_v[0][0] = launch_element<S, false, false>;
+    L.element_v[0][1] = launch_element<S, false, true>;
+    L.element_v[1][0] = launch_element<S, true, false>;
+    L.element_v[1][1] = launch_element<S, true, true>;
     L.elem_smem = sizeof(ElemSmem<S>);
-    L.elem_fn = (const void*)element_kernel<S, false>;
-    L.elem_fn_tf = (const void*)element_kernel<S, true>;
+    L.elem_fn = (const void*)element_kernel<S, false, false>;
+    L.elem_fn_v[0][0] = (const void*)element_kernel<S, false, false>;
+    L.elem_fn_v[0][1] = (const void*)element_kernel<S, false, true>;
+    L.elem_fn_v[1][0] = (const void*)element_kernel<S, true, false>;
+    L.elem_fn_v[1][1] = (const void*)element_kernel<S, true, true>;
     L.inv_threads = InvBlk<S::N>::THREADS;
     L.inv_smem = InvBlk<S::N>::SMEM;
     L.inv_fn = (const void*)inverse_blocked_kernel<S::N>;
@@ -215,7 +222,8 @@ struct hfem_ctx {
     cudaStream_t own = nullptr, stream = nullptr;
     std::string err;
     bool have_master = false, have_mesh = false, have_phys = false, have_sol = false, assembled = false;
-    int grid_elem = 0, grid_elem_tf = 0, grid_inv = 0, grid_tc = 0;
+    int grid_elem = 0, grid_inv = 0, grid_tc = 0;
+    int grid_elem_v[2][2] = {};         // per element-kernel variant [tf][gen], at most grid_elem
     // element-wise state arriving in pieces (hfem_assemble_host): the element
     // kernel of piece k waits for chunk_ev[k]
     cudaStream_t copy_stream = nullptr;
@@ -592,9 +600,10 @@ int ready(hfem_ctx* c) {
 // sequence can be captured into a CUDA graph).  Buffers must exist.
 int enqueue_assembly(hfem_ctx* c, bool matrix) {
     int rc;
-    const bool tf = c->precision == 1 || c->precision == 3;
-    const dim3 ge(tf ? c->grid_elem_tf : c->grid_elem);
-    auto element = tf ? c->L->element_tf : c->L->element;
+    const int tf = (c->precision == 1 || c->precision == 3) ? 1 : 0;
+    const int gen = (c->conv_stab != 0 || c->visc_model != 0) ? 1 : 0;
+    const dim3 ge(c->grid_elem_v[tf][gen]);
+    auto element = c->L->element_v[tf][gen];
     {
         Timed t(c, "element");
         if (c->pending_chunks > 0) {
@@ -1570,15 +1579,20 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
     c->stream = c->own;
     const Launch& L = *c->L;
     cudaFuncSetAttribute(L.elem_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
-    cudaFuncSetAttribute(L.elem_fn_tf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
+    for (int t = 0; t < 2; t++)
+        for (int g = 0; g < 2; g++)
+            cudaFuncSetAttribute(L.elem_fn_v[t][g], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.elem_smem);
     cudaFuncSetAttribute(L.q_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.q_smem);
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn, NT, L.elem_smem);
     c->grid_elem = std::max(1, std::min(d.ne, sms(device) * std::max(occ, 1)));
-    occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn_tf, NT, L.elem_smem);
-    // the workspace has grid_elem slots
-    c->grid_elem_tf = std::max(1, std::min(c->grid_elem, sms(device) * std::max(occ, 1)));
+    // the workspace has grid_elem slots: no variant runs more CTAs
+    for (int t = 0; t < 2; t++)
+        for (int g = 0; g < 2; g++) {
+            occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.elem_fn_v[t][g], NT, L.elem_smem);
+            c->grid_elem_v[t][g] = std::max(1, std::min(c->grid_elem, sms(device) * std::max(occ, 1)));
+        }
     cudaFuncSetAttribute(L.g1.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g1.smem);
     cudaFuncSetAttribute(L.g2.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.g2.smem);
     cudaFuncSetAttribute(L.tc_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.tc_smem);

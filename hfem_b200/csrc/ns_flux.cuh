@@ -115,8 +115,9 @@ __device__ __forceinline__ Dual<M> ns_sutherland(const double* __restrict__ para
 // partial derivatives (M = nc for the full Jacobian, 1 for one column of it).
 // viscous == false: the Euler flux (flux_euler2dNEW.c / flux_euler3dNEW.c), the
 // same expression without the stress and heat terms.  visc_model: 0 mu = 1,
-// 1 Sutherland's law (ns_sutherland).
-template <int ND, int M>
+// 1 Sutherland's law (ns_sutherland); GEN false compiles the constant-viscosity
+// flux alone.
+template <int ND, int M, bool GEN = false>
 __device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, const Dual<M>* w, Dual<M>* f,
                                              bool viscous = true, int visc_model = 0) {
     constexpr int NCU = ND + 2;
@@ -143,8 +144,11 @@ __device__ __forceinline__ void ns_flux_dual(const double* __restrict__ param, c
 #pragma unroll
     for (int i = 1; i < ND; i++) div = div + dv[i][i];
     const double kappa = gam / (Re * Pr);
-    const bool vm = viscous && visc_model != 0;
-    const D mu = vm ? ns_sutherland<ND, M>(param, w) : dc<NC>(1.0);
+    const bool vm = GEN && viscous && visc_model != 0;
+    D mu = dc<NC>(1.0);
+    if constexpr (GEN) {
+        if (vm) mu = ns_sutherland<ND, M>(param, w);
+    }
 #pragma unroll
     for (int d = 0; d < ND; d++) {
         f[d * NCU + 0] = w[1 + d];
@@ -324,6 +328,40 @@ __device__ __forceinline__ void ns_stab_apply(int method, const double* __restri
     }
 }
 
+// The stabilization term of fhat at one face point for the element kernel's
+// flux pass: sv = tau(uh)(u - uh), sd = its derivative along uh_k (k < ncu;
+// 0 otherwise), tcol = column k of tau (k < ncu).
+template <int ND>
+__device__ __forceinline__ void ns_stab_point(int method, const double* __restrict__ param, const double* nl,
+                                           const double* uh, const double* u, int k, double* sv, double* sd,
+                                           double* tcol) {
+    constexpr int NCU = ND + 2;
+    using DD = Dual<1>;
+    DD uhd[NCU], dv[NCU], st[NCU];
+#pragma unroll
+    for (int m = 0; m < NCU; m++) {
+        uhd[m].v = uh[m];
+        uhd[m].d[0] = (m == k) ? 1.0 : 0.0;
+        dv[m] = dc<1>(u[m]) - uhd[m];
+    }
+    ns_stab_apply<ND, 1>(method, param, nl, uhd, dv, st);
+#pragma unroll
+    for (int j = 0; j < NCU; j++) {
+        sv[j] = st[j].v;
+        sd[j] = st[j].d[0];
+    }
+    if (k < NCU) {
+#pragma unroll
+        for (int m = 0; m < NCU; m++) {
+            uhd[m] = dc<1>(uh[m]);
+            dv[m] = dc<1>(m == k ? 1.0 : 0.0);
+        }
+        ns_stab_apply<ND, 1>(method, param, nl, uhd, dv, st);
+#pragma unroll
+        for (int j = 0; j < NCU; j++) tcol[j] = st[j].v;
+    }
+}
+
 // Boundary flux fb(u, q, uh) of the NS boundary conditions at one point
 // (application/FM/fbou.cpp on a fixed mesh), in dual numbers so that one pass
 // per differentiated variable gives fb and its derivative:
@@ -334,7 +372,7 @@ __device__ __forceinline__ void ns_stab_apply(int method, const double* __restri
 //   7 slip wall: rho - rho_hat, m - (m.n) n - m_hat, E - E_hat.
 // w holds (u, q) (NC entries), uh the trace state (NCH); returns false for a
 // type without a restatement.
-template <int ND, int M>
+template <int ND, int M, bool GEN = false>
 __device__ __forceinline__ bool ns_fbou_dual(int bn, const double* __restrict__ param, const double* ui,
                                              const double* nl, const Dual<M>* w, const Dual<M>* uh, Dual<M>* fb,
                                              bool viscous = true, int conv_stab = 0, int visc_model = 0) {
@@ -353,12 +391,17 @@ __device__ __forceinline__ bool ns_fbou_dual(int bn, const double* __restrict__ 
         for (int k = 0; k < NCU; k++) wf[k] = uh[k];
 #pragma unroll
         for (int k = NCU; k < NC; k++) wf[k] = w[k];
-        ns_flux_dual<ND, M>(param, wf, f, viscous, visc_model);
-        Dual<M> du[NCU], st[NCU];
+        ns_flux_dual<ND, M, GEN>(param, wf, f, viscous, visc_model);
+        Dual<M> t;
+        if (!GEN || conv_stab == 0) {
+            t = tau * (w[ND + 1] - uh[ND + 1]);
+        } else {
+            Dual<M> du[NCU], st[NCU];
 #pragma unroll
-        for (int k = 0; k < NCU; k++) du[k] = w[k] - uh[k];
-        ns_stab_apply<ND, M>(conv_stab, param, nl, uh, du, st);
-        Dual<M> t = st[ND + 1];
+            for (int k = 0; k < NCU; k++) du[k] = w[k] - uh[k];
+            ns_stab_apply<ND, M>(conv_stab, param, nl, uh, du, st);
+            t = st[ND + 1];
+        }
 #pragma unroll
         for (int d = 0; d < ND; d++) t = t + nl[d] * f[d * NCU + ND + 1];
         fb[ND + 1] = t;
