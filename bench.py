@@ -94,6 +94,12 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # the timed region starts once the sampler has written its first line
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.05)
+        self.skip = 1 if os.path.getsize(self.path) > 0 else 0
 
     def stop(self):
         if self.proc is None:
@@ -106,7 +112,8 @@ class ClockSampler:
         self.fh.close()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        # the line written before the timed region is not one of its samples
+        for line in open(self.path).readlines()[getattr(self, "skip", 0):]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -621,7 +628,7 @@ def run_batched_task(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hfem", choices=["hfem", "reference"])
     ap.add_argument("--workload", default="ns3d_p3_48k", choices=sorted(WORKLOADS))
