@@ -293,7 +293,9 @@ int hfem_fp64_peak(int device, double* tflops);
  * and, for a bounded mesh, bf (ne x nfe, element-major, < 0 on boundary
  * -(ib + 1)), bcm (condition types 1, 2, 5, 6 or 7 per boundary) and bcs
  * (nch states per boundary) as hfem_set_boundary takes them (bf = NULL: no
- * boundary faces); appname 1 Navier-Stokes, 0 Euler -- and all outputs, per
+ * boundary faces); appname 1 Navier-Stokes, 0 Euler (constant tau =
+ * physicsparam[5] and constant viscosity: the models of hfem_set_models are
+ * not taken here) -- and all outputs, per
  * element: D (n^2; receives D^-1), DinvF (n*nb), K (nb*n), H (nb^2,
  * condensed), DinvRu (n), Rh (nb, condensed), Rh_uncondensed (nb), ru2
  * (||Ru||^2 before condensation), info (0, or 1 + pivot step of a singular D).
