@@ -27,6 +27,7 @@
 #include "elem_kernels.cuh"
 #include "schur_kernels.cuh"
 #include "tf32x3.cuh"
+#include "bulk_copy.cuh"
 
 namespace hfem {
 
@@ -57,8 +58,15 @@ struct EK {
     // shared-memory union: M^-1 C and M^-1 E, then either the q/flux phase
     // scratch or the B operand of the GEMM being run
     static constexpr int CME = S::NPV * S::NPV * S::ND + S::NPV * S::NDF * S::ND;
-    static constexpr int QPH = S::NPV * S::NPV + S::NGV * S::NC + S::NA * (S::NC + S::NCH) + S::NPV * S::NC +
-                               S::NDF * S::NCH + S::NPV * S::NCU;
+    // the q / flux phase region: M, point states, then u, uhe and the source,
+    // u and the source at even offsets (16-byte bulk copies land there)
+    static constexpr int O_UG = S::NPV * S::NPV;
+    static constexpr int O_UGF = O_UG + S::NGV * S::NC;
+    static constexpr int O_UHG = O_UGF + S::NA * S::NC;
+    static constexpr int O_U = (O_UHG + S::NA * S::NCH + 1) / 2 * 2;
+    static constexpr int O_UHE = O_U + S::NPV * S::NC;
+    static constexpr int O_SHU = (O_UHE + S::NDF * S::NCH + 1) / 2 * 2;
+    static constexpr int QPH = O_SHU + S::NPV * S::NCU;
     static constexpr int GPH = BDF > BKH + FSLP ? BDF : BKH + FSLP;
     static constexpr int UN = CME + (QPH > GPH ? QPH : GPH);
     // global workspace per CTA slot (doubles): wrl, the interior and boundary
@@ -68,8 +76,9 @@ struct EK {
     static constexpr int W_FNB = S::NA * S::NCH;
     static constexpr int W_Y = S::NPV * S::NGV * S::NCU * S::NC;
     static constexpr int WS = W_WRL + 2 * W_FSL + W_FNB + W_Y;
-    static_assert(CME % 2 == 0 && BKH % 2 == 0 && W_WRL % 2 == 0 && WS % 2 == 0,
+    static_assert(CME % 2 == 0 && BKH % 2 == 0 && W_WRL % 2 == 0 && WS % 2 == 0 && W_FSL % 2 == 0,
                   "16-byte alignment of the staged face slices");
+    static_assert(O_U % 2 == 0 && O_SHU % 2 == 0, "16-byte alignment of the bulk-copied element inputs");
 };
 
 // Cholesky solves L L' x = b for one column held in registers, in the axpy
@@ -153,6 +162,7 @@ struct ElemSmem {
     double sfc[S::NGF * S::NPF];           // face basis values shapfc(kk, q) = shapft[q + NGF*kk]
     double red[NT / 32];
     double rdg[S::NPV];                    // 1 / L(j, j) of the Cholesky factor of M
+    uint64_t bar_in, bar_sl;               // bulk-copy barriers: element inputs, face slices
     alignas(16) double un[EK<S>::UN];
     int perm[S::NDF];
     int inc_n[S::NPV];
@@ -187,12 +197,12 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
     double* Em = Cm + NPV * NPV * ND;              // [b + NPV (f + NDF d)]
     double* ph = sm.un + G::CME;
     double* M = ph;                                // q / flux phase
-    double* ug = M + NPV * NPV;
-    double* ugf = ug + NGV * NC;
-    double* uhg = ugf + NA * NC;
-    double* u = uhg + NA * NCH;
-    double* uhe = u + NPV * NC;
-    double* shu = uhe + NDF * NCH;
+    double* ug = ph + G::O_UG;
+    double* ugf = ph + G::O_UGF;
+    double* uhg = ph + G::O_UHG;
+    double* u = ph + G::O_U;
+    double* uhe = ph + G::O_UHE;
+    double* shu = ph + G::O_SHU;
     double* Bs = ph;                               // GEMM phases
 
     for (int t = tid; t < G::LDAV * G::KV; t += NT) {
@@ -205,6 +215,11 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
     }
     for (int t = tid; t < NGF * NPF; t += NT) sm.sfc[t] = T.shapft[t];
     for (int t = tid; t < NDF; t += NT) sm.perm[t] = T.perm[t];
+    if (tid == 0) {
+        bulk_bar_init(&sm.bar_in);
+        bulk_bar_init(&sm.bar_sl);
+    }
+    uint32_t ph_in = 0, ph_sl = 0;                 // barrier phases (the same in every thread)
     __syncthreads();
     for (int i = tid; i < NPV; i += NT) {
         int c = 0;
@@ -220,16 +235,36 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
     }
 
     for (int e = A.e_begin + blockIdx.x; e < A.ne; e += gridDim.x) {
+        bulk_proxy_fence();
         __syncthreads();
         const double* xg = A.dgnodes + (size_t)e * NPV * ND;
         const double* ugl = A.udg + (size_t)e * NPV * NC;
         const double* shg = A.sh + (size_t)e * NPV * NC;
-        for (int t = tid; t < NPV * ND; t += NT) sm.x[t] = xg[t];
-        for (int t = tid; t < NPV * NC; t += NT) u[t] = ugl[t];
-        for (int t = tid; t < NPV * NCU; t += NT) shu[t] = shg[t];
+        // the element's contiguous inputs (coordinates, u with q, source) by the
+        // TMA engine's bulk copies while the threads gather uh through elcon;
+        // plain loads when a caller's array is not 16-byte aligned
+        const bool bulk = bulk_aligned(xg) && bulk_aligned(ugl) && bulk_aligned(shg);
+        if (bulk) {
+            if (tid == 0) {
+                constexpr uint32_t BX = NPV * ND * 8, BU = NPV * NC * 8, BS = NPV * NCU * 8;
+                static_assert(BX % 16 == 0 && BU % 16 == 0 && BS % 16 == 0, "bulk copies move 16-byte multiples");
+                bulk_bar_expect(&sm.bar_in, BX + BU + BS);
+                bulk_load(sm.x, xg, BX, &sm.bar_in);
+                bulk_load(u, ugl, BU, &sm.bar_in);
+                bulk_load(shu, shg, BS, &sm.bar_in);
+            }
+        } else {
+            for (int t = tid; t < NPV * ND; t += NT) sm.x[t] = xg[t];
+            for (int t = tid; t < NPV * NC; t += NT) u[t] = ugl[t];
+            for (int t = tid; t < NPV * NCU; t += NT) shu[t] = shg[t];
+        }
         for (int t = tid; t < NDF * NCH; t += NT) {
             const int fdof = t / NCH, c = t % NCH;
             uhe[fdof + NDF * c] = A.uh[(size_t)A.elcon[(size_t)e * NDF + fdof] * NCH + c];
+        }
+        if (bulk) {
+            if (!bulk_bar_wait(&sm.bar_in, ph_in) && tid == 0 && A.err) atomicExch(A.err, 2);
+            ph_in ^= 1u;
         }
         __syncthreads();
         geometry<S>(T, sm.x, sm.jac, sm.Xx, sm.jacf, sm.nl);
@@ -704,14 +739,17 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
         // they are added to the element equations of the face's nodes
         // (D += P K, F += P H) by reductions in L2, face after face
         auto face_rows = [&](int fc, const double* slices, bool store, bool liftD, bool liftF) {
+            bulk_proxy_fence();
             __syncthreads();
             double* BK = Bs;                              // KFD x NKP  (ld LDBK)
             double* BH = Bs + G::LDBK * G::NKP;           // KFD x NHP  (ld LDBK)
             double* sfu = Bs + G::BKH;                    // the face's slices
             double* sfuh = sfu + NGF * NCH * NC;
-            // the slices arrive by 16-byte asynchronous copies while B is built
-            for (int t = tid; t < G::FSLP / 2; t += NT) cp_async16z(sfu + 2 * t, slices + 2 * t, true);
-            cp_async_commit();
+            // the slices arrive by one bulk copy (TMA engine) while B is built
+            if (tid == 0) {
+                bulk_bar_expect(&sm.bar_sl, G::FSLP * 8);
+                bulk_load(sfu, slices, G::FSLP * 8, &sm.bar_sl);
+            }
             // d' = 0 rows (the face basis at the face's nodes) and zero padding
             // directly; rows d' > 0 = shapfc (M^-1 C | M^-1 E)(face nodes) on the
             // tensor cores
@@ -742,7 +780,8 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                         bput<TF>(&BH[(q + NGF * (d + 1)) + G::LDBK * f2], -v);
                     }
                 });
-            cp_async_wait<0>();
+            if (!bulk_bar_wait(&sm.bar_sl, ph_sl) && tid == 0 && A.err) atomicExch(A.err, 2);
+            ph_sl ^= 1u;
             __syncthreads();
             constexpr int MTK = (NPF * NCH * NCU + 7) / 8;
             constexpr int KH0 = (NGF + 3) / 4;            // k-steps holding d' = 0 rows

@@ -63,6 +63,7 @@ struct ElemArgs {
     const int* bcm;
     const double* bcs;
     int inviscid;               // 1: Euler flux (app.appname 0)
+    int* err = nullptr;         // set to 2 when a bulk-copy wait expires (NULL: not recorded)
     int conv_stab = 0;          // app.convStabMethod: 0 constant tau, 1 Lax-Friedrichs, 2 Roe
     int visc_model = 0;         // app.viscosityModel: 0 constant, 1 Sutherland's law
     int e_begin = 0;            // element range [e_begin, ne) of this launch

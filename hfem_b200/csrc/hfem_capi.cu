@@ -245,7 +245,7 @@ struct hfem_ctx {
     int appname = 1;            // app.appname: 1 Navier-Stokes, 0 Euler
     int conv_stab = 0;          // app.convStabMethod: 0 constant tau, 1 Lax-Friedrichs, 2 Roe
     int visc_model = 0;         // app.viscosityModel: 0 constant, 1 Sutherland's law
-    int* tc_err = nullptr;
+    int* tc_err = nullptr;              // 1: a tcgen05 MMA wait expired; 2: an element bulk-copy wait expired
     double* rn_part = nullptr;
     // master tables
     double *shapvt = nullptr, *shapvg = nullptr, *svsv = nullptr, *shapft = nullptr, *shapfg = nullptr, *sfsf = nullptr;
@@ -532,6 +532,7 @@ ElemArgs elem_args(hfem_ctx* c) {
     a.inviscid = c->appname == 0;
     a.conv_stab = c->conv_stab;
     a.visc_model = c->visc_model;
+    a.err = c->tc_err;
     a.bf = c->bf;
     a.bcm = c->bcm;
     a.bcs = c->bcs;
@@ -694,14 +695,13 @@ int finish_assembly(hfem_ctx* c, bool matrix, double* rnorm_out) {
         CK(cudaStreamSynchronize(c->stream));
         for (int e = 0; e < c->dims.ne; e++)
             if (info[e]) return fail(c, HFEM_E_SINGULAR, "element %d: singular local matrix (pivot %d)", e, info[e]);
-        if (c->precision == 1) {
-            int terr = 0;
-            CK(cudaMemcpyAsync(&terr, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaStreamSynchronize(c->stream));
-            if (terr) return fail(c, HFEM_E_CUDA, "tensor-core Schur kernel: an MMA completion wait expired");
-        }
-        c->assembled = true;
     }
+    int terr = 0;
+    CK(cudaMemcpyAsync(&terr, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (terr == 1) return fail(c, HFEM_E_CUDA, "tensor-core Schur kernel: an MMA completion wait expired");
+    if (terr == 2) return fail(c, HFEM_E_CUDA, "element kernel: a bulk-copy completion wait expired");
+    if (matrix) c->assembled = true;
     double rn = 0.0;
     CK(cudaMemcpyAsync(&rn, c->rnorm, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
