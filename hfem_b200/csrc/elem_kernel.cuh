@@ -24,6 +24,7 @@
 // definition, mkmasterelement.m:113-115) in factored form.
 #pragma once
 #include <cuda_runtime.h>
+#include <type_traits>
 #include "elem_kernels.cuh"
 #include "schur_kernels.cuh"
 #include "tf32x3.cuh"
@@ -128,7 +129,11 @@ __device__ __forceinline__ void basis_ce_gemm(const double* a, int lda, const in
             af[mt][ks] = (r < MR && kk < KD) ? a[r + lda * kk] : 0.0;
         }
     }
-    for (int nt = warp; nt < NNT; nt += NW) {
+    // the warp's n-tiles unrolled, so their DMMA chains overlap
+#pragma unroll
+    for (int it = 0; it < (NNT + NW - 1) / NW; it++) {
+        const int nt = warp + it * NW;
+        if (nt >= NNT) break;
         const int n = 8 * nt + gr;
         double acc[MT][2];
 #pragma unroll
@@ -750,25 +755,18 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                 bulk_bar_expect(&sm.bar_sl, G::FSLP * 8);
                 bulk_load(sfu, slices, G::FSLP * 8, &sm.bar_sl);
             }
-            // d' = 0 rows (the face basis at the face's nodes) and zero padding
-            // directly; rows d' > 0 = shapfc (M^-1 C | M^-1 E)(face nodes) on the
-            // tensor cores
-            for (int t = tid; t < G::KFD * G::NKP; t += NT) {
-                const int k = t % G::KFD, a = t / G::KFD, q = k % NGF;
-                if (a < NPV && k >= NGF && k < NGF * ND1) continue;
-                double x = 0.0;
-                if (a < NPV && k < NGF) {
-                    const int p = sm.pos[fc * NPV + a];
-                    x = (p >= 0) ? sm.sfc[q + NGF * p] : 0.0;
+            // d' = 0 rows (the face basis at the face's nodes) directly (the zero
+            // padding is written once per element, before the first face); rows
+            // d' > 0 = shapfc (M^-1 C | M^-1 E)(face nodes) on the tensor cores
+            for (int t = tid; t < NGF * (NPV + NDF); t += NT) {
+                const int q = t % NGF, c = t / NGF;
+                if (c < NPV) {
+                    const int p = sm.pos[fc * NPV + c];
+                    bput<TF>(&BK[q + G::LDBK * c], (p >= 0) ? sm.sfc[q + NGF * p] : 0.0);
+                } else {
+                    const int f2 = c - NPV;
+                    bput<TF>(&BH[q + G::LDBK * f2], (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0);
                 }
-                bput<TF>(&BK[k + G::LDBK * a], x);
-            }
-            for (int t = tid; t < G::KFD * G::NHP; t += NT) {
-                const int k = t % G::KFD, f2 = t / G::KFD, q = k % NGF;
-                if (f2 < NDF && k >= NGF && k < NGF * ND1) continue;
-                double x = 0.0;
-                if (f2 < NDF && k < NGF) x = (f2 / NPF == fc) ? sm.sfc[q + NGF * (f2 % NPF)] : 0.0;
-                bput<TF>(&BH[k + G::LDBK * f2], x);
             }
             basis_ce_gemm<NGF, NPF, NPV, NPV * ND + NDF * ND, NT / 32>(
                 sm.sfc, NGF, sm.perm + fc * NPF, Cm, [&](int q, int n, double v) {
@@ -845,33 +843,42 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
                                 if (liftD) atomicAdd(&De[inode[u] + NPV * (j + NCU * (a + NPV * m))], acc[u][b][h]);
                             }
                         }
-                double acch[2][G::NTH][2];
+                // H in two column halves: half the accumulators live at a time
+                auto hpart = [&](auto b0c, auto nbc) {
+                    constexpr int B0 = decltype(b0c)::value, NBN = decltype(nbc)::value;
+                    double acch[2][NBN][2];
 #pragma unroll
-                for (int u = 0; u < 2; u++)
+                    for (int u = 0; u < 2; u++)
 #pragma unroll
-                    for (int b = 0; b < G::NTH; b++) acch[u][b][0] = acch[u][b][1] = 0.0;
+                        for (int b = 0; b < NBN; b++) acch[u][b][0] = acch[u][b][1] = 0.0;
 #pragma unroll
-                for (int ks = 0; ks < G::KFD / 4; ks++)
+                    for (int ks = 0; ks < G::KFD / 4; ks++)
 #pragma unroll
-                    for (int b = 0; b < G::NTH; b++) {
-                        if (4 * ks + 3 < NGF && (b < blo || b > bhi)) continue;
-                        const double bv = BH[(4 * ks + gc) + G::LDBK * (8 * b + gr)];
-                        dmma8x8x4(acch[0][b][0], acch[0][b][1], ks < KH0 ? aH0[0][ks < KH0 ? ks : 0] : aK[0][ks], bv);
-                        dmma8x8x4(acch[1][b][0], acch[1][b][1], ks < KH0 ? aH0[1][ks < KH0 ? ks : 0] : aK[1][ks], bv);
-                    }
-#pragma unroll
-                for (int u = 0; u < 2; u++)
-#pragma unroll
-                    for (int b = 0; b < G::NTH; b++)
-#pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            const int f2 = 8 * b + 2 * gc + h;
-                            if (rv[u] && f2 < NDF) {
-                                const int j = jj[u], ip = ipp[u], m = mm[u];
-                                if (store) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[u][b][h];
-                                if (liftF) atomicAdd(&Fe[inode[u] + NPV * (j + NCU * (m + NCH * f2))], acch[u][b][h]);
-                            }
+                        for (int bb = 0; bb < NBN; bb++) {
+                            const int b = B0 + bb;
+                            if (4 * ks + 3 < NGF && (b < blo || b > bhi)) continue;
+                            const double bv = BH[(4 * ks + gc) + G::LDBK * (8 * b + gr)];
+                            dmma8x8x4(acch[0][bb][0], acch[0][bb][1], ks < KH0 ? aH0[0][ks < KH0 ? ks : 0] : aK[0][ks], bv);
+                            dmma8x8x4(acch[1][bb][0], acch[1][bb][1], ks < KH0 ? aH0[1][ks < KH0 ? ks : 0] : aK[1][ks], bv);
                         }
+#pragma unroll
+                    for (int u = 0; u < 2; u++)
+#pragma unroll
+                        for (int bb = 0; bb < NBN; bb++)
+#pragma unroll
+                            for (int h = 0; h < 2; h++) {
+                                const int f2 = 8 * (B0 + bb) + 2 * gc + h;
+                                if (rv[u] && f2 < NDF) {
+                                    const int j = jj[u], ip = ipp[u], m = mm[u];
+                                    if (store) He[j + NCH * (fc * NPF + ip) + (size_t)NB * (m + NCH * f2)] = acch[u][bb][h];
+                                    if (liftF) atomicAdd(&Fe[inode[u] + NPV * (j + NCU * (m + NCH * f2))], acch[u][bb][h]);
+                                }
+                            }
+                };
+                constexpr int NTH1 = (G::NTH + 1) / 2;
+                hpart(std::integral_constant<int, 0>{}, std::integral_constant<int, NTH1>{});
+                if constexpr (G::NTH - NTH1 > 0)
+                    hpart(std::integral_constant<int, NTH1>{}, std::integral_constant<int, G::NTH - NTH1>{});
             }
             } else {
             // 3xTF32: the m-tile pair as one m16 tile, k-steps of 8
@@ -979,6 +986,20 @@ __global__ void __launch_bounds__(NT, 2) element_kernel(ElemArgs A) {
             }
             }
         };
+        // zero padding of the face B operands (rows past NGF ND1, columns past
+        // npv and ndf), the same for every face
+        {
+            double* BK = Bs;
+            double* BH = Bs + G::LDBK * G::NKP;
+            for (int t = tid; t < G::KFD * G::NKP; t += NT) {
+                const int k = t % G::KFD, a = t / G::KFD;
+                if (k >= NGF * ND1 || a >= NPV) bput<TF>(&BK[k + G::LDBK * a], 0.0);
+            }
+            for (int t = tid; t < G::KFD * G::NHP; t += NT) {
+                const int k = t % G::KFD, f2 = t / G::KFD;
+                if (k >= NGF * ND1 || f2 >= NDF) bput<TF>(&BH[k + G::LDBK * f2], 0.0);
+            }
+        }
         for (int fc = 0; fc < NFE; fc++) {
             const bool bnd = bfe && bfe[fc] < 0;
             // interior faces: the trace rows, lifted into D; boundary faces: fhat
