@@ -74,6 +74,12 @@ def newton_fixtures():
         np.savez_compressed(os.path.join(HERE, "ns2d_p2_n4_newton.npz"), rnorm_hist=ref["rnorm_hist"],
                             gmres_iters=ref["gmres_iters"], udg=ref["udg"], uh=ref["uh"])
         print("newton", ref["rnorm_hist"], ref["gmres_iters"])
+    # the Roe tensor and Sutherland's law on a walled channel, two Newton iterations
+    prob = with_models(ns2d_channel(n=4, porder=2), 2, 1)
+    ref = run_reference(prob, mode="newton", newton=dict(maxiter=2, precond=2, restart=50, tol=1e-10))
+    np.savez_compressed(os.path.join(HERE, "ns2d_channel_roe_suth_p2_n4_newton.npz"), rnorm_hist=ref["rnorm_hist"],
+                        gmres_iters=ref["gmres_iters"], udg=ref["udg"], uh=ref["uh"])
+    print("newton roe+sutherland channel", ref["rnorm_hist"], ref["gmres_iters"])
     # the full-size 2D workload: 2,048 elements, one Newton step
     prob = ns2d_vortex(n=32, porder=2)
     ref = run_reference(prob, mode="newton", newton=dict(maxiter=1, precond=2, restart=50, tol=1e-10))

@@ -8,7 +8,10 @@ present; the binary travels with the repository).  Its Newton residual history
 and final state must match the reference's own run (oracle/_ref/hfem_ref,
 stored in tests/golden) within 1e-12 of the first residual / 1e-12 relative:
   * the 4 x 4 x 2 vortex (2D, p = 2), two Newton iterations;
-  * the full-size 2D workload (32 x 32 x 2 = 2,048 triangles, p = 2), one step.
+  * the full-size 2D workload (32 x 32 x 2 = 2,048 triangles, p = 2), one step;
+  * a walled channel with the Roe stabilization tensor and Sutherland's law
+    (app.convStabMethod 2, app.viscosityModel 1, read by the reference's own
+    set-up and handed to the library by the shim), two iterations.
 """
 import os
 import subprocess
@@ -17,7 +20,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from hfem_b200.gen.problem import ns2d_vortex
+from hfem_b200.gen.problem import ns2d_channel, ns2d_vortex, with_models
 from hfem_b200.gen.refio import write_inputs
 
 pytestmark = pytest.mark.gpu
@@ -64,3 +67,13 @@ def test_reference_newton_driver_on_gpu_full_size_2d():
         p = np.random.default_rng(20261203).standard_normal((8, v.size))
         d = np.max(np.abs(p @ v - g[k + "_proj"]))
         assert d <= 1e-12 * g[k + "_absmax"][0] * np.sqrt(v.size), (k, d)
+
+
+def test_reference_newton_driver_on_gpu_roe_sutherland_channel():
+    g = dict(np.load(os.path.join(GOLDEN, "ns2d_channel_roe_suth_p2_n4_newton.npz")))
+    hist, udg, uh = run_driver(with_models(ns2d_channel(n=4, porder=2), 2, 1), 2)
+    r0 = g["rnorm_hist"][0]
+    print("drop-in driver, Roe + Sutherland channel:", hist, "reference:", g["rnorm_hist"])
+    assert hist.shape == g["rnorm_hist"].shape
+    assert np.max(np.abs(hist - g["rnorm_hist"])) <= 1e-12 * r0
+    assert rel(udg, g["udg"].ravel()) < 1e-12 and rel(uh, g["uh"].ravel()) < 1e-12

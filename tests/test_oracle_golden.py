@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from hfem_b200.gen.problem import as_euler, ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier, with_models
-from oracle import Oracle
+from oracle import Oracle, newton_solve
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = {
@@ -144,3 +144,17 @@ def test_newton_step_full_size_2d_matches_reference():
     assert np.max(np.abs(hist - g["rnorm_hist"])) <= 1e-12 * g["rnorm_hist"][0]
     for k, v in (("udg", udg), ("uh", uh)):
         assert np.max(np.abs(projections(k, v) - g[k + "_proj"])) <= 1e-12 * g[k + "_absmax"][0] * np.sqrt(v.size)
+
+
+def test_newton_with_roe_and_sutherland_matches_reference():
+    """The reference's Newton driver with the Roe tensor and Sutherland's law on
+    a walled channel (two iterations, line search as solveNonlinearProblem)."""
+    g = dict(np.load(os.path.join(HERE, "ns2d_channel_roe_suth_p2_n4_newton.npz")))
+    prob = with_models(ns2d_channel(n=4, porder=2), 2, 1)
+    o = Oracle(prob)
+    udg = o.getq(prob.udg, prob.uh)
+    udg, uh, _, hist = newton_solve(o, udg, prob.uh.copy(), prob.sh, 1e-10, 2)
+    r0 = g["rnorm_hist"][0]
+    assert len(hist) == len(g["rnorm_hist"])
+    assert np.max(np.abs(np.array(hist) - g["rnorm_hist"])) <= 1e-12 * r0
+    assert rel(udg.ravel(), g["udg"].ravel()) < 1e-12 and rel(uh.ravel(), g["uh"].ravel()) < 1e-12
