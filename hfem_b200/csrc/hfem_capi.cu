@@ -111,7 +111,7 @@ struct Launch {
     size_t ws;                  // workspace doubles per CTA slot (element_kernel)
     size_t q_smem;
     void (*getq)(dim3, size_t, cudaStream_t, const QArgs&);
-    void (*inverse)(dim3, cudaStream_t, int, double*, double*, int*);
+    void (*inverse)(dim3, cudaStream_t, int, double*, const double*, double*, int*);
     void (*element)(dim3, size_t, cudaStream_t, const ElemArgs&);
     // [tf][gen]: 3xTF32 contractions; Lax-Friedrichs / Roe tensor or Sutherland's law compiled in
     void (*element_v[2][2])(dim3, size_t, cudaStream_t, const ElemArgs&);
@@ -132,8 +132,8 @@ struct Launch {
 };
 
 template <int N>
-void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, double* Ru, int* info) {
-    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, info);
+void launch_inverse(dim3 g, cudaStream_t st, int ne, double* D, const double* Ru, double* RuOut, int* info) {
+    inverse_blocked_kernel<N><<<g, InvBlk<N>::THREADS, InvBlk<N>::SMEM, st>>>(ne, D, Ru, RuOut, info);
 }
 
 template <class S, bool TF, bool GEN>
@@ -263,6 +263,7 @@ struct hfem_ctx {
     double *udg = nullptr, *uh = nullptr, *sh = nullptr;
     // assembly outputs and workspace
     double *D = nullptr, *F = nullptr, *K = nullptr, *H = nullptr, *Ru = nullptr, *Rh = nullptr, *Ro = nullptr;
+    double* DinvRu = nullptr;           // D^-1 Ru of the last matrix pass (the update's input)
     double* DinvF = nullptr;
     double *ru2 = nullptr, *Hg = nullptr, *Rg = nullptr, *Rr = nullptr, *rnorm = nullptr, *ws = nullptr;
     int* info = nullptr;
@@ -516,6 +517,7 @@ int ensure_assembly_buffers(hfem_ctx* c) {
     if ((rc = dalloc(c, &c->K, ne * nb * n))) return rc;
     if ((rc = dalloc(c, &c->H, ne * nb * nb))) return rc;
     if ((rc = dalloc(c, &c->Ru, ne * n))) return rc;
+    if ((rc = dalloc(c, &c->DinvRu, ne * n))) return rc;
     if ((rc = dalloc(c, &c->Rh, ne * nb))) return rc;
     if ((rc = dalloc(c, &c->Ro, ne * nb))) return rc;
     if ((rc = dalloc(c, &c->ru2, ne))) return rc;
@@ -628,7 +630,9 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
         const int ne = c->dims.ne, n = c->n, nb = c->nb;
         {
             Timed t(c, "inverse");
-            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->info);
+            // D^-1 Ru to its own buffer: residual-only passes (a Newton line
+            // search) overwrite Ru while the update still needs D^-1 Ru
+            c->L->inverse(dim3(c->grid_inv), c->stream, ne, c->D, c->Ru, c->DinvRu, c->info);
             if ((rc = check_launch(c, "inverse"))) return rc;
         }
         if (c->precision != 1 && c->g1_sel < 0 && c->g2_sel < 0) {
@@ -664,7 +668,7 @@ int enqueue_assembly(hfem_ctx* c, bool matrix) {
         {
             Timed t(c, "gemv_Rh");
             batched_dgemv_kernel<<<sms(c->device) * 8, 256, 0, c->stream>>>(ne, nb, n, -1.0, c->K, (long long)nb * n,
-                                                                           c->Ru, n, c->Rh, nb);
+                                                                           c->DinvRu, n, c->Rh, nb);
             if ((rc = check_launch(c, "gemv_Rh"))) return rc;
         }
         {
@@ -728,7 +732,7 @@ int launch_getq(hfem_ctx* c, const double* duh, double alpha) {
     q.sh = c->sh;
     q.fc_q = c->fc_q;
     q.ne = c->dims.ne;
-    q.DinvRu = duh ? c->Ru : nullptr;
+    q.DinvRu = duh ? c->DinvRu : nullptr;
     q.DinvF = duh ? c->DinvF : nullptr;
     q.duh = duh;
     q.alpha = alpha;
@@ -1062,7 +1066,8 @@ int bj_blocked(hfem_ctx* c) {
     const int grid = std::max(1, std::min(nf, sms(c->device) * std::max(occ, 1)));
     // the kernel also solves with a right-hand side: c->w is free here and its
     // result is ignored
-    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->binfo);
+    inverse_blocked_kernel<B><<<grid, InvBlk<B>::THREADS, InvBlk<B>::SMEM, c->stream>>>(nf, c->Minv, c->w, c->w,
+                                                                                     c->binfo);
     return check_launch(c, "bj_inverse");
 }
 
@@ -1628,7 +1633,7 @@ int hfem_destroy(hfem_ctx* c) {
     cudaStreamSynchronize(c->stream);
     void* ptrs[] = {c->shapvt, c->shapvg, c->svsv, c->shapft, c->shapfg, c->sfsf, c->perm, c->dgnodes, c->elcon,
                     c->rowstart, c->colidx, c->blk_src, c->face_src, c->rowface, c->colface, c->udg, c->uh, c->sh,
-                    c->D, c->F, c->K, c->H, c->Ru, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
+                    c->D, c->F, c->K, c->H, c->Ru, c->DinvRu, c->Rh, c->Ro, c->ru2, c->Hg, c->Rg, c->Rr, c->rnorm, c->ws, c->DinvF,
                     c->info, c->Minv, c->V, c->w, c->x, c->pb, c->scal, c->part, c->binfo, c->udgi,
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
                     c->seg_ticket, c->seg_part, c->seg_partk, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
@@ -2363,7 +2368,7 @@ int device_buffer(hfem_ctx* c, int what, const double** src, size_t* need) {
         case 0: *src = c->Hg; *need = (size_t)d.nblocks * c->bsz * c->bsz; break;
         case 1: *src = c->Rg; *need = (size_t)d.nf * c->bsz; break;
         case 2: *src = c->Rr; *need = (size_t)d.nf * c->bsz; break;
-        case 3: *src = c->Ru; *need = (size_t)d.ne * c->n; break;
+        case 3: *src = c->DinvRu; *need = (size_t)d.ne * c->n; break;
         case 4: *src = c->DinvF; *need = (size_t)d.ne * c->n * c->nb; break;
         case 5: *src = c->H; *need = (size_t)d.ne * c->nb * c->nb; break;
         case 6: *src = c->Rh; *need = (size_t)d.ne * c->nb; break;
@@ -2588,7 +2593,7 @@ extern "C" int hfem_condense_noalloc(const hfem_dims* dims, const double* shapvt
     a.inviscid = appname == 0;
     L->element(dim3(ge), L->elem_smem, st, a);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
-    L->inverse(dim3(gi), st, d.ne, D, DinvRu, info);
+    L->inverse(dim3(gi), st, d.ne, D, DinvRu, DinvRu, info);
     if (cudaGetLastError() != cudaSuccess) return HFEM_E_CUDA;
     LiftArgs lh;
     lh.src = H;

@@ -16,7 +16,8 @@
 //      T applied to A(:, c) (a rank-8 update, one 8x8 output tile per DMMA pair).
 // No rows are swapped.  After the last panel the in-place result X satisfies
 // D^-1(k, p_m) = X(p_k, m) and (D^-1 Ru)(k) = X(p_k, Ru column), p_k the row
-// pivoted at step k.  A zero pivot reports 1 + step in info[e].
+// pivoted at step k.  A zero pivot reports 1 + step in info[e].  D^-1 replaces
+// D; D^-1 Ru goes to RuOut (which may be Ru itself).
 #pragma once
 #include <cuda_runtime.h>
 #include "schur_kernels.cuh"
@@ -144,7 +145,7 @@ __device__ __forceinline__ void inv_tile(double* __restrict__ A, const double* _
 
 template <int N>
 __global__ void __launch_bounds__(InvBlk<N>::THREADS, 2)
-    inverse_blocked_kernel(int ne, double* __restrict__ D, double* __restrict__ Ru, int* __restrict__ info) {
+    inverse_blocked_kernel(int ne, double* __restrict__ D, const double* Ru, double* RuOut, int* __restrict__ info) {
     using C = InvBlk<N>;
     constexpr int NP = C::NP, LDA = C::LDA, LDB = C::LDB, NW = C::THREADS / 32;
     extern __shared__ __align__(16) unsigned char inv_raw[];
@@ -254,7 +255,7 @@ __global__ void __launch_bounds__(InvBlk<N>::THREADS, 2)
             const int k = t % N, m = t / N;
             De[k + (size_t)N * piv[m]] = A[piv[k] + LDA * m];
         }
-        for (int k = tid; k < N; k += C::THREADS) Ru[(size_t)e * N + k] = A[piv[k] + LDA * C::RUC];
+        for (int k = tid; k < N; k += C::THREADS) RuOut[(size_t)e * N + k] = A[piv[k] + LDA * C::RUC];
         if (tid == 0) info[e] = 0;
         __syncthreads();
     }

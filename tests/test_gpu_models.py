@@ -72,3 +72,24 @@ def test_unsupported_models_rejected():
         with pytest.raises(HfemError):
             s._chk(s.lib.hfem_set_models(s.h, cs, vm), "set_models")
     s.close()
+
+
+def test_newton_line_search_matches_reference():
+    """Newton on a walled channel with the Roe tensor and Sutherland's law: the
+    full step raises the residual, so the line search of solveNonlinearProblem
+    (dgsolvers.cpp:106-205) halves the step with residual-only passes between
+    the updates; history and state against the reference driver's (fixture from
+    oracle/_ref/hfem_ref newton) within 1e-12."""
+    import os
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                  "ns2d_channel_roe_suth_p2_n4_newton.npz")))
+    p = with_models(ns2d_channel(n=4, porder=2), 2, 1)
+    s = HDGSolver(p)
+    s.getQ()
+    conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=2, gmres_tol=1e-10)
+    udg, uh = s.get_solution()
+    s.close()
+    r0 = g["rnorm_hist"][0]
+    assert len(hist) == len(g["rnorm_hist"]), (hist, g["rnorm_hist"])
+    assert np.max(np.abs(hist - g["rnorm_hist"])) <= 1e-12 * r0, (hist, g["rnorm_hist"])
+    assert rel(udg.ravel(), g["udg"].ravel()) < 1e-12 and rel(uh.ravel(), g["uh"].ravel()) < 1e-12
