@@ -9,14 +9,18 @@ import numpy as np
 import pytest
 
 from hfem_b200.core import HDGSolver
-from hfem_b200.gen.problem import ns2d_vortex, ns3d_fourier
+from hfem_b200.gen.problem import ns2d_channel, ns2d_vortex, ns3d_box, ns3d_fourier, with_models
 from oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
 CASES = [("2d_p2", lambda: ns2d_vortex(n=5, porder=2, seed=4)),
          ("2d_p3", lambda: ns2d_vortex(n=4, porder=3, seed=5)),
-         ("3d_p1", lambda: ns3d_fourier(n=3, porder=1, seed=6))]
+         ("3d_p1", lambda: ns3d_fourier(n=3, porder=1, seed=6)),
+         # bounded meshes (face blocks of boundary faces have fewer neighbours)
+         ("2d_p2_channel", lambda: ns2d_channel(n=4, porder=2, seed=7)),
+         ("2d_p2_channel_roe_sutherland", lambda: with_models(ns2d_channel(n=4, porder=2, seed=9), 2, 1)),
+         ("3d_p1_box", lambda: ns3d_box(n=2, porder=1))]
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])

@@ -93,3 +93,35 @@ def test_newton_line_search_matches_reference():
     assert len(hist) == len(g["rnorm_hist"]), (hist, g["rnorm_hist"])
     assert np.max(np.abs(hist - g["rnorm_hist"])) <= 1e-12 * r0, (hist, g["rnorm_hist"])
     assert rel(udg.ravel(), g["udg"].ravel()) < 1e-12 and rel(uh.ravel(), g["uh"].ravel()) < 1e-12
+
+
+def test_batch_line_search_equals_alone():
+    """Two packed problems whose full Newton steps are rejected: the batch's
+    per-problem line search (residual-only passes between per-problem updates)
+    reproduces each problem's own Newton history (per-problem GMRES to 1e-10,
+    so histories within 1e-8 of r0)."""
+    from hfem_b200.batch import BatchSolver
+    probs = [with_models(ns2d_channel(n=4, porder=2, seed=s), 2, 1) for s in (0, 3)]
+    alone = []
+    for p in probs:
+        s = HDGSolver(p)
+        s.getQ()
+        conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=2, gmres_tol=1e-10)
+        s.close()
+        alone.append(hist)
+    b = BatchSolver(probs)
+    b.s.getQ()
+    active = np.ones(len(probs), dtype=bool)
+    hb = [[] for _ in probs]
+    for it in range(2):
+        old, new = b.newton_iteration(1e-10, active, gmres_tol=1e-10)
+        for i in range(len(probs)):
+            if it == 0:
+                hb[i].append(old[i])
+            hb[i].append(new[i])
+    b.close()
+    for i in range(len(probs)):
+        h = np.array(hb[i])
+        assert h.shape == alone[i].shape, (h, alone[i])
+        assert np.max(np.abs(h - alone[i])) <= 1e-8 * alone[i][0], (h, alone[i])
+        assert alone[i][1] < alone[i][0]       # the line search took a partial step
