@@ -10,7 +10,10 @@ distributed GMRES / Newton are the module's own code, run as world_size 2
     (restated oracle): same iteration count, relative-residual history within
     1e-12, solution within 1e-12 relative;
   * two damped-Newton iterations over two ranks reproduce the single-domain
-    Newton residual history within 1e-12 of the first residual.
+    Newton residual history within 1e-12 of the first residual;
+  * on a walled channel with the Roe tensor and Sutherland's law, where the
+    full steps are rejected and the line search halves them, two ranks
+    reproduce the reference driver's history (tests/golden fixture) to 1e-12.
 """
 import os
 import socket
@@ -21,7 +24,7 @@ import pytest
 import torch
 
 from hfem_b200.dd import DDSolver, Exchange, partition
-from hfem_b200.gen.problem import ns2d_vortex
+from hfem_b200.gen.problem import ns2d_channel, ns2d_vortex, with_models
 from oracle import Oracle, newton_solve
 
 
@@ -163,3 +166,31 @@ def test_two_rank_newton_matches_single_domain(two_ranks):
     for res in two_ranks:
         assert len(res["nhist"]) == len(href)
         assert np.max(np.abs(res["nhist"] - np.array(href))) <= 1e-12 * href[0]
+
+
+def _channel_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        prob = with_models(ns2d_channel(n=4, porder=2), 2, 1)
+        prob.udg = Oracle(prob).getq(prob.udg, prob.uh)
+        part = partition(prob, world, rank)
+        dd = DDSolver(part, OracleBackend(part.prob), Exchange(part, prob.bsz, "cpu"))
+        ok, nhist = dd.newton(tol=1e-10, maxiter=2)
+        torch.save(dict(nhist=np.array(nhist)), os.path.join(out, f"chan{rank}.pt"))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_line_search_on_bounded_mesh_matches_reference(tmp_path):
+    import torch.multiprocessing as mp
+    out = str(tmp_path)
+    mp.start_processes(_channel_worker, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                  "ns2d_channel_roe_suth_p2_n4_newton.npz")))
+    for r in range(2):
+        h = torch.load(os.path.join(out, f"chan{r}.pt"), weights_only=False)["nhist"]
+        assert len(h) == len(g["rnorm_hist"])
+        assert np.max(np.abs(h - g["rnorm_hist"])) <= 1e-12 * g["rnorm_hist"][0], (h, g["rnorm_hist"])

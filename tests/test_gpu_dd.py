@@ -8,7 +8,9 @@ the all-reduces over CUDA tensors -- against the single-GPU solver chain:
   * the driver's block-Jacobi GMRES history equals hfem_gmres's within 1e-12
     and its solution within 1e-12 relative;
   * two Newton iterations match the reference driver's history
-    (tests/golden/ns2d_p2_n4_newton.npz) within 1e-12 of the first residual.
+    (tests/golden/ns2d_p2_n4_newton.npz) within 1e-12 of the first residual;
+  * so do two iterations on a walled channel with the Roe tensor and
+    Sutherland's law, where the line search rejects the full steps.
 """
 import os
 import socket
@@ -62,5 +64,19 @@ def test_dd_driver_on_gpu_backend(group):
     be = GPUBackend(partition(prob, 1, 0).prob, 0)
     dd = DDSolver(part, be, Exchange(part, prob.bsz, "cuda:0"))
     ok, nhist = dd.newton(tol=1e-14, maxiter=2)
+    be.s.close()
+    assert np.max(np.abs(np.array(nhist) - g["rnorm_hist"])) <= 1e-12 * g["rnorm_hist"][0], nhist
+
+
+
+def test_dd_line_search_on_gpu_backend(group):
+    from hfem_b200.dd import DDSolver, Exchange, GPUBackend, partition
+    from hfem_b200.gen.problem import ns2d_channel, with_models
+    g = dict(np.load(os.path.join(GOLDEN, "ns2d_channel_roe_suth_p2_n4_newton.npz")))
+    prob = with_models(ns2d_channel(n=4, porder=2), 2, 1)
+    part = partition(prob, 1, 0)
+    be = GPUBackend(part.prob, 0)
+    dd = DDSolver(part, be, Exchange(part, prob.bsz, "cuda:0"))
+    ok, nhist = dd.newton(tol=1e-10, maxiter=2)
     be.s.close()
     assert np.max(np.abs(np.array(nhist) - g["rnorm_hist"])) <= 1e-12 * g["rnorm_hist"][0], nhist
