@@ -124,6 +124,7 @@ struct Launch {
     GemmLaunch g1, g2;
     void (*schur_tc)(dim3, size_t, cudaStream_t, const SchurTcArgs&);
     size_t tc_smem;
+    int tc_tmem;                // tensor-memory columns of one tensor-core Schur CTA
     const void* tc_fn;
     void (*scatter_h)(dim3, cudaStream_t, const ScatterArgs&);
     void (*schur_fused)(cudaStream_t, int, const double*, const double*, const double*, double*, double*);
@@ -195,6 +196,7 @@ Launch make_launch() {
     L.g2 = GemmParams<typename SchurCfg<S>::g2>::make();
     L.schur_tc = launch_schur_tc<S>;
     L.tc_smem = TcCfg<S::N, S::NB>::SMEM;
+    L.tc_tmem = (int)TcCfg<S::N, S::NB>::TMEM_COLS;
     L.tc_fn = (const void*)schur_tc_kernel<S::N, S::NB>;
     L.scatter_h = launch_scatter_h<S>;
     L.schur_fused = launch_schur_fused<S>;
@@ -1606,8 +1608,8 @@ int hfem_create(const hfem_dims* dims, int device, hfem_ctx** out) {
         cudaFuncSetAttribute(g.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.tc_fn, TC_THREADS, L.tc_smem);
-    // each CTA holds 256 of the SM's 512 tensor-memory columns
-    c->grid_tc = std::max(1, std::min(d.ne, sms(device) * std::max(1, std::min(occ, 2))));
+    // the CTAs resident on an SM share its 512 tensor-memory columns
+    c->grid_tc = std::max(1, std::min(d.ne, sms(device) * std::max(1, std::min(occ, 512 / L.tc_tmem))));
     occ = 0;
     cudaFuncSetAttribute(L.inv_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.inv_smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, L.inv_fn, L.inv_threads, L.inv_smem);

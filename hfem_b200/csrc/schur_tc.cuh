@@ -14,6 +14,10 @@
 //     epilogues: DinvF goes to global memory (FP64, for the solution update)
 //     and into shared memory as the B operand of the second GEMM; the Schur
 //     update is applied to H in FP64.
+// The Schur update's two 128-row tiles of K have their own A buffers, TMEM
+// accumulators and barriers: the second tile is staged while the first
+// tile's MMAs run, and its MMAs run while the first tile's epilogue reads
+// and writes H.
 // Every mbarrier wait is bounded; on expiry the kernel records an error,
 // waits (bounded) for its MMAs, frees its tensor memory and returns.
 #pragma once
@@ -42,9 +46,14 @@ struct TcCfg {
     static constexpr uint32_t LBO_B = NBP * 16;       // bytes between k-chunks of B
     static constexpr int A_BYTES = 128 * KP * 4;
     static constexpr int B_BYTES = NBP * KP * 4;
-    static constexpr int SMEM = A_BYTES + B_BYTES + 1024;
-    static constexpr uint32_t TMEM_COLS = 256;
+    static constexpr int NA = MT2 > 1 ? 2 : 1;        // A buffers (one per row tile of K)
+    static constexpr int SMEM = NA * A_BYTES + B_BYTES + 1024;
+    // accumulators: one per A buffer, ACC columns apart; the allocation is a
+    // power of two of at least 32 columns
+    static constexpr uint32_t ACC = NBP <= 32 ? 32 : (NBP <= 64 ? 64 : (NBP <= 128 ? 128 : 256));
+    static constexpr uint32_t TMEM_COLS = NA * ACC < 32 ? 32 : NA * ACC;
     static_assert(N <= 128, "D must fit one 128-row MMA tile");
+    static_assert(MT2 <= 2, "K must fit two 128-row MMA tiles");
     static_assert(NBP <= 256, "nb must fit one MMA N");
 };
 
@@ -175,10 +184,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
     extern __shared__ __align__(16) unsigned char tc_raw[];
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) &
                                                            ~static_cast<uintptr_t>(1023));
-    float4* sA = reinterpret_cast<float4*>(base);                 // [kc][128 rows]
-    float4* sB = reinterpret_cast<float4*>(base + C::A_BYTES);    // [kc][NBP rows]
+    float4* sA[2] = {reinterpret_cast<float4*>(base),                       // [kc][128 rows]
+                     reinterpret_cast<float4*>(base + (C::NA - 1) * C::A_BYTES)};
+    float4* sB = reinterpret_cast<float4*>(base + C::NA * C::A_BYTES);      // [kc][NBP rows]
     float* sBf = reinterpret_cast<float*>(sB);
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tslot;
     __shared__ int s_bad;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -190,7 +200,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_bad = 0;
     }
@@ -198,12 +209,31 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tslot;
-    const uint32_t tlane = tmem + ((uint32_t)(32 * wq) << 16);
-    const uint32_t abase = smem_u32(sA), bbase = smem_u32(sB), barp = smem_u32(&bar);
+    const uint32_t acc[2] = {tmem, tmem + C::ACC};
+    const uint32_t lane_off = (uint32_t)(32 * wq) << 16;
+    const uint32_t abase[2] = {smem_u32(sA[0]), smem_u32(sA[1])}, bbase = smem_u32(sB);
+    const uint32_t barp[2] = {smem_u32(&bar[0]), smem_u32(&bar[1])};
     constexpr uint32_t IDESC = idesc_tf32(128, C::NBP);
-    uint32_t phase = 0;
-    int pend = 0;                                                 // thread 0: a commit whose wait expired
-    uint32_t pend_phase = 0;
+    uint32_t phase[2] = {0, 0};
+    int pend[2] = {0, 0};                                         // thread 0: commits whose wait expired
+    uint32_t pend_phase[2] = {0, 0};
+
+    auto issue = [&](int a, int t) {                              // thread 0: A buffer a x B -> accumulator t
+        tc_fence_after();
+#pragma unroll 1
+        for (int s = 0; s < C::KP / 8; s++)
+            tc_mma(acc[t], umma_desc(abase[a] + 2 * s * C::LBO_A, C::LBO_A, 128),
+                   umma_desc(bbase + 2 * s * C::LBO_B, C::LBO_B, 128), IDESC, s > 0 ? 1u : 0u);
+        tc_commit(barp[t]);
+    };
+    auto wait = [&](int t) {
+        if (!mbar_wait(barp[t], phase[t])) {
+            s_bad = 1;
+            if (tid == 0) pend[t] = 1, pend_phase[t] = phase[t];
+        }
+        phase[t] ^= 1;
+        tc_fence_after();
+    };
 
     for (int e = blockIdx.x; e < A.ne; e += gridDim.x) {
         const double* Di = A.Dinv + (size_t)e * N * N;
@@ -212,29 +242,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
         double* He = A.H + (size_t)e * NB * NB;
         double* DFe = A.DinvF + (size_t)e * N * NB;
         // ---- stage A = D^-1 (row m, k) and B = F^T (row nn, k) as FP32
-        stage_rows<N, 128>(sA, Di, N, 0, N, tid);
+        stage_rows<N, 128>(sA[0], Di, N, 0, N, tid);
         stage_cols<N, NB, C::NBP>(sB, Fe, tid);
         proxy_fence();
         __syncthreads();
-        // ---- GEMM 1: TMEM[:, 0:NBP) = D^-1 F
-        if (tid == 0) {
-            tc_fence_after();
-#pragma unroll 1
-            for (int s = 0; s < C::KP / 8; s++)
-                tc_mma(tmem, umma_desc(abase + 2 * s * C::LBO_A, C::LBO_A, 128),
-                       umma_desc(bbase + 2 * s * C::LBO_B, C::LBO_B, 128), IDESC, s > 0 ? 1u : 0u);
-            tc_commit(barp);
-        }
-        if (!mbar_wait(barp, phase)) {
-            s_bad = 1;
-            if (tid == 0) pend = 1, pend_phase = phase;
-        }
-        phase ^= 1;
-        tc_fence_after();
+        // ---- GEMM 1: accumulator 0 = D^-1 F
+        if (tid == 0) issue(0, 0);
+        wait(0);
         // ---- epilogue 1: DinvF to global (FP64) and to sB as B = DinvF^T (row nn, k)
         for (int cb = grp; cb < C::NBP / 8; cb += TC_GROUPS) {
             uint32_t r[8];
-            tmem_ld8(tlane + 8 * cb, r);
+            tmem_ld8(acc[0] + lane_off + 8 * cb, r);
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 const int nn = 8 * cb + j;
@@ -245,40 +263,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
             }
         }
         tc_fence_before();
-        // ---- GEMM 2 per 128-row tile of K: TMEM[:, 0:NBP) = K_tile DinvF, H_tile -= it
-        for (int mt = 0; mt < C::MT2; mt++) {
-            __syncthreads();                  // sA free (GEMM done), TMEM reads of the last epilogue done
-            stage_rows<N, 128>(sA, Ke, NB, 128 * mt, NB, tid);
+        // ---- GEMM 2: the row tiles of K, each in its own A buffer and accumulator
+        __syncthreads();                  // sA[0] free (GEMM 1 done), accumulator 0 read
+        stage_rows<N, 128>(sA[0], Ke, NB, 0, NB, tid);
+        proxy_fence();
+        __syncthreads();
+        if (s_bad) break;
+        if (tid == 0) issue(0, 0);
+        if constexpr (C::MT2 > 1) {
+            stage_rows<N, 128>(sA[1], Ke, NB, 128, NB, tid);      // while tile 0's MMAs run
             proxy_fence();
             __syncthreads();
-            if (s_bad) break;
-            if (tid == 0) {
-                tc_fence_after();
+            if (tid == 0) issue(1, 1);
+        }
 #pragma unroll 1
-                for (int s = 0; s < C::KP / 8; s++)
-                    tc_mma(tmem, umma_desc(abase + 2 * s * C::LBO_A, C::LBO_A, 128),
-                           umma_desc(bbase + 2 * s * C::LBO_B, C::LBO_B, 128), IDESC, s > 0 ? 1u : 0u);
-                tc_commit(barp);
-            }
-            if (!mbar_wait(barp, phase)) {
-                s_bad = 1;
-                if (tid == 0) pend = 1, pend_phase = phase;
-            }
-            phase ^= 1;
-            tc_fence_after();
+        for (int mt = 0; mt < C::MT2; mt++) {
+            const int t = mt;                                     // row tile mt: A buffer and accumulator mt
+            wait(t);
             const int rg = 128 * mt + row;
             for (int cb = grp; cb < C::NBP / 8; cb += 2 * TC_GROUPS) {
-                uint32_t r0[8], r1[8];
                 const bool two = cb + TC_GROUPS < C::NBP / 8;
-                tmem_ld8_nowait(tlane + 8 * cb, r0);
-                if (two) tmem_ld8_nowait(tlane + 8 * (cb + TC_GROUPS), r1);
-                tmem_wait_ld();
                 double h[16];
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     const int nn = 8 * (j < 8 ? cb : cb + TC_GROUPS) + (j & 7);
                     h[j] = (rg < NB && nn < NB && (j < 8 || two)) ? He[rg + (size_t)NB * nn] : 0.0;
                 }
+                uint32_t r0[8], r1[8];
+                tmem_ld8_nowait(acc[t] + lane_off + 8 * cb, r0);
+                if (two) tmem_ld8_nowait(acc[t] + lane_off + 8 * (cb + TC_GROUPS), r1);
+                tmem_wait_ld();
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     const int nn = 8 * (j < 8 ? cb : cb + TC_GROUPS) + (j & 7);
@@ -286,16 +300,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) schur_tc_kernel(SchurTcArgs A) 
                     if (rg < NB && nn < NB && (j < 8 || two)) He[rg + (size_t)NB * nn] = h[j] - (double)__uint_as_float(bits);
                 }
             }
-            tc_fence_before();
         }
-        __syncthreads();
+        tc_fence_before();
+        __syncthreads();                  // accumulators read, sA / sB free for the next element
         if (s_bad) break;
     }
     __syncthreads();
     if (s_bad && tid == 0) {
         atomicExch(A.err, 1);
         // let any MMA still in flight finish before the tensor memory is released
-        if (pend) mbar_wait(barp, pend_phase);
+        for (int t = 0; t < 2; t++)
+            if (pend[t]) mbar_wait(barp[t], pend_phase[t]);
     }
     __syncthreads();
     if (warp == 0) {
