@@ -616,7 +616,7 @@ def run_batched_task(args):
                      "max_rnorm_rel_diff_vs_plain": float(np.max(np.abs(rn - np.array(r_plain)) / np.array(r_plain))),
                      "tiles": {f"{k[0]}d_p{k[1]}": v for k, v in m.tiles.items()}}
         if prec == 1:
-            out[name]["dtype"] = "tf32 Schur GEMMs, f64 element LU / residual"
+            out[name]["dtype"] = "3xtf32 element contractions, tf32 Schur GEMMs where the autotuner picks them, f64 element LU / residual"
             out[name]["fp64_shapes"] = [f"{k[0]}d_p{k[1]}" for k in m.fp64_shapes]
         m.close()
     out["value"] = out["graph_mixed"]["value"]

@@ -22,19 +22,6 @@ struct Shape {
     static constexpr int NA = NGF * NFE;          // face points of one element
     static constexpr int NQ = NGV * ND1;          // (volume point, derivative) pairs
     static constexpr int MAXINC = ND;             // faces meeting at a node
-    // per-CTA global workspace (doubles)
-    static constexpr int W_WRL = NQ * NCU * NC;
-    static constexpr int W_SMIC = NGV * NPV * ND;
-    static constexpr int W_SMIE = NGV * NDF * ND;
-    static constexpr int W_SMICF = NA * NPV * ND;
-    static constexpr int W_SMIEF = NA * NDF * ND;
-    static constexpr int W_FNU = NA * NCH * NC;
-    static constexpr int W_FNUH = NA * NCH * NCH;
-    // boundary faces: the boundary flux and its Jacobians at the face points
-    static constexpr int W_FNUB = NA * NCH * NC;
-    static constexpr int W_FNUHB = NA * NCH * NCH;
-    static constexpr int W_FNB = NA * NCH;
-    static constexpr int WS = W_WRL + W_SMIC + W_SMIE + W_SMICF + W_SMIEF + W_FNU + W_FNUH + W_FNUB + W_FNUHB + W_FNB;
 };
 
 struct Tables {                 // master element tables, reference layouts
