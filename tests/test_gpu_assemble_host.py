@@ -5,14 +5,15 @@ import numpy as np
 import pytest
 
 from hfem_b200.core import HDGSolver
-from hfem_b200.gen.problem import ns2d_channel, ns3d_fourier
+from hfem_b200.gen.problem import ns2d_channel, ns3d_fourier, with_models
 
 pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("make,chunks", [(lambda: ns3d_fourier(n=3, porder=2), 4),
                                          (lambda: ns2d_channel(n=4, porder=3), 3),
-                                         (lambda: ns3d_fourier(n=3, porder=1), 1000)])
+                                         (lambda: ns3d_fourier(n=3, porder=1), 1000),
+                                         (lambda: with_models(ns2d_channel(n=4, porder=2), 2, 1), 3)])
 def test_assemble_host_equals_set_and_assemble(make, chunks):
     import torch
     prob = make()

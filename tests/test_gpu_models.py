@@ -125,3 +125,23 @@ def test_batch_line_search_equals_alone():
         assert h.shape == alone[i].shape, (h, alone[i])
         assert np.max(np.abs(h - alone[i])) <= 1e-8 * alone[i][0], (h, alone[i])
         assert alone[i][1] < alone[i][0]       # the line search took a partial step
+
+
+@pytest.mark.parametrize("mode", [1, 3], ids=["mixed", "split_tf32"])
+def test_mixed_newton_with_line_search_reaches_fp64_tolerance(mode):
+    """Mixed precision on the problem whose full steps the line search rejects:
+    Newton still ends at the FP64 residual tolerance, at the FP64 run's state."""
+    p = with_models(ns2d_channel(n=4, porder=2), 2, 1)
+    out = {}
+    for m in (0, mode):
+        s = HDGSolver(p)
+        s.set_precision(m)
+        s.getQ()
+        conv, hist = s.solveNonlinearProblem(newton_tol=1e-10, maxiter=30, gmres_tol=1e-10)
+        out[m] = (conv, hist, s.get_solution())
+        s.close()
+    for m in out:
+        assert out[m][0] == 1 and out[m][1][-1] < 1e-10, (m, out[m][1])
+    (u0, h0), (u1, h1) = out[0][2], out[mode][2]
+    assert rel(u1, u0) < 1e-8 and rel(h1, h0) < 1e-8
+
