@@ -285,6 +285,10 @@ struct hfem_ctx {
     long long* seg_pstart = nullptr;
     int *seg_pseg = nullptr, *seg_p0 = nullptr, *seg_ticket = nullptr;
     double *seg_part = nullptr, *seg_h = nullptr, *seg_y = nullptr, *seg_nrm = nullptr;
+    // GMRES bookkeeping on the device (GmState): Hessenberg, rotations, g, rhs norms, states
+    double *gm_H = nullptr, *gm_cs = nullptr, *gm_sn = nullptr, *gm_g = nullptr, *gm_nrmb = nullptr, *gm_hist = nullptr;
+    int *gm_state = nullptr, *gm_its = nullptr, *gm_jc = nullptr;
+    size_t gm_hist_n = 0;
     unsigned char* seg_act = nullptr;
     int* seg_k = nullptr;
     int seg_restart = 0;
@@ -1289,6 +1293,12 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
         // CGS2 (restart + 1 rows), P problems each
         if ((rc = dalloc(c, &c->seg_h, (size_t)(2 * restart + 3) * P))) return rc;
         if ((rc = dalloc(c, &c->seg_y, (size_t)restart * P))) return rc;
+        if ((rc = dalloc(c, &c->gm_H, (size_t)(restart + 1) * restart * P)) ||
+            (rc = dalloc(c, &c->gm_cs, (size_t)restart * P)) || (rc = dalloc(c, &c->gm_sn, (size_t)restart * P)) ||
+            (rc = dalloc(c, &c->gm_g, (size_t)(restart + 1) * P)) || (rc = dalloc(c, &c->gm_nrmb, (size_t)P)) ||
+            (rc = dalloc(c, &c->gm_state, (size_t)P)) || (rc = dalloc(c, &c->gm_its, (size_t)P)) ||
+            (rc = dalloc(c, &c->gm_jc, (size_t)P)))
+            return rc;
         c->seg_restart = restart;
         c->seg_hP = P;
     }
@@ -1303,6 +1313,10 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
     // p=3, 2.5M unknowns: 33 ms with MGS, 75 ms with CGS2 per 69 steps; batches
     // of 2D requests, 0.3-2M unknowns, were slower with CGS2 too).
     const bool cgs2 = restart + 1 <= 64 && n <= (1ll << 17);
+    if (hist && hist_len > 0 && c->gm_hist_n < (size_t)hist_len) {
+        if ((rc = dalloc(c, &c->gm_hist, (size_t)hist_len))) return rc;
+        c->gm_hist_n = (size_t)hist_len;
+    }
     if (cgs2 && c->seg_partk_n < (size_t)c->npieces * (restart + 1)) {
         if ((rc = dalloc(c, &c->seg_partk, (size_t)c->npieces * (restart + 1)))) return rc;
         c->seg_partk_n = (size_t)c->npieces * (restart + 1);
@@ -1330,9 +1344,25 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
     const int np = c->npieces;
     double* d_h = c->seg_h;                   // Hessenberg column, entry (i, p) at i * P + p
     double* d_h2 = c->seg_h + (size_t)(restart + 2) * P;   // CGS2's second projection, same layout
+    // the Givens rotations, residual estimates and stopping tests run on the
+    // device (gm_* kernels, one thread per problem); the host reads the
+    // problems' masks back only every GM_CHECK steps and at the start of a
+    // cycle, so the Arnoldi steps are enqueued without a round trip each
+    constexpr int GM_CHECK = 8;
+    const GmState GS{P, restart, maxit, tol, c->gm_H, c->gm_cs, c->gm_sn, c->gm_g, c->gm_nrmb, c->gm_state,
+                     c->gm_its, c->gm_jc, c->seg_act, (hist && hist_len > 0) ? c->gm_hist : nullptr,
+                     (hist && hist_len > 0) ? hist_len : 0};
+    const int gb = (P + 127) / 128;
     std::vector<unsigned char> act(P, 1);
     auto set_act = [&]() -> int {
         CK(cudaMemcpyAsync(c->seg_act, act.data(), P, cudaMemcpyHostToDevice, c->stream));
+        return 0;
+    };
+    auto any_active = [&](bool& live) -> int {
+        CK(cudaMemcpyAsync(act.data(), c->seg_act, P, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        live = false;
+        for (int p = 0; p < P; p++) live = live || act[p];
         return 0;
     };
     auto axpy_dot = [&](const double* hprev, const double* vprev, double* w, const double* b, double* out, int sq) {
@@ -1340,41 +1370,17 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
     };
     if ((rc = set_act())) return rc;
     axpy_dot(nullptr, nullptr, c->pb, c->pb, c->seg_nrm, 1);
-    std::vector<double> nrmb(P), beta(P), hcol((size_t)(restart + 2) * P), h2col((size_t)(restart + 1) * P);
-    CK(cudaMemcpyAsync(nrmb.data(), c->seg_nrm, sizeof(double) * P, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (double& v : nrmb)
-        if (v == 0.0) v = 1.0;
-    const size_t ldh = (size_t)(restart + 1) * restart;
-    std::vector<double> H(ldh * P), cs((size_t)restart * P), sn((size_t)restart * P), gv((size_t)(restart + 1) * P),
-        Y((size_t)restart * P);
-    std::vector<int> state(P, 2), its(P, 0), jc(P, 0);   // state 2 running, 1 converged, 0 maxit, -1 breakdown
-    std::vector<char> incycle(P, 0);
+    gm_init_kernel<<<gb, 128, 0, c->stream>>>(GS, c->seg_nrm);
     while (true) {
-        int running = 0;
-        for (int p = 0; p < P; p++) act[p] = state[p] == 2, running += state[p] == 2;
-        if (!running) break;
-        if ((rc = set_act())) return rc;
-        // r = M^-1 b - M^-1 A x, beta = |r| per problem
+        // r = M^-1 b - M^-1 A x, beta = |r| per problem, on the problems still running
+        gm_running_kernel<<<gb, 128, 0, c->stream>>>(GS);
         if ((rc = matvec_warp(c, c->x, c->w, prec, mv_act))) return rc;
         seg_sub_from_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, c->pb, c->w);
         axpy_dot(nullptr, nullptr, c->w, c->w, c->seg_nrm, 1);
-        CK(cudaMemcpyAsync(beta.data(), c->seg_nrm, sizeof(double) * P, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        int live = 0;
-        for (int p = 0; p < P; p++) {
-            incycle[p] = 0;
-            jc[p] = 0;
-            if (state[p] != 2) continue;
-            if (beta[p] / nrmb[p] <= tol) { state[p] = 1; continue; }
-            incycle[p] = 1;
-            live++;
-            std::fill(gv.begin() + (size_t)p * (restart + 1), gv.begin() + (size_t)(p + 1) * (restart + 1), 0.0);
-            gv[(size_t)p * (restart + 1)] = beta[p];
-        }
+        gm_cycle_kernel<<<gb, 128, 0, c->stream>>>(GS, c->seg_nrm);
+        bool live = false;
+        if ((rc = any_active(live))) return rc;
         if (!live) break;
-        for (int p = 0; p < P; p++) act[p] = incycle[p];
-        if ((rc = set_act())) return rc;
         seg_scale_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, c->seg_nrm, c->w, c->V);
         for (int j = 0; j < restart && live; j++) {
             double* vj = c->V + (size_t)j * n;
@@ -1398,81 +1404,20 @@ int gmres_seg_impl(hfem_ctx* c, int precond, int restart, double tol, int maxit,
                 }
                 seg_scale_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, d_h + (size_t)(j + 1) * P, vn, vn);
             }
+            gm_givens_kernel<<<gb, 128, 0, c->stream>>>(GS, j, d_h, cgs2 ? d_h2 : nullptr);
             if ((rc = check_launch(c, "arnoldi"))) return rc;
-            CK(cudaMemcpyAsync(hcol.data(), d_h, sizeof(double) * (size_t)(j + 2) * P, cudaMemcpyDeviceToHost,
-                               c->stream));
-            if (cgs2)
-                CK(cudaMemcpyAsync(h2col.data(), d_h2, sizeof(double) * (size_t)(j + 1) * P, cudaMemcpyDeviceToHost,
-                                   c->stream));
-            CK(cudaStreamSynchronize(c->stream));
-            if (cgs2)
-                for (size_t q = 0; q < (size_t)(j + 1) * P; q++) hcol[q] += h2col[q];
-            bool changed = false;
-            for (int p = 0; p < P; p++) {
-                if (!incycle[p]) continue;
-                double* h = H.data() + ldh * p;
-                double* cp = cs.data() + (size_t)restart * p;
-                double* sp = sn.data() + (size_t)restart * p;
-                double* gp = gv.data() + (size_t)(restart + 1) * p;
-                for (int i = 0; i <= j + 1; i++) h[i + (restart + 1) * j] = hcol[(size_t)i * P + p];
-                const double nn = hcol[(size_t)(j + 1) * P + p];
-                for (int i = 0; i < j; i++) {
-                    const double a = h[i + (restart + 1) * j], b = h[i + 1 + (restart + 1) * j];
-                    h[i + (restart + 1) * j] = cp[i] * a + sp[i] * b;
-                    h[i + 1 + (restart + 1) * j] = -sp[i] * a + cp[i] * b;
-                }
-                const double a = h[j + (restart + 1) * j], b = h[j + 1 + (restart + 1) * j];
-                const double rr = std::sqrt(a * a + b * b);
-                cp[j] = a / rr;
-                sp[j] = b / rr;
-                h[j + (restart + 1) * j] = rr;
-                h[j + 1 + (restart + 1) * j] = 0.0;
-                gp[j + 1] = -sp[j] * gp[j];
-                gp[j] = cp[j] * gp[j];
-                its[p]++;
-                jc[p] = j + 1;
-                const double res = std::fabs(gp[j + 1]);
-                if (p == 0 && hist && its[0] - 1 < hist_len) hist[its[0] - 1] = res / nrmb[0];
-                int stop = 2;
-                if (res / nrmb[p] <= tol) stop = 1;
-                else if (its[p] >= maxit) stop = 0;
-                else if (nn == 0.0) stop = -1;
-                if (stop != 2) {
-                    state[p] = stop;
-                    incycle[p] = 0;
-                    live--;
-                    changed = true;
-                }
-            }
-            if (changed && live) {
-                for (int p = 0; p < P; p++) act[p] = incycle[p];
-                if ((rc = set_act())) return rc;
-            }
+            if ((j + 1) % GM_CHECK == 0 && j + 1 < restart && (rc = any_active(live))) return rc;
         }
         // x += V y for every problem that took part in this cycle
-        std::vector<int> kk(P, 0);
-        std::fill(Y.begin(), Y.end(), 0.0);
-        for (int p = 0; p < P; p++) {
-            const int J = jc[p];
-            act[p] = J > 0;
-            kk[p] = J;
-            if (!J) continue;
-            const double* h = H.data() + ldh * p;
-            const double* gp = gv.data() + (size_t)(restart + 1) * p;
-            double* y = Y.data() + (size_t)restart * p;
-            for (int i = J - 1; i >= 0; i--) {
-                double s = gp[i];
-                for (int k = i + 1; k < J; k++) s -= h[i + (restart + 1) * k] * y[k];
-                y[i] = s / h[i + (restart + 1) * i];
-            }
-        }
-        if ((rc = set_act())) return rc;
-        CK(cudaMemcpyAsync(c->seg_k, kk.data(), sizeof(int) * P, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->seg_y, Y.data(), sizeof(double) * Y.size(), cudaMemcpyHostToDevice, c->stream));
+        gm_solve_kernel<<<gb, 128, 0, c->stream>>>(GS, c->seg_y, c->seg_k);
         seg_combine_kernel<<<np, SEG_THREADS, 0, c->stream>>>(SP, n, c->seg_k, restart, c->V, c->seg_y, c->x);
         if ((rc = check_launch(c, "combine_seg"))) return rc;
-        CK(cudaStreamSynchronize(c->stream));
     }
+    std::vector<int> state(P), its(P);
+    CK(cudaMemcpyAsync(state.data(), c->gm_state, sizeof(int) * P, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(its.data(), c->gm_its, sizeof(int) * P, cudaMemcpyDeviceToHost, c->stream));
+    if (hist && hist_len > 0)
+        CK(cudaMemcpyAsync(hist, c->gm_hist, sizeof(double) * hist_len, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     flush_timer(c);
     for (int p = 0; p < P; p++) {
@@ -1640,7 +1585,8 @@ int hfem_destroy(hfem_ctx* c) {
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
                     c->seg_ticket, c->seg_part, c->seg_partk, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
-                    c->d_lvl_lo, c->d_lvl_up, c->Mg32};
+                    c->d_lvl_lo, c->d_lvl_up, c->Mg32, c->gm_H, c->gm_cs, c->gm_sn, c->gm_g, c->gm_nrmb, c->gm_hist,
+                    c->gm_state, c->gm_its, c->gm_jc};
     for (void* p : ptrs)
         if (p) pool_free(p);
     for (auto& p : c->timer.pending) {

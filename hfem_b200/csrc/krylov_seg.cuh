@@ -317,4 +317,112 @@ __global__ void __launch_bounds__(256) bsr_matvec_warp_kernel(int nrows, const i
     }
 }
 
+
+// ---- GMRES bookkeeping on the device (one thread per problem), so that the
+// host enqueues Arnoldi steps without reading every Hessenberg column back.
+// Per problem p: H ((restart + 1) x restart, column-major), Givens cosines and
+// sines (restart), g (restart + 1), the rhs norm nrmb, state (2 running,
+// 1 converged, 0 iteration limit, -1 breakdown), iterations, the cycle's step
+// count jc, and act (the segment mask every segment kernel reads).
+struct GmState {
+    int P, restart, maxit;
+    double tol;
+    double *H, *cs, *sn, *g, *nrmb;
+    int *state, *its, *jc;
+    unsigned char* act;
+    double* hist;               // problem 0's relative residual per iteration (hist_len entries) or NULL
+    int hist_len;
+};
+
+__global__ void gm_init_kernel(GmState S, const double* __restrict__ nrm) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.P) return;
+    S.nrmb[p] = nrm[p] == 0.0 ? 1.0 : nrm[p];
+    S.state[p] = 2;
+    S.its[p] = 0;
+}
+
+// the mask of the problems still running
+__global__ void gm_running_kernel(GmState S) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < S.P) S.act[p] = S.state[p] == 2;
+}
+
+// start of a restart cycle: beta = |r| per problem (nrm)
+__global__ void gm_cycle_kernel(GmState S, const double* __restrict__ nrm) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.P) return;
+    S.jc[p] = 0;
+    unsigned char a = 0;
+    if (S.state[p] == 2) {
+        if (nrm[p] / S.nrmb[p] <= S.tol) {
+            S.state[p] = 1;
+        } else {
+            a = 1;
+            double* gp = S.g + (size_t)(S.restart + 1) * p;
+            gp[0] = nrm[p];
+            for (int i = 1; i <= S.restart; i++) gp[i] = 0.0;
+        }
+    }
+    S.act[p] = a;
+}
+
+// Arnoldi step j: the new Hessenberg column (h, plus h2 for the second CGS
+// projection), the previous rotations applied, the new rotation, the residual
+// estimate and the stopping test (kernel/gmres_bilu0.m:17-105)
+__global__ void gm_givens_kernel(GmState S, int j, const double* __restrict__ h, const double* __restrict__ h2) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.P || !S.act[p]) return;
+    const int R = S.restart, P = S.P;
+    double* hc = S.H + (size_t)(R + 1) * R * p + (size_t)(R + 1) * j;
+    double* cp = S.cs + (size_t)R * p;
+    double* sp = S.sn + (size_t)R * p;
+    double* gp = S.g + (size_t)(R + 1) * p;
+    for (int i = 0; i <= j + 1; i++) hc[i] = h[(size_t)i * P + p] + ((h2 && i <= j) ? h2[(size_t)i * P + p] : 0.0);
+    const double nn = h[(size_t)(j + 1) * P + p];
+    for (int i = 0; i < j; i++) {
+        const double a = hc[i], b = hc[i + 1];
+        hc[i] = cp[i] * a + sp[i] * b;
+        hc[i + 1] = -sp[i] * a + cp[i] * b;
+    }
+    const double a = hc[j], b = hc[j + 1];
+    const double rr = sqrt(a * a + b * b);
+    cp[j] = a / rr;
+    sp[j] = b / rr;
+    hc[j] = rr;
+    hc[j + 1] = 0.0;
+    gp[j + 1] = -sp[j] * gp[j];
+    gp[j] = cp[j] * gp[j];
+    const int it = ++S.its[p];
+    S.jc[p] = j + 1;
+    const double res = fabs(gp[j + 1]);
+    if (p == 0 && S.hist && it - 1 < S.hist_len) S.hist[it - 1] = res / S.nrmb[0];
+    int stop = 2;
+    if (res / S.nrmb[p] <= S.tol) stop = 1;
+    else if (it >= S.maxit) stop = 0;
+    else if (nn == 0.0) stop = -1;
+    if (stop != 2) {
+        S.state[p] = stop;
+        S.act[p] = 0;
+    }
+}
+
+// end of a cycle: y = H^-1 g by back substitution for every problem that took
+// steps, its step count and mask for the combination x += V y
+__global__ void gm_solve_kernel(GmState S, double* __restrict__ y, int* __restrict__ kseg) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= S.P) return;
+    const int R = S.restart, J = S.jc[p];
+    S.act[p] = J > 0;
+    kseg[p] = J;
+    const double* hp = S.H + (size_t)(R + 1) * R * p;
+    const double* gp = S.g + (size_t)(R + 1) * p;
+    double* yp = y + (size_t)R * p;
+    for (int i = J - 1; i >= 0; i--) {
+        double s = gp[i];
+        for (int k = i + 1; k < J; k++) s -= hp[i + (R + 1) * k] * yp[k];
+        yp[i] = s / hp[i + (R + 1) * i];
+    }
+}
+
 }  // namespace hfem
