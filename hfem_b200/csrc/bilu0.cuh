@@ -274,4 +274,376 @@ __global__ void __launch_bounds__(1024) bilu0_apply_cta_kernel(BiluSolveArgs A, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Scheduled forms for block sizes up to 32, for orderings whose levels hold
+// few rows.  One CTA walks the levels with a CTA barrier between them, one
+// warp per row of a level, lane r owning row r of the row's blocks.  The host
+// flattens every index chain into per-slot lists (a slot is a row's place in
+// the level order), and each warp stages what does not depend on the previous
+// level -- its next row's lists, and the blocks that are final before that
+// level starts -- into registers and shared memory by asynchronous copies
+// before the level barrier; after the barrier it fetches only what the
+// previous levels produced, in one round of copies.
+//
+// Every array these kernels write (the factors, y, v) is written by this one
+// CTA, so the L1-cached copies below see its own writes after a barrier.
+constexpr int BILU_ROWMAX = 7;   // blocks per row: 2 nfe - 1 for triangles (5) and tetrahedra (7)
+
+// Per-slot records, fixed stride so one asynchronous copy fetches a slot's
+// whole description (ints):
+//   factorisation (BILU_FREC): [0] row i, [1] rowstart[i], [2] blocks in the
+//     row, [3] records n_r, [4] U blocks n_u; [8 + 2t, 9 + 2t] record t, t < 32:
+//     per earlier neighbour k in order {M_ik's block in the row, updates n},
+//     then n x {M_il's block in the row, 0}; [72 + t] U block t, t < 32: the
+//     positions of U_kk^-1 and the U_kl in the order the records use them;
+//   solves (BILU_SREC): [0] row i, [1] entries n_e (at most BILU_ROWMAX - 1),
+//     [2] position of U_ii^-1 (upper solve), [3] the row's slot; [4 + 2j,
+//     5 + 2j] entry j: {position of L_ik or U_ik, k}; [16 + j] k's slot.
+// Slots: a row's result (y_i in the lower solve, v_i in the upper) is also
+// kept in a shared-memory slot from its level to the last level that reads
+// it; the host assigns the slots (an interval colouring of those live
+// ranges), so that a level reads its neighbours' results from shared memory.
+constexpr int BILU_FREC = 128, BILU_SREC = 32;
+
+struct BiluSched {
+    int nlo, nup;               // levels of the lower (and factorisation) order and of the upper order
+    const int* lvl_lo;          // level l: slots lvl_lo[l] .. lvl_lo[l+1] of the lower order
+    const int* lvl_up;
+    const int* frec;            // per slot of the lower order
+    const int* lrec;            // per slot of the lower order
+    const int* urec;            // per slot of the upper order
+    int nslot_lo, nslot_up;     // slots of each solve (0: results read from global memory)
+};
+
+// 4- or 8-byte asynchronous global->shared copy, cached in L1.
+template <class T>
+__device__ __forceinline__ void bl_cp_async(T* smem, const T* gmem) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element copies of 4 or 8 bytes");
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gmem), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void bl_cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void bl_cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <class T>
+__device__ __forceinline__ void bl_warp_copy(T* s, const T* g, int n, int lane) {
+    for (int t = lane; t < n; t += 32) bl_cp_async(s + t, g + t);
+}
+// a slot's record into the warp's record area (issued ahead; waited for by the next copy round)
+__device__ __forceinline__ void bl_fetch_record(int* rc, const int* rec, int stride, int lane) {
+    __syncwarp();
+    if (4 * lane < stride) bl_cp_async16(rc + 4 * lane, rec + 4 * lane);
+}
+
+template <int B>
+struct BiluFacCfg {
+    static constexpr int B2 = B * B;
+    static constexpr int UBUF = B <= 20 ? 8 : 4;                       // U blocks staged per round
+    static constexpr size_t BLK_BYTES = (((size_t)(BILU_ROWMAX + UBUF) * B2 * sizeof(double) + 15) / 16) * 16;
+    static constexpr size_t WARP_BYTES = BLK_BYTES + BILU_FREC * 4;
+    static constexpr int NW0 = (int)((200 * 1024) / WARP_BYTES);
+    static constexpr int NW = NW0 > 8 ? 8 : NW0;                       // warps of the CTA
+    static constexpr size_t SMEM = WARP_BYTES * NW;
+};
+
+// The factorisation of every level in one CTA: row i, held in shared memory,
+// takes for each earlier neighbour k in order L_ik = M_ik U_kk^-1 and
+// M_il -= L_ik U_kl, then inverts its diagonal block by Gauss-Jordan with
+// partial pivoting in registers (row r in lane r; the pivot is the first row
+// of largest magnitude, as in smem_blk_inv), and is written back.  The block
+// products sum in the order of smem_blk_mul.
+template <int B>
+__global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S, double* Mg, int* info) {
+    static_assert(B <= 32, "one lane per block row");
+    using C = BiluFacCfg<B>;
+    constexpr int B2 = C::B2, UBUF = C::UBUF;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ __align__(16) unsigned char bf_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int r = lane < B ? lane : 0;   // lanes >= B repeat row 0 and store nothing
+    double* rowbuf = reinterpret_cast<double*>(bf_raw + (size_t)w * C::WARP_BYTES);
+    double* ubuf = rowbuf + (size_t)BILU_ROWMAX * B2;
+    int* rc = reinterpret_cast<int*>(bf_raw + (size_t)w * C::WARP_BYTES + C::BLK_BYTES);
+    // stage U blocks ub .. ub + UBUF - 1 of the row's list
+    auto stage = [&](int ub, int nu) {
+        __syncwarp();
+        const int n = min(UBUF, nu - ub);
+        for (int j = 0; j < n; j++) bl_warp_copy(ubuf + (size_t)j * B2, Mg + (size_t)rc[72 + ub + j] * B2, B2, lane);
+        bl_cp_wait_all();
+        __syncwarp();
+    };
+    auto factor_row = [&]() {
+        bl_cp_wait_all();
+        __syncwarp();
+        const int i = rc[0], r0 = rc[1], nrb = rc[2], nrec = rc[3], nu = rc[4];
+        bl_warp_copy(rowbuf, Mg + (size_t)r0 * B2, nrb * B2, lane);
+        int uc = 0, rb = 0;
+        stage(0, nu);
+        for (int j = 0; j < nrec;) {
+            const int pl = rc[8 + 2 * j], nupd = rc[9 + 2 * j];
+            j++;
+            if (uc - rb == UBUF) stage(rb = uc, nu);
+            const double* Ukk = ubuf + (size_t)(uc - rb) * B2;
+            uc++;
+            double* Mik = rowbuf + (size_t)pl * B2;
+            double m[B], lv[B];
+#pragma unroll
+            for (int c = 0; c < B; c++) m[c] = Mik[r + B * c];
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < B; q++) t = fma(m[q], Ukk[q + B * c], t);
+                lv[c] = t;
+            }
+            if (lane < B)
+#pragma unroll
+                for (int c = 0; c < B; c++) Mik[r + B * c] = lv[c];
+            for (int u = 0; u < nupd; u++) {
+                const int ql = rc[8 + 2 * j];
+                j++;
+                if (uc - rb == UBUF) stage(rb = uc, nu);
+                const double* Ukl = ubuf + (size_t)(uc - rb) * B2;
+                uc++;
+                double* Mil = rowbuf + (size_t)ql * B2;
+#pragma unroll
+                for (int c = 0; c < B; c++) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int q = 0; q < B; q++) t = fma(lv[q], Ukl[q + B * c], t);
+                    if (lane < B) Mil[r + B * c] -= t;
+                }
+            }
+        }
+        // the diagonal block (first in the row)
+        double a[B];
+        int piv[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) a[c] = rowbuf[r + B * c];
+        int bad = 0;
+#pragma unroll
+        for (int k = 0; k < B; k++) {
+            double v = (lane >= k && lane < B) ? fabs(a[k]) : -1.0;
+            int p = lane;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v2 = __shfl_xor_sync(FULL, v, o);
+                const int p2 = __shfl_xor_sync(FULL, p, o);
+                if (v2 > v || (v2 == v && p2 < p)) {
+                    v = v2;
+                    p = p2;
+                }
+            }
+            // one lane's choice for all (lanes agree unless the block holds NaNs)
+            p = __shfl_sync(FULL, p, 0);
+            v = __shfl_sync(FULL, v, 0);
+            piv[k] = p;
+            if (v == 0.0) {
+                bad = k + 1;
+                break;
+            }
+            const int src = lane == k ? p : (lane == p ? k : lane);
+#pragma unroll
+            for (int c = 0; c < B; c++) a[c] = __shfl_sync(FULL, a[c], src);
+            const double dinv = 1.0 / __shfl_sync(FULL, a[k], k);
+            if (lane == k)
+#pragma unroll
+                for (int c = 0; c < B; c++) a[c] = (c == k ? 1.0 : a[c]) * dinv;
+            const double col = a[k];
+#pragma unroll
+            for (int c = 0; c < B; c++) {
+                const double pc = __shfl_sync(FULL, a[c], k);
+                if (lane != k) a[c] = (c == k ? 0.0 : a[c]) - col * pc;
+            }
+        }
+        if (!bad) {
+#pragma unroll
+            for (int k = B - 1; k >= 0; k--) {
+                const int p = piv[k];
+                const double ak = a[k];
+#pragma unroll
+                for (int c = k + 1; c < B; c++)
+                    if (c == p) {
+                        a[k] = a[c];
+                        a[c] = ak;
+                    }
+            }
+            if (lane < B)
+#pragma unroll
+                for (int c = 0; c < B; c++) rowbuf[r + B * c] = a[c];
+        }
+        __syncwarp();
+        for (int t = lane; t < nrb * B2; t += 32) Mg[(size_t)r0 * B2 + t] = rowbuf[t];
+        if (lane == 0) info[i] = bad;
+    };
+    if (S.nlo > 0 && w < S.lvl_lo[1]) bl_fetch_record(rc, S.frec + (size_t)w * BILU_FREC, BILU_FREC, lane);
+    for (int l = 0; l < S.nlo; l++) {
+        const int sb = S.lvl_lo[l], se = S.lvl_lo[l + 1];
+        for (int s = sb + w; s < se; s += nw) {
+            if (s != sb + w) bl_fetch_record(rc, S.frec + (size_t)s * BILU_FREC, BILU_FREC, lane);
+            factor_row();
+        }
+        if (l + 1 < S.nlo && S.lvl_lo[l + 1] + w < S.lvl_lo[l + 2])
+            bl_fetch_record(rc, S.frec + (size_t)(S.lvl_lo[l + 1] + w) * BILU_FREC, BILU_FREC, lane);
+        __syncthreads();
+    }
+}
+
+template <int B, class MT>
+struct BiluSolCfg {
+    static constexpr int B2 = B * B;
+    static constexpr size_t BLK_BYTES = ((BILU_ROWMAX * B2 * sizeof(MT) + 15) / 16) * 16;
+    static constexpr size_t WARP_BYTES = BLK_BYTES + 3 * BILU_SREC * 4;   // blocks, three records
+    static constexpr size_t BUDGET = 200 * 1024;                          // shared memory of the CTA
+    // warps for a slot table of nslot rows (0: too large for shared memory)
+    static int warps(int nslot) {
+        const size_t tab = (size_t)nslot * B * sizeof(double);
+        if (tab + WARP_BYTES > BUDGET) return 0;
+        const size_t n = (BUDGET - tab) / WARP_BYTES;
+        return n > 16 ? 16 : (int)n;
+    }
+    static size_t smem(int nw, int nslot) { return WARP_BYTES * nw + (size_t)nslot * B * sizeof(double); }
+};
+
+__device__ __forceinline__ void bl_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bl_cp_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Both triangular solves in one CTA, v = U^-1 L^-1 x, software-pipelined
+// over the levels: a warp's record for level l + 2 and the blocks and
+// right-hand side entry of its row of level l + 1 are requested before the
+// barrier that ends level l, so after the barrier only the neighbours' vector
+// entries (the previous levels' results) are loaded.  Level l's record lives
+// in record buffer l mod 2; a warp's further rows of a level (levels wider
+// than the CTA) go through the third buffer without the pipeline.  For
+// B <= 16 the two half-warps take alternate entries and add their partial
+// sums by one shuffle; the upper solve's product with U_ii^-1 takes the row's
+// sums from the lanes that hold them.
+template <int B, class MT>
+__global__ void __launch_bounds__(512, 1) bilu0_solve_sched_kernel(BiluSched S, const MT* __restrict__ Mg,
+                                                                   const double* __restrict__ x, double* y,
+                                                                   double* v) {
+    static_assert(B <= 32, "one lane per block row");
+    using C = BiluSolCfg<B, MT>;
+    constexpr int B2 = C::B2, H = B <= 16 ? 2 : 1, LW = 32 / H;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ __align__(16) unsigned char bs_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int g = lane / LW, r = lane % LW;
+    const int rr = r < B ? r : 0;
+    MT* blk = reinterpret_cast<MT*>(bs_raw + (size_t)w * C::WARP_BYTES);
+    int* rcb = reinterpret_cast<int*>(bs_raw + (size_t)w * C::WARP_BYTES + C::BLK_BYTES);   // 3 x BILU_SREC
+    double* tab = reinterpret_cast<double*>(bs_raw + (size_t)nw * C::WARP_BYTES);           // slot table
+    // the row of record rc: its blocks (U_ii^-1 after them for the upper
+    // solve) by asynchronous copies, and its right-hand side entry
+    auto issue_row = [&](const int* rc, const double* b, bool upper) {
+        const int i = rc[0], ne = rc[1];
+        for (int j = 0; j < ne; j++) bl_warp_copy(blk + (size_t)j * B2, Mg + (size_t)rc[4 + 2 * j] * B2, B2, lane);
+        if (upper) bl_warp_copy(blk + (size_t)ne * B2, Mg + (size_t)rc[2] * B2, B2, lane);
+        return b[(size_t)i * B + rr];
+    };
+    // sum_j (block j row r) . vec_kj over the row's entries, whole row in every
+    // lane; vec_kj from k's slot when the solve has slots
+    auto rowsum = [&](const int* rc, const double* vec, bool slots) {
+        const int ne = rc[1];
+        auto src = [&](int j) { return slots ? tab + (size_t)rc[16 + j] * B : vec + (size_t)rc[5 + 2 * j] * B; };
+        double t = 0.0;
+        if (g < ne) {
+            double va[B], vb[B];
+            const bool two = g + H < ne;
+            const double* ka = src(g);
+            const double* kb = src(two ? g + H : g);
+#pragma unroll
+            for (int c = 0; c < B; c++) va[c] = ka[c];
+#pragma unroll
+            for (int c = 0; c < B; c++) vb[c] = kb[c];
+            const MT* ba = blk + (size_t)g * B2 + rr;
+            double d = 0.0;
+#pragma unroll
+            for (int c = 0; c < B; c++) d = fma((double)ba[B * c], va[c], d);
+            t = d;
+            if (two) {
+                const MT* bb = blk + (size_t)(g + H) * B2 + rr;
+                d = 0.0;
+#pragma unroll
+                for (int c = 0; c < B; c++) d = fma((double)bb[B * c], vb[c], d);
+                t += d;
+            }
+            for (int j = g + 2 * H; j < ne; j += H) {
+                const MT* bj = blk + (size_t)j * B2 + rr;
+                const double* kj = src(j);
+                d = 0.0;
+#pragma unroll
+                for (int c = 0; c < B; c++) d = fma((double)bj[B * c], kj[c], d);
+                t += d;
+            }
+        }
+        if (H == 2) t += __shfl_xor_sync(FULL, t, 16);
+        return t;
+    };
+    // one triangular solve over its levels; out_i = rhs_i - sum (lower) or
+    // U_ii^-1 (rhs_i - sum) (upper)
+    auto sweep = [&](int nlev, const int* lvl, const int* rec, const double* b, const double* vec, double* out,
+                     bool upper, bool slots) {
+        double rhs = 0.0;
+        // prologue: the records of levels 0 and 1, the row of level 0
+        if (nlev > 0 && w < lvl[1]) bl_fetch_record(rcb, rec + (size_t)w * BILU_SREC, BILU_SREC, lane);
+        bl_cp_wait_all();
+        __syncwarp();
+        if (nlev > 0 && w < lvl[1]) rhs = issue_row(rcb, b, upper);
+        bl_cp_commit();
+        if (nlev > 1 && lvl[1] + w < lvl[2])
+            bl_fetch_record(rcb + BILU_SREC, rec + (size_t)(lvl[1] + w) * BILU_SREC, BILU_SREC, lane);
+        bl_cp_commit();
+        for (int l = 0; l < nlev; l++) {
+            const int sb = lvl[l], se = lvl[l + 1];
+            int* rc = rcb + (l & 1) * BILU_SREC;
+            for (int s = sb + w; s < se; s += nw) {
+                if (s == sb + w) {
+                    bl_cp_wait_but_one();   // this row's blocks (the next record may still be in flight)
+                } else {
+                    rc = rcb + 2 * BILU_SREC;
+                    bl_fetch_record(rc, rec + (size_t)s * BILU_SREC, BILU_SREC, lane);
+                    bl_cp_wait_all();
+                    __syncwarp();
+                    rhs = issue_row(rc, b, upper);
+                    bl_cp_wait_all();
+                }
+                __syncwarp();
+                const double t = rowsum(rc, vec, slots);
+                double o = rhs - t;
+                if (upper) {
+                    const MT* Dinv = blk + (size_t)rc[1] * B2 + rr;
+                    double u = 0.0;
+#pragma unroll
+                    for (int c = 0; c < B; c++) u = fma((double)Dinv[B * c], __shfl_sync(FULL, o, c), u);
+                    o = u;
+                }
+                if (g == 0 && r < B) {
+                    out[(size_t)rc[0] * B + r] = o;
+                    if (slots) tab[(size_t)rc[3] * B + r] = o;
+                }
+            }
+            // the row of level l + 1 (its record arrived during this level), the record of level l + 2
+            __syncwarp();
+            if (l + 1 < nlev && lvl[l + 1] + w < lvl[l + 2]) {
+                bl_cp_wait_all();
+                __syncwarp();
+                rhs = issue_row(rcb + ((l + 1) & 1) * BILU_SREC, b, upper);
+            }
+            bl_cp_commit();
+            if (l + 2 < nlev && lvl[l + 2] + w < lvl[l + 3])
+                bl_fetch_record(rcb + (l & 1) * BILU_SREC, rec + (size_t)(lvl[l + 2] + w) * BILU_SREC, BILU_SREC,
+                                lane);
+            bl_cp_commit();
+            __syncthreads();
+        }
+        bl_cp_wait_all();
+    };
+    sweep(S.nlo, S.lvl_lo, S.lrec, x, y, y, false, S.nslot_lo > 0);
+    __syncthreads();   // the slot table changes hands
+    sweep(S.nup, S.lvl_up, S.urec, y, v, v, true, S.nslot_up > 0);
+}
+
 }  // namespace hfem

@@ -297,6 +297,10 @@ struct hfem_ctx {
     bool have_order = false;
     std::vector<int> h_o2u, h_u2o, lvl_lo, lvl_up;
     int *d_u2o = nullptr, *d_rows_lo = nullptr, *d_rows_up = nullptr, *d_fptr = nullptr, *d_fpos = nullptr;
+    // flattened per-slot lists of the one-CTA factorisation and solves (BiluSched)
+    int *d_frec = nullptr, *d_lrec = nullptr, *d_urec = nullptr;
+    bool bilu_sched = false;            // the one-CTA factorisation and solves apply (BiluSched)
+    int bilu_nslot_lo = 0, bilu_nslot_up = 0;   // slot-table rows of the one-CTA solves
     int *d_lvl_lo = nullptr, *d_lvl_up = nullptr;
     cudaGraphExec_t bilu_exec = nullptr;    // the factorisation's per-level launches, replayed as one graph
     double *Mg = nullptr, *bl_t = nullptr, *bl_y = nullptr;
@@ -758,6 +762,12 @@ int dot(hfem_ctx* c, const double* a, const double* b, double* out, bool sq) {
 }
 
 // ---------------------------------------------------------------- BILU0
+// Block sizes with one-CTA (scheduled) instances of the factorisation and the
+// solves; they run when the levels are short (few rows per level, as the MDF
+// order gives), where a launch or a CTA per row of a level would leave the GPU
+// waiting on the dependency chain.
+bool bilu_sched_bsz(int b) { return b == 8 || b == 12 || b == 15 || b == 16 || b == 20 || b == 30; }
+
 // Same arithmetic as the LU of the oracle's restatement, so that the weights,
 // and with them the ordering, are reproduced bit for bit.
 int host_lu_factor(int n, double* a, int* piv) {
@@ -914,12 +924,122 @@ int compute_ordering(hfem_ctx* c) {
         fptr[i + 1] = (int)fpos.size();
     }
     if (fpos.empty()) fpos.push_back(0);
+    // a new ordering (hfem_reset_ordering) replaces the previous one's tables
+    for (int** q : {&c->d_u2o, &c->d_rows_lo, &c->d_rows_up, &c->d_fptr, &c->d_fpos, &c->d_lvl_lo, &c->d_lvl_up,
+                    &c->d_frec, &c->d_lrec, &c->d_urec})
+        if (*q) {
+            pool_free(*q);
+            *q = nullptr;
+        }
+    // per-slot records of the one-CTA forms (BiluSched), when the block size
+    // has an instance, the levels are short and every row fits their limits
+    std::vector<int> frec, lrec, urec;
+    c->bilu_sched = bilu_sched_bsz(b) && (long long)nf < 32LL * std::max(nl, nu);
+    for (int s = 0; s < nf && c->bilu_sched; s++) {
+        const int i = rows_lo[s];
+        if (rs[i + 1] - rs[i] > BILU_ROWMAX) c->bilu_sched = false;
+    }
+    if (c->bilu_sched) {
+        frec.assign((size_t)nf * BILU_FREC, 0);
+        lrec.assign((size_t)nf * BILU_SREC, 0);
+        urec.assign((size_t)nf * BILU_SREC, 0);
+        for (int s = 0; s < nf && c->bilu_sched; s++) {
+            const int i = rows_lo[s];
+            int* F = &frec[(size_t)s * BILU_FREC];
+            F[0] = i;
+            F[1] = rs[i];
+            F[2] = rs[i + 1] - rs[i];
+            int nr = 0, nuu = 0;
+            for (int f = fptr[i]; f < fptr[i + 1] && c->bilu_sched; f++) {
+                const int p = fpos[f], k = ci[p];
+                if (nr >= 32 || nuu >= 32) { c->bilu_sched = false; break; }
+                const int head = nr++;
+                F[8 + 2 * head] = p - rs[i];
+                F[72 + nuu++] = rs[k];
+                for (int q = rs[i]; q < rs[i + 1]; q++) {
+                    const int l = ci[q];
+                    if (u2o[l] <= u2o[k]) continue;
+                    const int m = row_find(rs, ci, k, l);
+                    if (m < 0) continue;
+                    if (nr >= 32 || nuu >= 32) { c->bilu_sched = false; break; }
+                    F[8 + 2 * nr++] = q - rs[i];
+                    F[72 + nuu++] = m;
+                    F[9 + 2 * head]++;
+                }
+            }
+            F[3] = nr;
+            F[4] = nuu;
+            int* L = &lrec[(size_t)s * BILU_SREC];
+            L[0] = i;
+            for (int q = rs[i] + 1; q < rs[i + 1]; q++)
+                if (u2o[ci[q]] < u2o[i]) {
+                    L[4 + 2 * L[1]] = q;
+                    L[5 + 2 * L[1]] = ci[q];
+                    L[1]++;
+                }
+        }
+        for (int s = 0; s < nf; s++) {
+            const int i = rows_up[s];
+            int* U = &urec[(size_t)s * BILU_SREC];
+            U[0] = i;
+            U[2] = rs[i];
+            for (int q = rs[i] + 1; q < rs[i + 1]; q++)
+                if (u2o[ci[q]] > u2o[i]) {
+                    U[4 + 2 * U[1]] = q;
+                    U[5 + 2 * U[1]] = ci[q];
+                    U[1]++;
+                }
+        }
+        // slots: row i's result is live from its level to the last level that
+        // reads it (later neighbours in the lower solve, earlier ones in the
+        // upper); rows take the free slots of ranges that ended before their level
+        auto assign = [&](const std::vector<int>& L, const std::vector<int>& ptr, const std::vector<int>& rows,
+                          bool lower, std::vector<int>& rec) {
+            const int nlev = (int)ptr.size() - 1;
+            std::vector<int> end(L), slot(nf, 0), freed_ptr(nlev + 1, 0), freed(nf), free_list;
+            for (int i = 0; i < nf; i++)
+                for (int q = rs[i] + 1; q < rs[i + 1]; q++) {
+                    const int k = ci[q];
+                    if (lower ? u2o[k] > u2o[i] : u2o[k] < u2o[i]) end[i] = std::max(end[i], L[k]);
+                }
+            for (int i = 0; i < nf; i++) freed_ptr[end[i] + 1]++;
+            for (int l = 0; l < nlev; l++) freed_ptr[l + 1] += freed_ptr[l];
+            {
+                std::vector<int> fill(freed_ptr.begin(), freed_ptr.end() - 1);
+                for (int i = 0; i < nf; i++) freed[fill[end[i]]++] = i;
+            }
+            int n = 0;
+            for (int l = 0; l < nlev; l++) {
+                if (l > 0)
+                    for (int t = freed_ptr[l - 1]; t < freed_ptr[l]; t++) free_list.push_back(slot[freed[t]]);
+                for (int t = ptr[l]; t < ptr[l + 1]; t++) {
+                    const int i = rows[t];
+                    if (free_list.empty()) slot[i] = n++;
+                    else {
+                        slot[i] = free_list.back();
+                        free_list.pop_back();
+                    }
+                }
+            }
+            for (int t = 0; t < nf; t++) {
+                int* R = &rec[(size_t)t * BILU_SREC];
+                R[3] = slot[R[0]];
+                for (int j = 0; j < R[1]; j++) R[16 + j] = slot[R[5 + 2 * j]];
+            }
+            return n;
+        };
+        c->bilu_nslot_lo = assign(lev, c->lvl_lo, rows_lo, true, lrec);
+        c->bilu_nslot_up = assign(levu, c->lvl_up, rows_up, false, urec);
+    }
     int rc;
     if ((rc = upload(c, &c->d_u2o, u2o.data(), (size_t)nf)) || (rc = upload(c, &c->d_rows_lo, rows_lo.data(), (size_t)nf)) ||
         (rc = upload(c, &c->d_rows_up, rows_up.data(), (size_t)nf)) ||
         (rc = upload(c, &c->d_fptr, fptr.data(), fptr.size())) || (rc = upload(c, &c->d_fpos, fpos.data(), fpos.size())) ||
         (rc = upload(c, &c->d_lvl_lo, c->lvl_lo.data(), c->lvl_lo.size())) ||
-        (rc = upload(c, &c->d_lvl_up, c->lvl_up.data(), c->lvl_up.size())))
+        (rc = upload(c, &c->d_lvl_up, c->lvl_up.data(), c->lvl_up.size())) ||
+        (c->bilu_sched && ((rc = upload(c, &c->d_frec, frec.data(), frec.size())) ||
+                           (rc = upload(c, &c->d_lrec, lrec.data(), lrec.size())) ||
+                           (rc = upload(c, &c->d_urec, urec.data(), urec.size())))))
         return rc;
     if (!c->Mg && (rc = dalloc(c, &c->Mg, b2 * nblk))) return rc;
     if (!c->bl_t && (rc = dalloc(c, &c->bl_t, (size_t)nf * b))) return rc;
@@ -931,6 +1051,30 @@ int compute_ordering(hfem_ctx* c) {
     }
     c->have_order = true;
     return 0;
+}
+
+BiluSched bilu_sched_args(const hfem_ctx* c) {
+    return BiluSched{(int)c->lvl_lo.size() - 1, (int)c->lvl_up.size() - 1, c->d_lvl_lo, c->d_lvl_up,
+                     c->d_frec, c->d_lrec, c->d_urec, c->bilu_nslot_lo, c->bilu_nslot_up};
+}
+
+template <int B>
+void launch_bilu_factor_sched(hfem_ctx* c, const BiluSched& S) {
+    using C = BiluFacCfg<B>;
+    cudaFuncSetAttribute(bilu0_factor_sched_kernel<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+    bilu0_factor_sched_kernel<B><<<1, 32 * C::NW, C::SMEM, c->stream>>>(S, c->Mg, c->binfo);
+}
+template <int B, class MT>
+void launch_bilu_solve_sched(hfem_ctx* c, BiluSched S, const MT* M, const double* x, double* v) {
+    using C = BiluSolCfg<B, MT>;
+    int nslot = std::max(S.nslot_lo, S.nslot_up), nw = C::warps(nslot);
+    if (nw == 0) {   // results too many to keep: read them from global memory
+        S.nslot_lo = S.nslot_up = nslot = 0;
+        nw = C::warps(0);
+    }
+    const size_t smem = C::smem(nw, nslot);
+    cudaFuncSetAttribute(bilu0_solve_sched_kernel<B, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    bilu0_solve_sched_kernel<B, MT><<<1, 32 * nw, smem, c->stream>>>(S, M, x, c->bl_y, v);
 }
 
 void enqueue_bilu0_levels(hfem_ctx* c, cudaStream_t st) {
@@ -952,7 +1096,16 @@ int bilu0_factor(hfem_ctx* c) {
     const int nf = c->dims.nf, b = c->bsz;
     const size_t b2 = (size_t)b * b;
     CK(cudaMemcpyAsync(c->Mg, c->Hg, sizeof(double) * b2 * c->dims.nblocks, cudaMemcpyDeviceToDevice, c->stream));
-    if (!c->bilu_exec) {
+    if (c->bilu_sched) {
+        const BiluSched S = bilu_sched_args(c);
+        switch (b) {
+#define HFEM_BF(B) \
+    case B: launch_bilu_factor_sched<B>(c, S); break;
+            HFEM_BF(8) HFEM_BF(12) HFEM_BF(15) HFEM_BF(16) HFEM_BF(20) HFEM_BF(30)
+#undef HFEM_BF
+            default: break;
+        }
+    } else if (!c->bilu_exec) {
         cudaStream_t cap = nullptr;
         cudaGraph_t g = nullptr;
         if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) == cudaSuccess &&
@@ -966,7 +1119,8 @@ int bilu0_factor(hfem_ctx* c) {
         if (cap) cudaStreamDestroy(cap);
         cudaGetLastError();
     }
-    if (c->bilu_exec) CK(cudaGraphLaunch(c->bilu_exec, c->stream));
+    if (c->bilu_sched) {
+    } else if (c->bilu_exec) CK(cudaGraphLaunch(c->bilu_exec, c->stream));
     else enqueue_bilu0_levels(c, c->stream);
     int rc = check_launch(c, "bilu0_factor");
     if (rc) return rc;
@@ -992,6 +1146,20 @@ int bilu0_apply(hfem_ctx* c, const double* x, double* v) {
     BiluSolveArgs a{c->bsz, c->rowstart, c->colidx, c->d_u2o, nullptr, 0, f32 ? (const void*)c->Mg32 : c->Mg, x,
                     c->bl_y, v};
     const int nlo = (int)c->lvl_lo.size() - 1, nup = (int)c->lvl_up.size() - 1;
+    if (c->bilu_sched) {
+        const BiluSched S = bilu_sched_args(c);
+        switch (c->bsz) {
+#define HFEM_BS(B)                                                          \
+    case B:                                                                 \
+        if (f32) launch_bilu_solve_sched<B, float>(c, S, c->Mg32, x, v);     \
+        else launch_bilu_solve_sched<B, double>(c, S, c->Mg, x, v);          \
+        break;
+            HFEM_BS(8) HFEM_BS(12) HFEM_BS(15) HFEM_BS(16) HFEM_BS(20) HFEM_BS(30)
+#undef HFEM_BS
+            default: break;
+        }
+        return check_launch(c, "bilu0_apply");
+    }
     // few rows per level: one CTA walks all levels (no launch per level)
     if ((long long)c->dims.nf < 64LL * std::max(nlo, nup)) {
         if (f32)
@@ -1585,7 +1753,7 @@ int hfem_destroy(hfem_ctx* c) {
                     c->eprob, c->fprob, c->pparam, c->palpha, c->seg_pstart, c->seg_pseg, c->seg_p0,
                     c->seg_ticket, c->seg_part, c->seg_partk, c->seg_h, c->seg_y, c->seg_nrm, c->seg_act, c->seg_k, c->tc_err, c->rn_part, c->bf, c->bcm, c->bcs, c->Minv32,
                     c->d_u2o, c->d_rows_lo, c->d_rows_up, c->d_fptr, c->d_fpos, c->Mg, c->bl_t, c->bl_y,
-                    c->d_lvl_lo, c->d_lvl_up, c->Mg32, c->gm_H, c->gm_cs, c->gm_sn, c->gm_g, c->gm_nrmb, c->gm_hist,
+                    c->d_lvl_lo, c->d_lvl_up, c->Mg32, c->d_frec, c->d_lrec, c->d_urec, c->gm_H, c->gm_cs, c->gm_sn, c->gm_g, c->gm_nrmb, c->gm_hist,
                     c->gm_state, c->gm_its, c->gm_jc};
     for (void* p : ptrs)
         if (p) pool_free(p);

@@ -4,6 +4,9 @@
 * GMRES(50) with BILU0 to 1e-10: same iteration count (+-1) and solution
   within 1e-8 relative; the first residual estimates agree to 1e-9.
 * Newton with BILU0 converges to the FP64 residual tolerance.
+
+Block sizes up to 32 with short levels (the MDF order's) run the one-CTA
+factorisation and solves; block size 50 the per-level launches.
 """
 import numpy as np
 import pytest
@@ -20,7 +23,9 @@ CASES = [("2d_p2", lambda: ns2d_vortex(n=5, porder=2, seed=4)),
          # bounded meshes (face blocks of boundary faces have fewer neighbours)
          ("2d_p2_channel", lambda: ns2d_channel(n=4, porder=2, seed=7)),
          ("2d_p2_channel_roe_sutherland", lambda: with_models(ns2d_channel(n=4, porder=2, seed=9), 2, 1)),
-         ("3d_p1_box", lambda: ns3d_box(n=2, porder=1))]
+         ("3d_p1_box", lambda: ns3d_box(n=2, porder=1)),
+         # block size 50: the per-level launches (the one-CTA forms take blocks up to 32)
+         ("3d_p3_box", lambda: ns3d_box(n=2, porder=3))]
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
