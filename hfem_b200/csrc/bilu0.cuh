@@ -351,9 +351,11 @@ struct BiluFacCfg {
 // The factorisation of every level in one CTA: row i, held in shared memory,
 // takes for each earlier neighbour k in order L_ik = M_ik U_kk^-1 and
 // M_il -= L_ik U_kl, then inverts its diagonal block by Gauss-Jordan with
-// partial pivoting in registers (row r in lane r; the pivot is the first row
-// of largest magnitude, as in smem_blk_inv), and is written back.  The block
-// products sum in the order of smem_blk_mul.
+// partial pivoting in registers, and is written back.  The inverse is the one
+// smem_blk_inv computes (same pivots: the first position of largest magnitude;
+// same operations), with each lane keeping its row and tracking the position
+// the row swaps give it, so a swap costs no data movement.  The block products
+// sum in the order of smem_blk_mul.
 template <int B>
 __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S, double* Mg, int* info) {
     static_assert(B <= 32, "one lane per block row");
@@ -417,45 +419,42 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
                 }
             }
         }
-        // the diagonal block (first in the row)
+        // the diagonal block (first in the row), inverted in place: lane r
+        // holds the row now at position pos (row swaps move positions only)
         double a[B];
         int piv[B];
 #pragma unroll
         for (int c = 0; c < B; c++) a[c] = rowbuf[r + B * c];
-        int bad = 0;
+        int pos = lane, bad = 0;
 #pragma unroll
         for (int k = 0; k < B; k++) {
-            double v = (lane >= k && lane < B) ? fabs(a[k]) : -1.0;
-            int p = lane;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double v2 = __shfl_xor_sync(FULL, v, o);
-                const int p2 = __shfl_xor_sync(FULL, p, o);
-                if (v2 > v || (v2 == v && p2 < p)) {
-                    v = v2;
-                    p = p2;
-                }
-            }
-            // one lane's choice for all (lanes agree unless the block holds NaNs)
-            p = __shfl_sync(FULL, p, 0);
-            v = __shfl_sync(FULL, v, 0);
-            piv[k] = p;
-            if (v == 0.0) {
+            // pivot: the first position >= k of largest magnitude in column k,
+            // compared across the warp as (high word, low word) of |a|, then position
+            const bool cand = pos >= k && pos < B;
+            const double m = cand ? fabs(a[k]) : 0.0;
+            const unsigned hi = m > 0.0 ? (unsigned)__double2hiint(m) : 0u;
+            const unsigned lo = m > 0.0 ? (unsigned)__double2loint(m) : 0u;
+            const unsigned mh = __reduce_max_sync(FULL, cand ? hi : 0u);
+            const unsigned ml = __reduce_max_sync(FULL, (cand && hi == mh) ? lo : 0u);
+            if (mh == 0u && ml == 0u) {
                 bad = k + 1;
                 break;
             }
-            const int src = lane == k ? p : (lane == p ? k : lane);
-#pragma unroll
-            for (int c = 0; c < B; c++) a[c] = __shfl_sync(FULL, a[c], src);
-            const double dinv = 1.0 / __shfl_sync(FULL, a[k], k);
-            if (lane == k)
+            const unsigned key =
+                __reduce_min_sync(FULL, (cand && hi == mh && lo == ml) ? (unsigned)(pos * 32 + lane) : 0xffffffffu);
+            const int pp = (int)(key >> 5), lp = (int)(key & 31u);
+            piv[k] = pp;
+            if (pos == k) pos = pp;
+            else if (lane == lp) pos = k;
+            const double dinv = 1.0 / __shfl_sync(FULL, a[k], lp);
+            if (lane == lp)
 #pragma unroll
                 for (int c = 0; c < B; c++) a[c] = (c == k ? 1.0 : a[c]) * dinv;
             const double col = a[k];
 #pragma unroll
             for (int c = 0; c < B; c++) {
-                const double pc = __shfl_sync(FULL, a[c], k);
-                if (lane != k) a[c] = (c == k ? 0.0 : a[c]) - col * pc;
+                const double pc = __shfl_sync(FULL, a[c], lp);
+                if (lane != lp) a[c] = (c == k ? 0.0 : a[c]) - col * pc;
             }
         }
         if (!bad) {
@@ -470,9 +469,10 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
                         a[c] = ak;
                     }
             }
+            __syncwarp();
             if (lane < B)
 #pragma unroll
-                for (int c = 0; c < B; c++) rowbuf[r + B * c] = a[c];
+                for (int c = 0; c < B; c++) rowbuf[pos + B * c] = a[c];
         }
         __syncwarp();
         for (int t = lane; t < nrb * B2; t += 32) Mg[(size_t)r0 * B2 + t] = rowbuf[t];
