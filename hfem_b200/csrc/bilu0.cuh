@@ -8,9 +8,10 @@
 // the updates of its earlier neighbours k in increasing order -- the same
 // sequence of block updates the reference's right-looking loop applies to
 // row i -- so rows whose earlier neighbours are all final can be factored
-// concurrently.  The host groups rows into such levels; one launch per level
-// (one CTA per row), and the triangular solves of the apply run level by
-// level the same way.
+// concurrently.  The host groups rows into such levels, and the factorisation
+// and the triangular solves of the apply walk them level by level: in one CTA
+// when the levels are short (the scheduled forms at the end of this file),
+// else one launch per level (one CTA per row).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -511,12 +512,12 @@ __device__ __forceinline__ void bl_cp_commit() { asm volatile("cp.async.commit_g
 __device__ __forceinline__ void bl_cp_wait_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // Both triangular solves in one CTA, v = U^-1 L^-1 x, software-pipelined
-// over the levels: a warp's record for level l + 2 and the blocks and
-// right-hand side entry of its row of level l + 1 are requested before the
-// barrier that ends level l, so after the barrier only the neighbours' vector
-// entries (the previous levels' results) are loaded.  Level l's record lives
-// in record buffer l mod 2; a warp's further rows of a level (levels wider
-// than the CTA) go through the third buffer without the pipeline.  For
+// over each warp's rows: warp w owns slots w, w + nw, ... of the level order,
+// and after the barrier that ends a level in which it finished a row it
+// requests the blocks and right-hand side entry of its next row (typically
+// several levels later) and the record of the row after that, so a row's own
+// data has arrived by the time its level starts and only the neighbours'
+// results (previous levels') are read after the barrier.  For
 // B <= 16 the two half-warps take alternate entries and add their partial
 // sums by one shuffle; the upper solve's product with U_ii^-1 takes the row's
 // sums from the lanes that hold them.
@@ -586,30 +587,42 @@ __global__ void __launch_bounds__(512, 1) bilu0_solve_sched_kernel(BiluSched S, 
     // U_ii^-1 (rhs_i - sum) (upper)
     auto sweep = [&](int nlev, const int* lvl, const int* rec, const double* b, const double* vec, double* out,
                      bool upper, bool slots) {
+        const int nrow = nlev > 0 ? lvl[nlev] : 0;
+        // this warp's rows: slots w, w + nw, w + 2 nw, ... of the level order
+        // (about nw / (rows per level) levels apart); the record of the warp's
+        // j-th row lives in record buffer j mod 2
+        int s = w, j = 0;
         double rhs = 0.0;
-        // prologue: the records of levels 0 and 1, the row of level 0
-        if (nlev > 0 && w < lvl[1]) bl_fetch_record(rcb, rec + (size_t)w * BILU_SREC, BILU_SREC, lane);
+        // prologue: the records of the first two rows, the blocks of the first
+        if (s < nrow) bl_fetch_record(rcb, rec + (size_t)s * BILU_SREC, BILU_SREC, lane);
         bl_cp_wait_all();
         __syncwarp();
-        if (nlev > 0 && w < lvl[1]) rhs = issue_row(rcb, b, upper);
+        if (s < nrow) rhs = issue_row(rcb, b, upper);
         bl_cp_commit();
-        if (nlev > 1 && lvl[1] + w < lvl[2])
-            bl_fetch_record(rcb + BILU_SREC, rec + (size_t)(lvl[1] + w) * BILU_SREC, BILU_SREC, lane);
+        if (s + nw < nrow) bl_fetch_record(rcb + BILU_SREC, rec + (size_t)(s + nw) * BILU_SREC, BILU_SREC, lane);
         bl_cp_commit();
+        // request the warp's next row (slot s, its j-th): its blocks (its record
+        // arrived while the previous row waited), then the record of the row after it
+        auto advance = [&]() {
+            __syncwarp();
+            if (s < nrow) {
+                bl_cp_wait_all();
+                __syncwarp();
+                rhs = issue_row(rcb + (j & 1) * BILU_SREC, b, upper);
+            }
+            bl_cp_commit();
+            if (s + nw < nrow)
+                bl_fetch_record(rcb + ((j + 1) & 1) * BILU_SREC, rec + (size_t)(s + nw) * BILU_SREC, BILU_SREC, lane);
+            bl_cp_commit();
+        };
+        // a warp that finished a row requests its next one after the barrier,
+        // off the path of the level that row ended
+        bool pend = false;
         for (int l = 0; l < nlev; l++) {
-            const int sb = lvl[l], se = lvl[l + 1];
-            int* rc = rcb + (l & 1) * BILU_SREC;
-            for (int s = sb + w; s < se; s += nw) {
-                if (s == sb + w) {
-                    bl_cp_wait_but_one();   // this row's blocks (the next record may still be in flight)
-                } else {
-                    rc = rcb + 2 * BILU_SREC;
-                    bl_fetch_record(rc, rec + (size_t)s * BILU_SREC, BILU_SREC, lane);
-                    bl_cp_wait_all();
-                    __syncwarp();
-                    rhs = issue_row(rc, b, upper);
-                    bl_cp_wait_all();
-                }
+            for (const int se = lvl[l + 1]; s < se;) {
+                if (pend) advance();
+                const int* rc = rcb + (j & 1) * BILU_SREC;
+                bl_cp_wait_but_one();   // this row's blocks (the next row's record may still be in flight)
                 __syncwarp();
                 const double t = rowsum(rc, vec, slots);
                 double o = rhs - t;
@@ -624,20 +637,15 @@ __global__ void __launch_bounds__(512, 1) bilu0_solve_sched_kernel(BiluSched S, 
                     out[(size_t)rc[0] * B + r] = o;
                     if (slots) tab[(size_t)rc[3] * B + r] = o;
                 }
+                s += nw;
+                j++;
+                pend = true;
             }
-            // the row of level l + 1 (its record arrived during this level), the record of level l + 2
-            __syncwarp();
-            if (l + 1 < nlev && lvl[l + 1] + w < lvl[l + 2]) {
-                bl_cp_wait_all();
-                __syncwarp();
-                rhs = issue_row(rcb + ((l + 1) & 1) * BILU_SREC, b, upper);
-            }
-            bl_cp_commit();
-            if (l + 2 < nlev && lvl[l + 2] + w < lvl[l + 3])
-                bl_fetch_record(rcb + (l & 1) * BILU_SREC, rec + (size_t)(lvl[l + 2] + w) * BILU_SREC, BILU_SREC,
-                                lane);
-            bl_cp_commit();
             __syncthreads();
+            if (pend) {
+                advance();
+                pend = false;
+            }
         }
         bl_cp_wait_all();
     };
