@@ -277,14 +277,14 @@ __global__ void __launch_bounds__(1024) bilu0_apply_cta_kernel(BiluSolveArgs A, 
 
 // ---------------------------------------------------------------------------
 // Scheduled forms for block sizes up to 32, for orderings whose levels hold
-// few rows.  One CTA walks the levels with a CTA barrier between them, one
-// warp per row of a level, lane r owning row r of the row's blocks.  The host
-// flattens every index chain into per-slot lists (a slot is a row's place in
-// the level order), and each warp stages what does not depend on the previous
-// level -- its next row's lists, and the blocks that are final before that
-// level starts -- into registers and shared memory by asynchronous copies
-// before the level barrier; after the barrier it fetches only what the
-// previous levels produced, in one round of copies.
+// few rows.  One CTA walks the levels with a CTA barrier between them; warp w
+// owns slots w, w + nw, ... of the level order (a slot is a row's place in
+// it), lane r owning row r of the row's blocks.  The host flattens every
+// index chain into one fixed-stride record per slot, and each warp requests
+// what does not depend on earlier levels -- its next row's record, and the
+// blocks that are final before that row's level starts -- by asynchronous
+// copies as soon as its previous row is done, typically levels ahead; after
+// a row's level barrier only what the previous levels produced is fetched.
 //
 // Every array these kernels write (the factors, y, v) is written by this one
 // CTA, so the L1-cached copies below see its own writes after a barrier.
@@ -343,7 +343,7 @@ struct BiluFacCfg {
     static constexpr int B2 = B * B;
     static constexpr int UBUF = B <= 20 ? 8 : 4;                       // U blocks staged per round
     static constexpr size_t BLK_BYTES = (((size_t)(BILU_ROWMAX + UBUF) * B2 * sizeof(double) + 15) / 16) * 16;
-    static constexpr size_t WARP_BYTES = BLK_BYTES + BILU_FREC * 4;
+    static constexpr size_t WARP_BYTES = BLK_BYTES + 2 * BILU_FREC * 4;  // blocks, two records
     static constexpr int NW0 = (int)((200 * 1024) / WARP_BYTES);
     static constexpr int NW = NW0 > 8 ? 8 : NW0;                       // warps of the CTA
     static constexpr size_t SMEM = WARP_BYTES * NW;
@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
     const int r = lane < B ? lane : 0;   // lanes >= B repeat row 0 and store nothing
     double* rowbuf = reinterpret_cast<double*>(bf_raw + (size_t)w * C::WARP_BYTES);
     double* ubuf = rowbuf + (size_t)BILU_ROWMAX * B2;
-    int* rc = reinterpret_cast<int*>(bf_raw + (size_t)w * C::WARP_BYTES + C::BLK_BYTES);
+    int* rcb = reinterpret_cast<int*>(bf_raw + (size_t)w * C::WARP_BYTES + C::BLK_BYTES);   // 2 x BILU_FREC
+    int* rc = rcb;   // the record of the warp's current row
     // stage U blocks ub .. ub + UBUF - 1 of the row's list
     auto stage = [&](int ub, int nu) {
         __syncwarp();
@@ -377,11 +378,9 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
         bl_cp_wait_all();
         __syncwarp();
     };
+    // the row's own blocks were requested by advance (below); stage(0) waits for them
     auto factor_row = [&]() {
-        bl_cp_wait_all();
-        __syncwarp();
         const int i = rc[0], r0 = rc[1], nrb = rc[2], nrec = rc[3], nu = rc[4];
-        bl_warp_copy(rowbuf, Mg + (size_t)r0 * B2, nrb * B2, lane);
         int uc = 0, rb = 0;
         stage(0, nu);
         for (int j = 0; j < nrec;) {
@@ -479,17 +478,42 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
         for (int t = lane; t < nrb * B2; t += 32) Mg[(size_t)r0 * B2 + t] = rowbuf[t];
         if (lane == 0) info[i] = bad;
     };
-    if (S.nlo > 0 && w < S.lvl_lo[1]) bl_fetch_record(rc, S.frec + (size_t)w * BILU_FREC, BILU_FREC, lane);
-    for (int l = 0; l < S.nlo; l++) {
-        const int sb = S.lvl_lo[l], se = S.lvl_lo[l + 1];
-        for (int s = sb + w; s < se; s += nw) {
-            if (s != sb + w) bl_fetch_record(rc, S.frec + (size_t)s * BILU_FREC, BILU_FREC, lane);
-            factor_row();
+    // warp w owns slots w, w + nw, ... of the level order; the record of its
+    // jr-th row lives in record buffer jr mod 2.  A row's own blocks change
+    // only while it is factored, so they are requested as soon as the warp's
+    // previous row is done (after the barrier that ends its level), typically
+    // levels before the row's own level starts.
+    const int nrow = S.nlo > 0 ? S.lvl_lo[S.nlo] : 0;
+    int s = w, jr = 0;
+    auto advance = [&]() {   // row jr (slot s): its blocks, then the record of the warp's next row
+        __syncwarp();
+        if (s < nrow) {
+            bl_cp_wait_all();
+            __syncwarp();
+            rc = rcb + (jr & 1) * BILU_FREC;
+            bl_warp_copy(rowbuf, Mg + (size_t)rc[1] * B2, rc[2] * B2, lane);
         }
-        if (l + 1 < S.nlo && S.lvl_lo[l + 1] + w < S.lvl_lo[l + 2])
-            bl_fetch_record(rc, S.frec + (size_t)(S.lvl_lo[l + 1] + w) * BILU_FREC, BILU_FREC, lane);
+        if (s + nw < nrow)
+            bl_fetch_record(rcb + ((jr + 1) & 1) * BILU_FREC, S.frec + (size_t)(s + nw) * BILU_FREC, BILU_FREC, lane);
+    };
+    if (s < nrow) bl_fetch_record(rcb, S.frec + (size_t)s * BILU_FREC, BILU_FREC, lane);
+    advance();
+    bool pend = false;
+    for (int l = 0; l < S.nlo; l++) {
+        for (const int se = S.lvl_lo[l + 1]; s < se;) {
+            if (pend) advance();
+            factor_row();
+            s += nw;
+            jr++;
+            pend = true;
+        }
         __syncthreads();
+        if (pend) {
+            advance();
+            pend = false;
+        }
     }
+    bl_cp_wait_all();
 }
 
 template <int B, class MT>
