@@ -354,9 +354,10 @@ struct BiluFacCfg {
 // M_il -= L_ik U_kl, then inverts its diagonal block by Gauss-Jordan with
 // partial pivoting in registers, and is written back.  The inverse is the one
 // smem_blk_inv computes (same pivots: the first position of largest magnitude;
-// same operations), with each lane keeping its row and tracking the position
-// the row swaps give it, so a swap costs no data movement.  The block products
-// sum in the order of smem_blk_mul.
+// same operations), with the lanes of a row keeping it and tracking the
+// position the row swaps give it, so a swap costs no data movement.  The block
+// products sum in the order of smem_blk_mul.  For B <= 16 the two half-warps
+// split every row's columns, halving each lane's products and eliminations.
 template <int B>
 __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S, double* Mg, int* info) {
     static_assert(B <= 32, "one lane per block row");
@@ -365,7 +366,12 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char bf_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int r = lane < B ? lane : 0;   // lanes >= B repeat row 0 and store nothing
+    // for B <= 16 each half-warp holds half of every block row's columns:
+    // lane h * 16 + r owns row r, columns h * CH .. h * CH + CH - 1
+    constexpr int H = B <= 16 ? 2 : 1, LW = 32 / H, CH = (B + H - 1) / H;
+    const int h = lane / LW, rl = lane % LW, cb = h * CH;
+    const bool act = rl < B;
+    const int r = act ? rl : 0;   // lanes of rows >= B repeat row 0 and store nothing
     double* rowbuf = reinterpret_cast<double*>(bf_raw + (size_t)w * C::WARP_BYTES);
     double* ubuf = rowbuf + (size_t)BILU_ROWMAX * B2;
     int* rcb = reinterpret_cast<int*>(bf_raw + (size_t)w * C::WARP_BYTES + C::BLK_BYTES);   // 2 x BILU_FREC
@@ -390,19 +396,29 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
             const double* Ukk = ubuf + (size_t)(uc - rb) * B2;
             uc++;
             double* Mik = rowbuf + (size_t)pl * B2;
-            double m[B], lv[B];
+            // L_ik = M_ik U_kk^-1: the lane's columns of row r (the whole row of
+            // M_ik, which the other half-warp may have just updated, is read)
+            double m[B], lv[CH];
+            __syncwarp();
 #pragma unroll
-            for (int c = 0; c < B; c++) m[c] = Mik[r + B * c];
+            for (int q = 0; q < B; q++) m[q] = Mik[r + B * q];
 #pragma unroll
-            for (int c = 0; c < B; c++) {
+            for (int cc = 0; cc < CH; cc++) {
+                const int c = min(cb + cc, B - 1);
                 double t = 0.0;
 #pragma unroll
                 for (int q = 0; q < B; q++) t = fma(m[q], Ukk[q + B * c], t);
-                lv[c] = t;
+                lv[cc] = t;
             }
-            if (lane < B)
+            __syncwarp();
+            if (act)
 #pragma unroll
-                for (int c = 0; c < B; c++) Mik[r + B * c] = lv[c];
+                for (int cc = 0; cc < CH; cc++)
+                    if (cb + cc < B) Mik[r + B * (cb + cc)] = lv[cc];
+            __syncwarp();
+            // M_il -= L_ik U_kl with the whole row r of L_ik
+#pragma unroll
+            for (int q = 0; q < B; q++) m[q] = Mik[r + B * q];
             for (int u = 0; u < nupd; u++) {
                 const int ql = rc[8 + 2 * j];
                 j++;
@@ -411,29 +427,32 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
                 uc++;
                 double* Mil = rowbuf + (size_t)ql * B2;
 #pragma unroll
-                for (int c = 0; c < B; c++) {
+                for (int cc = 0; cc < CH; cc++) {
+                    const int c = min(cb + cc, B - 1);
                     double t = 0.0;
 #pragma unroll
-                    for (int q = 0; q < B; q++) t = fma(lv[q], Ukl[q + B * c], t);
-                    if (lane < B) Mil[r + B * c] -= t;
+                    for (int q = 0; q < B; q++) t = fma(m[q], Ukl[q + B * c], t);
+                    if (act && cb + cc < B) Mil[r + B * c] -= t;
                 }
             }
         }
-        // the diagonal block (first in the row), inverted in place: lane r
-        // holds the row now at position pos (row swaps move positions only)
-        double a[B];
+        // the diagonal block (first in the row), inverted in place: the lanes
+        // of row r hold the row now at position pos (row swaps move positions only)
+        double a[CH];
         int piv[B];
+        __syncwarp();
 #pragma unroll
-        for (int c = 0; c < B; c++) a[c] = rowbuf[r + B * c];
-        int pos = lane, bad = 0;
+        for (int cc = 0; cc < CH; cc++) a[cc] = cb + cc < B ? rowbuf[r + B * (cb + cc)] : 0.0;
+        int pos = rl, bad = 0;
 #pragma unroll
         for (int k = 0; k < B; k++) {
+            const int hk = k / CH, kc = k % CH;   // the half and slot holding column k
             // pivot: the first position >= k of largest magnitude in column k,
             // compared across the warp as (high word, low word) of |a|, then position
-            const bool cand = pos >= k && pos < B;
-            const double m = cand ? fabs(a[k]) : 0.0;
-            const unsigned hi = m > 0.0 ? (unsigned)__double2hiint(m) : 0u;
-            const unsigned lo = m > 0.0 ? (unsigned)__double2loint(m) : 0u;
+            const bool cand = h == hk && pos >= k && pos < B;
+            const double mg = cand ? fabs(a[kc]) : 0.0;
+            const unsigned hi = mg > 0.0 ? (unsigned)__double2hiint(mg) : 0u;
+            const unsigned lo = mg > 0.0 ? (unsigned)__double2loint(mg) : 0u;
             const unsigned mh = __reduce_max_sync(FULL, cand ? hi : 0u);
             const unsigned ml = __reduce_max_sync(FULL, (cand && hi == mh) ? lo : 0u);
             if (mh == 0u && ml == 0u) {
@@ -442,37 +461,56 @@ __global__ void __launch_bounds__(256, 1) bilu0_factor_sched_kernel(BiluSched S,
             }
             const unsigned key =
                 __reduce_min_sync(FULL, (cand && hi == mh && lo == ml) ? (unsigned)(pos * 32 + lane) : 0xffffffffu);
-            const int pp = (int)(key >> 5), lp = (int)(key & 31u);
+            const int pp = (int)(key >> 5), lp = (int)(key & 31u), lr = lp % LW;
             piv[k] = pp;
             if (pos == k) pos = pp;
-            else if (lane == lp) pos = k;
-            const double dinv = 1.0 / __shfl_sync(FULL, a[k], lp);
-            if (lane == lp)
+            else if (rl == lr) pos = k;
+            const double dinv = 1.0 / __shfl_sync(FULL, a[kc], lp);
+            if (rl == lr)
 #pragma unroll
-                for (int c = 0; c < B; c++) a[c] = (c == k ? 1.0 : a[c]) * dinv;
-            const double col = a[k];
+                for (int cc = 0; cc < CH; cc++) a[cc] = (cb + cc == k ? 1.0 : a[cc]) * dinv;
+            const double col = __shfl_sync(FULL, a[kc], hk * LW + rl);
 #pragma unroll
-            for (int c = 0; c < B; c++) {
-                const double pc = __shfl_sync(FULL, a[c], lp);
-                if (lane != lp) a[c] = (c == k ? 0.0 : a[c]) - col * pc;
+            for (int cc = 0; cc < CH; cc++) {
+                const double pc = __shfl_sync(FULL, a[cc], h * LW + lr);
+                if (rl != lr) a[cc] = (cb + cc == k ? 0.0 : a[cc]) - col * pc;
             }
         }
         if (!bad) {
+            // undo the column order of the pivots: swap columns k and piv[k], last first
 #pragma unroll
             for (int k = B - 1; k >= 0; k--) {
                 const int p = piv[k];
-                const double ak = a[k];
+                const int hk = k / CH, kc = k % CH, hp = p / CH, pc = p % CH;
+                if (p != k && hk == hp) {
+                    if (h == hk) {
+                        const double ak = a[kc];
 #pragma unroll
-                for (int c = k + 1; c < B; c++)
-                    if (c == p) {
-                        a[k] = a[c];
-                        a[c] = ak;
+                        for (int cc = 0; cc < CH; cc++)
+                            if (cc == pc) {
+                                a[kc] = a[cc];
+                                a[cc] = ak;
+                            }
                     }
+                } else if (p != k) {
+                    double xp = 0.0;
+#pragma unroll
+                    for (int cc = 0; cc < CH; cc++)
+                        if (cc == pc) xp = a[cc];
+                    const double vk = __shfl_sync(FULL, a[kc], hk * LW + rl);
+                    const double vp = __shfl_sync(FULL, xp, hp * LW + rl);
+                    if (h == hk) a[kc] = vp;
+                    if (h == hp)
+#pragma unroll
+                        for (int cc = 0; cc < CH; cc++)
+                            if (cc == pc) a[cc] = vk;
+                }
             }
             __syncwarp();
-            if (lane < B)
+            if (act)
 #pragma unroll
-                for (int c = 0; c < B; c++) rowbuf[pos + B * c] = a[c];
+                for (int cc = 0; cc < CH; cc++)
+                    if (cb + cc < B) rowbuf[pos + B * (cb + cc)] = a[cc];
         }
         __syncwarp();
         for (int t = lane; t < nrb * B2; t += 32) Mg[(size_t)r0 * B2 + t] = rowbuf[t];
